@@ -1,0 +1,184 @@
+/*
+ * mppi_backend.h — C ABI of the B200 (CUDA, sm_100a) MPPI backend.
+ *
+ * This is the seam the reference keeps between its driver and its GPU code
+ * (MarshallVielmetti/mppi_metal src/metal_backend.hpp:22-108, the
+ * Objective-C++ MetalBackend class).  Each entry point below names the
+ * MetalBackend method it replaces.  Plain C: opaque handle, plain pointers and
+ * sizes, int status (0 = success), and an optional caller buffer for the
+ * error text (err may be NULL, as the reference's std::string* error may be).
+ *
+ * Ownership: nothing passed in is retained; device buffers belong to the
+ * backend and are released by mppi_backend_destroy.  A backend is not
+ * thread-safe; use one per host thread (each owns its CUDA stream).
+ *
+ * The C++ driver (include/mppi_metal/mppi_driver.hpp) is the public API and
+ * calls this layer; tests and benchmarks may call it directly.
+ */
+#ifndef MPPI_B200_BACKEND_H
+#define MPPI_B200_BACKEND_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define MPPI_OK 0
+#define MPPI_ERR_INVALID 1     /* bad argument / shape / state */
+#define MPPI_ERR_PLUGIN 2      /* plugin source missing, unreadable or failing to compile */
+#define MPPI_ERR_CALLABLE 3    /* a named callable is not defined by the plugin */
+#define MPPI_ERR_CUDA 4        /* CUDA runtime / driver failure */
+#define MPPI_ERR_NO_DEVICE 5   /* no usable CUDA device */
+#define MPPI_ERR_NOT_INIT 6    /* backend not initialized */
+
+typedef struct mppi_backend mppi_backend;
+
+/* DriverConfig as the backend needs it (reference mppi_types.hpp:46-62). */
+typedef struct mppi_backend_config {
+  uint32_t state_dim;
+  uint32_t control_dim;
+  uint32_t horizon;
+  uint32_t sample_count;
+  float lambda;
+  uint32_t covariance_form; /* 0: sigma = per-dim std-dev; 1: sigma = full covariance */
+  const float* sigma;       /* control_dim or control_dim^2 floats */
+  const float* sigma_inv;   /* same shape; read only when control_cost != 0 */
+  const float* u_min;       /* control_dim */
+  const float* u_max;       /* control_dim */
+  uint32_t numeric_mode;    /* DriverConfig::NumericMode (0 = FP32) */
+  uint32_t control_cost;    /* DriverOptions::control_cost */
+} mppi_backend_config;
+
+/* ModelPluginSpec (reference mppi_types.hpp:79-101). */
+typedef struct mppi_backend_plugin {
+  const char* source_path;   /* CUDA source with the __device__ callables */
+  const char* dynamics;      /* required */
+  const char* stage_cost;    /* NULL or "": library default (0) */
+  const char* terminal_cost; /* NULL or "": library default (0) */
+  uint64_t model_params_size; /* ParamLayout sizes: every blob bound or */
+  uint64_t cost_params_size;  /* overridden later has exactly this size */
+  uint64_t seed;              /* RngConfig::seed; the device key is its low 32 bits */
+} mppi_backend_plugin;
+
+/* Per-agent inputs of a batch (project extension; NULL = shared). */
+typedef struct mppi_batch_agents {
+  const void* model_params;
+  uint64_t model_params_stride; /* bytes between consecutive agents' blobs */
+  const void* cost_params;
+  uint64_t cost_params_stride;
+  const float* sigma;           /* [N][control_dim] or [N][control_dim^2] */
+} mppi_batch_agents;
+
+/* Constructs an empty backend (MetalBackend::MetalBackend, metal_backend.mm:215). */
+int mppi_backend_create(mppi_backend** out);
+/* Releases the backend and its device memory (MetalBackend::~MetalBackend). */
+void mppi_backend_destroy(mppi_backend* b);
+
+/* Compiles the plugin with the library kernels and allocates device state
+ * (MetalBackend::initialize, metal_backend.hpp:35-39 / metal_backend.mm:225-573). */
+int mppi_backend_initialize(mppi_backend* b, const mppi_backend_plugin* plugin,
+                            const mppi_backend_config* config, char* err, size_t err_len);
+
+/* Uploads the bound parameter blobs (MetalBackend::bind_params,
+ * metal_backend.hpp:42-46 / metal_backend.mm:579-600).  Sizes must equal the
+ * plugin's ParamLayout sizes (0 with a NULL pointer unbinds). */
+int mppi_backend_bind_params(mppi_backend* b, const void* model_params, size_t model_bytes,
+                             const void* cost_params, size_t cost_bytes, char* err,
+                             size_t err_len);
+
+/* One control step: rollout -> weights -> update (MetalBackend::dispatch_rollout,
+ * metal_backend.hpp:57-68 / metal_backend.mm:604-741).  Blob overrides with
+ * bytes == 0 use the bound params.  diag3 = {best, mean, ESS}; may be NULL. */
+int mppi_backend_dispatch_rollout(mppi_backend* b, uint64_t step_index, const float* x0,
+                                  const float* u_nominal, const void* model_params,
+                                  size_t model_bytes, const void* cost_params,
+                                  size_t cost_bytes, float* u_out, float* diag3, char* err,
+                                  size_t err_len);
+
+/* Closed loop, one agent (MetalBackend::dispatch_simulation, metal_backend.hpp:72-83
+ * / metal_backend.mm:747-929).  History rows are the local steps 0..T-1. */
+int mppi_backend_dispatch_simulation(mppi_backend* b, uint32_t num_steps,
+                                     uint64_t start_step_index, const float* x0,
+                                     const float* u_nominal, const void* model_params,
+                                     size_t model_bytes, const void* cost_params,
+                                     size_t cost_bytes, float* states_out,
+                                     float* controls_out, float* costs_out, char* err,
+                                     size_t err_len);
+
+/* Closed loop, N agents (MetalBackend::dispatch_batch_simulation,
+ * metal_backend.hpp:88-100 / metal_backend.mm:935-1124).  u_nominal_packed
+ * NULL = zeros.  agents NULL = shared params / sigma.  Outputs may be NULL. */
+int mppi_backend_dispatch_batch_simulation(mppi_backend* b, uint32_t num_agents,
+                                           uint32_t num_steps, uint64_t start_step_index,
+                                           const float* x0_packed,
+                                           const float* u_nominal_packed,
+                                           const mppi_batch_agents* agents, float* states_out,
+                                           float* controls_out, float* costs_out,
+                                           float* terminal_states_out, char* err,
+                                           size_t err_len);
+
+/* Releases per-shape device buffers and cached graphs (MetalBackend::reset,
+ * metal_backend.hpp:103). */
+int mppi_backend_reset(mppi_backend* b, char* err, size_t err_len);
+
+/* ---- device-resident batch (split form of dispatch_batch_simulation) ------
+ * prepare: upload N agents' states / nominals / per-agent inputs;
+ * run:     num_steps closed-loop steps on the resident data (no host copies;
+ *          captured once into a CUDA graph per shape and replayed);
+ * fetch:   download the histories of the last run.
+ * dispatch_batch_simulation == prepare + run + fetch. */
+int mppi_backend_batch_prepare(mppi_backend* b, uint32_t num_agents, uint32_t num_steps,
+                               const float* x0_packed, const float* u_nominal_packed,
+                               const mppi_batch_agents* agents, uint32_t want_states,
+                               uint32_t want_controls, uint32_t want_costs,
+                               uint32_t want_terminal, char* err, size_t err_len);
+int mppi_backend_batch_run(mppi_backend* b, uint64_t start_step_index, char* err,
+                           size_t err_len);
+int mppi_backend_batch_fetch(mppi_backend* b, float* states_out, float* controls_out,
+                             float* costs_out, float* terminal_states_out, float* x_out,
+                             float* u_nominal_out, char* err, size_t err_len);
+
+/* ---- inspection (parity tests; no reference counterpart) ------------------ */
+/* Per-sample costs of the last pass for agents [a0, a0 + n): [n][K]. */
+int mppi_backend_last_costs(mppi_backend* b, uint32_t a0, uint32_t n, float* out, char* err,
+                            size_t err_len);
+/* Normalised weights of the last pass for agents [a0, a0 + n): [n][K]. */
+int mppi_backend_last_weights(mppi_backend* b, uint32_t a0, uint32_t n, float* out,
+                              char* err, size_t err_len);
+/* Standard normals and shaped noise of samples [k0, k0 + count) of one agent
+ * at one step, with the rollout's own sampling code: [count][H][m] each
+ * (either may be NULL).  sigma NULL = the configured sigma. */
+int mppi_backend_sample_noise(mppi_backend* b, uint64_t step_index, uint32_t agent,
+                              uint32_t k0, uint32_t count, const float* sigma,
+                              float* normals_out, float* eps_out, char* err, size_t err_len);
+/* Mean device time (ms) of the rollout and combine kernels of the prepared
+ * batch shape over `iters` back-to-back launches, timed with CUDA events on
+ * the backend's stream. */
+int mppi_backend_time_passes(mppi_backend* b, uint32_t iters, float* rollout_ms,
+                             float* combine_ms, char* err, size_t err_len);
+/* Launch geometry chosen for the prepared batch shape. */
+int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
+                             uint32_t* stage_rows, uint32_t* smem_bytes,
+                             uint32_t* kernels_per_step);
+
+/* Philox-2x32-10 words computed on the device (known-answer tests). */
+int mppi_device_philox(uint64_t n, const uint32_t* ctr0, const uint32_t* ctr1,
+                       const uint32_t* key, uint32_t* out_pairs, char* err, size_t err_len);
+
+/* Compiles a plugin with the library kernels for sm_100a without loading
+ * the result (needs no GPU).  log receives the NVRTC log, including ptxas's
+ * register / shared-memory / spill report for every kernel. */
+int mppi_compile_check(const mppi_backend_plugin* plugin, const mppi_backend_config* config,
+                       char* log, size_t log_len, char* err, size_t err_len);
+
+/* Library version string. */
+const char* mppi_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPPI_B200_BACKEND_H */

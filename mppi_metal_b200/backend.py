@@ -1,0 +1,246 @@
+"""numpy wrapper over the backend C ABI (include/mppi_b200/mppi_backend.h).
+
+The layer under ``MPPIDriver``: one compiled module + device state per
+instance.  Tests use it for the per-pass parity checks (costs, weights,
+noise) and the benchmark for the device-resident closed loop.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+
+
+class BackendError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+        self.msg = msg
+
+
+def _f32(a) -> Optional[np.ndarray]:
+    if a is None:
+        return None
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _check(rc: int, eb) -> None:
+    if rc != _lib.MPPI_OK:
+        raise BackendError(rc, eb.value.decode(errors="replace"))
+
+
+def _blob(b: Optional[bytes]):
+    if not b:
+        return None, 0
+    buf = ctypes.create_string_buffer(bytes(b), len(b))
+    return ctypes.cast(buf, ctypes.c_void_p), len(b), buf
+
+
+class Backend:
+    """One MPPI problem on the GPU: plugin + config + device buffers."""
+
+    def __init__(self, plugin: str, state_dim: int, control_dim: int, horizon: int,
+                 sample_count: int, lam: float, sigma, u_min, u_max, sigma_inv=None,
+                 cov_full: bool = False, control_cost: bool = False,
+                 stage_cost: str = "mppi_stage_cost", terminal_cost: str = "mppi_terminal_cost",
+                 dynamics: str = "mppi_dynamics", model_params_size: int = 0,
+                 cost_params_size: int = 0, seed: int = 0):
+        self.lib = _lib.load()
+        h = ctypes.c_void_p()
+        if self.lib.mppi_backend_create(ctypes.byref(h)) != _lib.MPPI_OK:
+            raise MemoryError("mppi_backend_create failed")
+        self.h = h
+        self.n, self.m, self.H, self.K = state_dim, control_dim, horizon, sample_count
+        self.lam = lam
+        self.seed = seed
+        sig = _f32(sigma)
+        sinv = _f32(sigma_inv if sigma_inv is not None else np.zeros_like(sig))
+        lo, hi = _f32(u_min), _f32(u_max)
+        cfg = _lib.BackendConfig(state_dim, control_dim, horizon, sample_count, lam,
+                                 1 if cov_full else 0, _p(sig), _p(sinv), _p(lo), _p(hi), 0,
+                                 1 if control_cost else 0)
+        path = plugin if plugin.endswith(".cu") or "/" in plugin else _lib.plugin_path(plugin)
+        plug = _lib.BackendPlugin(path.encode(), dynamics.encode(), stage_cost.encode(),
+                                  terminal_cost.encode(), model_params_size, cost_params_size,
+                                  seed & 0xFFFFFFFFFFFFFFFF)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_initialize(self.h, ctypes.byref(plug), ctypes.byref(cfg),
+                                                eb, len(eb)), eb)
+        self.N = 0
+        self.T = 0
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.mppi_backend_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    # -- MetalBackend-shaped calls ----------------------------------------------
+    def bind_params(self, model_params: Optional[bytes], cost_params: Optional[bytes]) -> None:
+        mp = _blob(model_params)
+        cp = _blob(cost_params)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_bind_params(self.h, mp[0], mp[1], cp[0], cp[1], eb, len(eb)),
+               eb)
+
+    def dispatch_rollout(self, step: int, x0, u_nom, model_override: Optional[bytes] = None,
+                         cost_override: Optional[bytes] = None):
+        x0, u_nom = _f32(x0), _f32(u_nom)
+        mo, co = _blob(model_override), _blob(cost_override)
+        u_out = np.zeros(self.H * self.m, np.float32)
+        diag = np.zeros(3, np.float32)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_dispatch_rollout(self.h, step, _p(x0), _p(u_nom), mo[0],
+                                                      mo[1], co[0], co[1], _p(u_out), _p(diag),
+                                                      eb, len(eb)), eb)
+        self.N, self.T = 1, 0
+        return u_out, diag
+
+    def simulate(self, T: int, start_step: int, x0, u_nom):
+        x0, u_nom = _f32(x0), _f32(u_nom)
+        st = np.zeros((T, self.n), np.float32)
+        ct = np.zeros((T, self.m), np.float32)
+        co = np.zeros(T, np.float32)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_dispatch_simulation(self.h, T, start_step, _p(x0), _p(u_nom),
+                                                         None, 0, None, 0, _p(st), _p(ct), _p(co),
+                                                         eb, len(eb)), eb)
+        self.N, self.T = 1, T
+        return dict(states=st, controls=ct, costs=co)
+
+    def _agents(self, cost_params=None, cost_stride=0, model_params=None, model_stride=0,
+                sigma=None):
+        if cost_params is None and model_params is None and sigma is None:
+            return None, []
+        mp = _blob(model_params)
+        cp = _blob(cost_params)
+        sg = _f32(sigma)
+        ag = _lib.BatchAgents(mp[0], model_stride, cp[0], cost_stride, _p(sg))
+        return ag, [mp, cp, sg]
+
+    def prepare(self, N: int, T: int, x0_packed, u_nom_packed=None, cost_params=None,
+                cost_stride: int = 0, model_params=None, model_stride: int = 0, sigma=None,
+                want_states=True, want_controls=True, want_costs=True, want_terminal=True):
+        x0 = _f32(x0_packed)
+        un = _f32(u_nom_packed)
+        ag, keep = self._agents(cost_params, cost_stride, model_params, model_stride, sigma)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_batch_prepare(
+            self.h, N, T, _p(x0), _p(un), ctypes.byref(ag) if ag is not None else None,
+            int(want_states), int(want_controls), int(want_costs), int(want_terminal), eb,
+            len(eb)), eb)
+        self.N, self.T = N, T
+        self._flags = (want_states, want_controls, want_costs, want_terminal)
+
+    def run(self, start_step: int = 0) -> None:
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_batch_run(self.h, start_step, eb, len(eb)), eb)
+
+    def fetch(self):
+        N, T = self.N, self.T
+        ws, wc, wk, wt = self._flags
+        st = np.zeros((T, N, self.n), np.float32) if ws else None
+        ct = np.zeros((T, N, self.m), np.float32) if wc else None
+        co = np.zeros((T, N), np.float32) if wk else None
+        te = np.zeros((N, self.n), np.float32) if wt else None
+        x = np.zeros((N, self.n), np.float32)
+        un = np.zeros((N, self.H * self.m), np.float32)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_batch_fetch(self.h, _p(st), _p(ct), _p(co), _p(te), _p(x),
+                                                 _p(un), eb, len(eb)), eb)
+        return dict(states=st, controls=ct, costs=co, terminal=te, x=x, u_nom=un)
+
+    def simulate_batch(self, N: int, T: int, start_step: int, x0_packed, u_nom_packed=None,
+                       cost_params=None, cost_stride: int = 0, model_params=None,
+                       model_stride: int = 0, sigma=None):
+        x0 = _f32(x0_packed)
+        un = _f32(u_nom_packed)
+        ag, keep = self._agents(cost_params, cost_stride, model_params, model_stride, sigma)
+        st = np.zeros((T, N, self.n), np.float32)
+        ct = np.zeros((T, N, self.m), np.float32)
+        co = np.zeros((T, N), np.float32)
+        te = np.zeros((N, self.n), np.float32)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_dispatch_batch_simulation(
+            self.h, N, T, start_step, _p(x0), _p(un),
+            ctypes.byref(ag) if ag is not None else None, _p(st), _p(ct), _p(co), _p(te), eb,
+            len(eb)), eb)
+        self.N, self.T = N, T
+        return dict(states=st, controls=ct, costs=co, terminal=te)
+
+    # -- inspection ------------------------------------------------------------
+    def last_costs(self, a0: int = 0, n: Optional[int] = None) -> np.ndarray:
+        n = self.N - a0 if n is None else n
+        out = np.zeros((n, self.K), np.float32)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_last_costs(self.h, a0, n, _p(out), eb, len(eb)), eb)
+        return out
+
+    def last_weights(self, a0: int = 0, n: Optional[int] = None) -> np.ndarray:
+        n = self.N - a0 if n is None else n
+        out = np.zeros((n, self.K), np.float32)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_last_weights(self.h, a0, n, _p(out), eb, len(eb)), eb)
+        return out
+
+    def sample_noise(self, step: int, agent: int, k0: int, count: int, sigma=None):
+        sg = _f32(sigma)
+        nrm = np.zeros((count, self.H, self.m), np.float32)
+        eps = np.zeros((count, self.H, self.m), np.float32)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_sample_noise(self.h, step, agent, k0, count, _p(sg), _p(nrm),
+                                                  _p(eps), eb, len(eb)), eb)
+        return nrm, eps
+
+    def time_passes(self, iters: int = 20):
+        r = ctypes.c_float()
+        c = ctypes.c_float()
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_time_passes(self.h, iters, ctypes.byref(r), ctypes.byref(c),
+                                                 eb, len(eb)), eb)
+        return r.value, c.value
+
+    def launch_info(self) -> dict:
+        vals = [ctypes.c_uint32() for _ in range(5)]
+        self.lib.mppi_backend_launch_info(self.h, *[ctypes.byref(v) for v in vals])
+        keys = ["block", "nblk", "stage_rows", "smem_bytes", "kernels_per_step"]
+        return {k: v.value for k, v in zip(keys, vals)}
+
+
+def device_philox(c0, c1, key) -> np.ndarray:
+    """Philox-2x32-10 words computed by the library's device kernel."""
+    lib = _lib.load()
+    c0 = np.ascontiguousarray(c0, dtype=np.uint32)
+    c1 = np.ascontiguousarray(c1, dtype=np.uint32)
+    key = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros((c0.size, 2), np.uint32)
+    eb = _lib.err_buf()
+    _check(lib.mppi_device_philox(c0.size, _p(c0), _p(c1), _p(key), _p(out), eb, len(eb)), eb)
+    return out
+
+
+def compile_check(plugin: str, state_dim: int, control_dim: int, cov_full: bool = False,
+                  control_cost: bool = False, stage_cost: str = "mppi_stage_cost",
+                  terminal_cost: str = "mppi_terminal_cost", dynamics: str = "mppi_dynamics",
+                  model_params_size: int = 0, cost_params_size: int = 0):
+    """NVRTC-compile a plugin with the library kernels for sm_100a (no GPU).
+    Returns (status, error, log)."""
+    lib = _lib.load()
+    path = plugin if plugin.endswith(".cu") or "/" in plugin else _lib.plugin_path(plugin)
+    plug = _lib.BackendPlugin(path.encode(), dynamics.encode(), stage_cost.encode(),
+                              terminal_cost.encode(), model_params_size, cost_params_size, 0)
+    cfg = _lib.BackendConfig(state_dim, control_dim, 8, 64, 1.0, 1 if cov_full else 0, None, None,
+                             None, None, 0, 1 if control_cost else 0)
+    log = ctypes.create_string_buffer(1 << 18)
+    eb = _lib.err_buf(1 << 16)
+    rc = lib.mppi_compile_check(ctypes.byref(plug), ctypes.byref(cfg), log, len(log), eb, len(eb))
+    return rc, eb.value.decode(errors="replace"), log.value.decode(errors="replace")

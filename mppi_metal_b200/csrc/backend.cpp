@@ -1,0 +1,1005 @@
+// backend.cpp — the CUDA backend behind include/mppi_b200/mppi_backend.h.
+//
+// Host side of the hot path: owns the per-driver kernel module (NVRTC), the
+// CUDA stream, device buffers and pinned staging buffers, chooses the launch
+// geometry, and issues rollout + combine launches (captured into a CUDA graph
+// for closed loops).  Replaces the reference's MetalBackend
+// (src/metal_backend.mm): there, one command buffer per call encodes four
+// passes per step with buffer barriers and waits for completion; here each
+// control step is two kernels, a T-step closed loop is one graph launch, and
+// the host waits once per call.
+//
+// Device data layout for a batch of N agents (all FP32, agent-major):
+//   io:       [step_base u32 x4][x N*n][u_nom N*H*m][u_out N*H*m][diag N*3][stats N*4]
+//             (step_base..u_nom is one upload, u_out..diag one download)
+//   costs     [N][K]            per-sample costs of the last pass
+//   partials  [N][nblk][ps]     per-CTA softmax / weighted-noise partials
+//   history   [T][N][n], [T][N][m], [T][N]; terminal [N][n]
+//   per-agent blobs [N][pad16(size)], per-agent sigma [N][m or m*m]
+#include "../../include/mppi_b200/mppi_backend.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "device/mppi_launch.h"
+#include "nvrtc_module.hpp"
+
+namespace {
+
+using mppi_b200::KernelModule;
+
+void set_err(char* err, size_t len, const std::string& msg) {
+  if (err != nullptr && len > 0) {
+    const size_t n = std::min(len - 1, msg.size());
+    memcpy(err, msg.data(), n);
+    err[n] = '\0';
+  }
+}
+
+size_t pad4(size_t n) { return (n + 3) & ~size_t(3); }
+size_t pad16(size_t n) { return (n + 15) & ~size_t(15); }
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  // Returns true when the buffer was (re)allocated.
+  cudaError_t ensure(size_t n, bool* grew = nullptr) {
+    if (n == 0) n = 16;
+    if (p && n <= bytes) return cudaSuccess;
+    release();
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e == cudaSuccess) bytes = n;
+    if (grew) *grew = true;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  PinnedBuf() = default;
+  PinnedBuf(const PinnedBuf&) = delete;
+  PinnedBuf& operator=(const PinnedBuf&) = delete;
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  cudaError_t ensure(size_t n) {
+    if (n == 0) n = 16;
+    if (p && n <= bytes) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMallocHost(&p, n);
+    if (e == cudaSuccess) bytes = n;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// Cholesky factor of a row-major SPD matrix (lower triangle), in double.
+bool cholesky(uint32_t m, const float* a, std::vector<float>* l) {
+  std::vector<double> L((size_t)m * m, 0.0);
+  for (uint32_t i = 0; i < m; ++i) {
+    for (uint32_t j = 0; j <= i; ++j) {
+      double s = a[i * m + j];
+      for (uint32_t k = 0; k < j; ++k) s -= L[i * m + k] * L[j * m + k];
+      if (i == j) {
+        if (!(s > 0.0)) return false;
+        L[i * m + i] = std::sqrt(s);
+      } else {
+        L[i * m + j] = s / L[j * m + j];
+      }
+    }
+  }
+  l->assign(L.begin(), L.end());
+  return true;
+}
+
+struct LaunchGeom {
+  int variant = 1;  // index into kRolloutBlocks
+  uint32_t block = 128;
+  uint32_t nblk = 0;
+  uint32_t stage_rows = 0;
+  uint32_t pstride = 0;
+  size_t smem = 0;
+};
+
+}  // namespace
+
+struct mppi_backend {
+  // ---- configuration (fixed at initialize) ----
+  bool initialized = false;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  uint32_t n = 0, m = 0, H = 0, K = 0;
+  float lambda = 1.0f;
+  bool cov_full = false;
+  bool control_cost = false;
+  uint32_t seed = 0;
+  uint64_t mp_size = 0, cp_size = 0;
+  std::vector<float> sigma_dev;  // std-devs (diag) or Cholesky factor (full)
+  std::vector<float> sigma_inv;
+  std::vector<float> u_min, u_max;
+  std::shared_ptr<const KernelModule> mod;
+  int num_sms = 148;
+  size_t max_smem_optin = 0;
+
+  // ---- constant device data ----
+  DevBuf d_consts;  // [sigma m*m][sigma_inv m*m][u_min m][u_max m] padded
+  DevBuf d_mp_bound, d_cp_bound, d_mp_ovr, d_cp_ovr, d_zero;
+  bool mp_bound = false, cp_bound = false;
+
+  // ---- per-shape state ----
+  uint32_t N = 0, T = 0;
+  LaunchGeom geom;
+  DevBuf d_io, d_costs, d_partials;
+  DevBuf d_hs, d_hc, d_hk, d_term;
+  DevBuf d_agent_sigma, d_agent_mp, d_agent_cp;
+  bool want_s = false, want_c = false, want_k = false, want_t = false;
+  // parameter pointers of the prepared run
+  const uint8_t* run_mp = nullptr;
+  const uint8_t* run_cp = nullptr;
+  uint64_t run_mp_stride = 0, run_cp_stride = 0;
+  const float* run_sigma = nullptr;
+  uint32_t run_sigma_stride = 0;
+  uint64_t generation = 0;  // bumps whenever a device buffer is reallocated
+
+  PinnedBuf h_up, h_down;
+
+  // ---- closed-loop graph cache ----
+  cudaGraphExec_t graph = nullptr;
+  std::string graph_key;
+
+  ~mppi_backend() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  size_t sig_len() const { return cov_full ? (size_t)m * m : m; }
+  size_t HM() const { return (size_t)H * m; }
+
+  // io buffer offsets (floats)
+  size_t off_x() const { return 4; }
+  size_t off_unom() const { return off_x() + pad4((size_t)N * n); }
+  size_t off_uout() const { return off_unom() + pad4((size_t)N * HM()); }
+  size_t off_diag() const { return off_uout() + pad4((size_t)N * HM()); }
+  size_t off_stats() const { return off_diag() + pad4((size_t)N * 3); }
+  size_t io_floats() const { return off_stats() + pad4((size_t)N * 4); }
+
+  float* io() const { return d_io.as<float>(); }
+  const float* c_sigma() const { return d_consts.as<float>(); }
+  const float* c_sigma_inv() const { return d_consts.as<float>() + pad4((size_t)m * m); }
+  const float* c_umin() const { return d_consts.as<float>() + 2 * pad4((size_t)m * m); }
+  const float* c_umax() const { return c_umin() + pad4(m); }
+};
+
+namespace {
+
+#define CK(call)                                                                      \
+  do {                                                                                \
+    cudaError_t _e = (call);                                                          \
+    if (_e != cudaSuccess) {                                                          \
+      set_err(err, err_len, std::string("CUDA error: ") + cudaGetErrorString(_e) +     \
+                                " (" #call ")");                                     \
+      return (_e == cudaErrorNoDevice || _e == cudaErrorInsufficientDriver)           \
+                 ? MPPI_ERR_NO_DEVICE                                                 \
+                 : MPPI_ERR_CUDA;                                                     \
+    }                                                                                 \
+  } while (0)
+
+bool valid_identifier(const char* s) {
+  if (!s || !*s) return false;
+  for (const char* c = s; *c; ++c) {
+    const bool ok = (*c == '_') || (*c >= 'a' && *c <= 'z') || (*c >= 'A' && *c <= 'Z') ||
+                    (c != s && *c >= '0' && *c <= '9');
+    if (!ok) return false;
+  }
+  return true;
+}
+
+// Launch geometry for N agents (fixed K, H): block size and how the noise
+// is kept for the weighted sums.  Staging the whole horizon during the
+// rollout avoids regenerating it; it needs H*m*block*4 bytes per CTA, so it
+// is used while that keeps >= 2 CTAs per SM, otherwise the noise is
+// regenerated in chunks after the costs are known.
+LaunchGeom choose_geometry(const mppi_backend* b) {
+  LaunchGeom g;
+  const size_t HM = b->HM();
+  const size_t budget = std::min<size_t>(b->max_smem_optin ? b->max_smem_optin : 232448, 232448);
+  // Prefer 128 threads; fall back to 64 for very long horizons.
+  const int order[2] = {1, 0};
+  for (int vi : order) {
+    const uint32_t block = mppi_b200::kRolloutBlocks[vi];
+    const size_t fixed = pad4(HM) * 4 + (size_t)block * 4;
+    const size_t full = fixed + HM * block * 4;
+    g.variant = vi;
+    g.block = block;
+    if (full <= budget / 2 - 4096) {
+      g.stage_rows = (uint32_t)HM;
+      g.smem = full;
+      break;
+    }
+    // chunked regeneration: ~32 KB of staging, whole time steps per chunk
+    uint32_t rows = (uint32_t)(32768 / ((size_t)block * 4));
+    rows = std::max<uint32_t>(b->m, rows / b->m * b->m);
+    rows = std::min<uint32_t>(rows, (uint32_t)HM);
+    g.stage_rows = rows;
+    g.smem = fixed + (size_t)rows * block * 4;
+    if (vi == 1) break;
+  }
+  g.nblk = (b->K + g.block - 1) / g.block;
+  g.pstride = (uint32_t)pad4(MPPI_PARTIAL_HEAD + HM);
+  return g;
+}
+
+int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool wk, bool wt,
+                 char* err, size_t err_len) {
+  bool grew = false;
+  CK(cudaStreamSynchronize(b->stream));  // buffers below may be in use
+  b->N = N;
+  b->T = T;
+  b->geom = choose_geometry(b);
+  CK(b->d_io.ensure(b->io_floats() * 4, &grew));
+  CK(b->d_costs.ensure((size_t)N * b->K * 4, &grew));
+  CK(b->d_partials.ensure((size_t)N * b->geom.nblk * b->geom.pstride * 4, &grew));
+  b->want_s = ws;
+  b->want_c = wc;
+  b->want_k = wk;
+  b->want_t = wt;
+  if (ws) CK(b->d_hs.ensure((size_t)T * N * b->n * 4, &grew));
+  if (wc) CK(b->d_hc.ensure((size_t)T * N * b->m * 4, &grew));
+  if (wk) CK(b->d_hk.ensure((size_t)T * N * 4, &grew));
+  if (wt) CK(b->d_term.ensure((size_t)N * b->n * 4, &grew));
+  CK(b->h_up.ensure((b->off_uout() + 64) * 4 + 2 * pad16(b->mp_size + b->cp_size) + 64));
+  CK(b->h_down.ensure((b->io_floats() + 64) * 4));
+  if (grew) ++b->generation;
+  const void* k = (const void*)b->mod->rollout[b->geom.variant];
+  if (b->geom.smem > 48 * 1024)
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem));
+  return MPPI_OK;
+}
+
+MppiRolloutArgs rollout_args(const mppi_backend* b, uint32_t step_local) {
+  MppiRolloutArgs a{};
+  a.num_agents = b->N;
+  a.K = b->K;
+  a.H = b->H;
+  a.nblk = b->geom.nblk;
+  a.stage_rows = b->geom.stage_rows;
+  a.seed = b->seed;
+  a.step_local = step_local;
+  a.pstride = b->geom.pstride;
+  a.lambda = b->lambda;
+  a.sigma_stride = b->run_sigma_stride;
+  a.sigma_inv_stride = 0;
+  a.step_base = reinterpret_cast<const uint32_t*>(b->io());
+  a.x = b->io() + b->off_x();
+  a.u_nom = b->io() + b->off_unom();
+  a.sigma = b->run_sigma;
+  a.sigma_inv = b->c_sigma_inv();
+  a.u_min = b->c_umin();
+  a.u_max = b->c_umax();
+  a.model_params = b->run_mp;
+  a.cost_params = b->run_cp;
+  a.model_stride = b->run_mp_stride;
+  a.cost_stride = b->run_cp_stride;
+  a.costs = b->d_costs.as<float>();
+  a.partials = b->d_partials.as<float>();
+  return a;
+}
+
+MppiCombineArgs combine_args(const mppi_backend* b, uint32_t step_local, bool propagate) {
+  MppiCombineArgs c{};
+  c.num_agents = b->N;
+  c.K = b->K;
+  c.H = b->H;
+  c.nblk = b->geom.nblk;
+  c.pstride = b->geom.pstride;
+  c.step_local = step_local;
+  c.lambda = b->lambda;
+  c.propagate = propagate ? 1u : 0u;
+  c.step_base = reinterpret_cast<const uint32_t*>(b->io());
+  c.partials = b->d_partials.as<float>();
+  c.u_min = b->c_umin();
+  c.u_max = b->c_umax();
+  c.model_params = b->run_mp;
+  c.model_stride = b->run_mp_stride;
+  c.u_nom = b->io() + b->off_unom();
+  c.u_out = b->io() + b->off_uout();
+  c.diag = b->io() + b->off_diag();
+  c.stats = b->io() + b->off_stats();
+  c.x = b->io() + b->off_x();
+  c.hist_states = b->want_s ? b->d_hs.as<float>() : nullptr;
+  c.hist_controls = b->want_c ? b->d_hc.as<float>() : nullptr;
+  c.hist_costs = b->want_k ? b->d_hk.as<float>() : nullptr;
+  c.terminal = b->want_t ? b->d_term.as<float>() : nullptr;
+  return c;
+}
+
+size_t combine_smem(const mppi_backend* b) {
+  return (pad4(b->geom.nblk) + pad4(b->HM())) * 4;
+}
+
+cudaError_t launch_rollout(mppi_backend* b, uint32_t step_local) {
+  MppiRolloutArgs a = rollout_args(b, step_local);
+  void* args[] = {&a};
+  return cudaLaunchKernel((const void*)b->mod->rollout[b->geom.variant],
+                          dim3(b->geom.nblk, b->N), dim3(b->geom.block), args, b->geom.smem,
+                          b->stream);
+}
+
+cudaError_t launch_combine(mppi_backend* b, uint32_t step_local, bool propagate) {
+  MppiCombineArgs c = combine_args(b, step_local, propagate);
+  void* args[] = {&c};
+  return cudaLaunchKernel((const void*)b->mod->combine, dim3(b->N), dim3(256), args,
+                          combine_smem(b), b->stream);
+}
+
+// Resolves the parameter blob pointers of a run: per-agent blobs, an
+// override, the bound blob, or a zero word (the reference binds a 1-byte zero
+// buffer when nothing is bound, metal_backend.mm:595-600).
+const uint8_t* pick_params(mppi_backend* b, bool is_model, const void* ovr, size_t ovr_bytes) {
+  DevBuf& bound = is_model ? b->d_mp_bound : b->d_cp_bound;
+  DevBuf& obuf = is_model ? b->d_mp_ovr : b->d_cp_ovr;
+  const bool has_bound = is_model ? b->mp_bound : b->cp_bound;
+  if (ovr != nullptr && ovr_bytes > 0) return obuf.as<uint8_t>();
+  if (has_bound) return bound.as<uint8_t>();
+  return b->d_zero.as<uint8_t>();
+}
+
+int check_init(mppi_backend* b, char* err, size_t err_len) {
+  if (b == nullptr) {
+    set_err(err, err_len, "backend handle is null.");
+    return MPPI_ERR_INVALID;
+  }
+  if (!b->initialized) {
+    set_err(err, err_len, "MPPI backend is not initialized.");
+    return MPPI_ERR_NOT_INIT;
+  }
+  cudaError_t e = cudaSetDevice(b->device);
+  if (e != cudaSuccess) {
+    set_err(err, err_len, std::string("cudaSetDevice failed: ") + cudaGetErrorString(e));
+    return MPPI_ERR_CUDA;
+  }
+  return MPPI_OK;
+}
+
+// Uploads [step_base][x][u_nom] (and blob overrides) with one pinned copy each.
+int upload_state(mppi_backend* b, uint64_t start_step, const float* x, const float* u_nom,
+                 const void* mp_ovr, size_t mp_bytes, const void* cp_ovr, size_t cp_bytes,
+                 char* err, size_t err_len) {
+  // the pinned staging buffer may still feed an earlier asynchronous copy
+  CK(cudaStreamSynchronize(b->stream));
+  float* up = b->h_up.as<float>();
+  const size_t nx = (size_t)b->N * b->n, nu = (size_t)b->N * b->HM();
+  uint32_t sb = (uint32_t)start_step;
+  memcpy(up, &sb, 4);
+  memcpy(up + b->off_x(), x, nx * 4);
+  if (u_nom)
+    memcpy(up + b->off_unom(), u_nom, nu * 4);
+  else
+    memset(up + b->off_unom(), 0, nu * 4);
+  CK(cudaMemcpyAsync(b->io(), up, b->off_uout() * 4, cudaMemcpyHostToDevice, b->stream));
+  uint8_t* tail = reinterpret_cast<uint8_t*>(up + b->off_uout());
+  if (mp_ovr && mp_bytes) {
+    CK(b->d_mp_ovr.ensure(pad16(b->mp_size)));
+    memset(tail, 0, pad16(b->mp_size));
+    memcpy(tail, mp_ovr, mp_bytes);
+    CK(cudaMemcpyAsync(b->d_mp_ovr.p, tail, pad16(b->mp_size), cudaMemcpyHostToDevice,
+                       b->stream));
+    tail += pad16(b->mp_size);
+  }
+  if (cp_ovr && cp_bytes) {
+    CK(b->d_cp_ovr.ensure(pad16(b->cp_size)));
+    memset(tail, 0, pad16(b->cp_size));
+    memcpy(tail, cp_ovr, cp_bytes);
+    CK(cudaMemcpyAsync(b->d_cp_ovr.p, tail, pad16(b->cp_size), cudaMemcpyHostToDevice,
+                       b->stream));
+  }
+  return MPPI_OK;
+}
+
+int check_override_sizes(mppi_backend* b, size_t mp_bytes, const void* mp, size_t cp_bytes,
+                         const void* cp, char* err, size_t err_len) {
+  if (mp && mp_bytes > 0 && mp_bytes != b->mp_size) {
+    set_err(err, err_len,
+            "model_params_override.bytes (" + std::to_string(mp_bytes) +
+                ") does not match ParamLayout::model_params_size (" +
+                std::to_string(b->mp_size) + ").");
+    return MPPI_ERR_INVALID;
+  }
+  if (cp && cp_bytes > 0 && cp_bytes != b->cp_size) {
+    set_err(err, err_len,
+            "cost_params_override.bytes (" + std::to_string(cp_bytes) +
+                ") does not match ParamLayout::cost_params_size (" +
+                std::to_string(b->cp_size) + ").");
+    return MPPI_ERR_INVALID;
+  }
+  return MPPI_OK;
+}
+
+// Enqueues T closed-loop steps (rollout + combine/propagate each), through a
+// CUDA graph captured once per (shape, buffers) and replayed afterwards.
+int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
+  char keybuf[256];
+  snprintf(keybuf, sizeof(keybuf), "%u/%u/%llu/%d/%d%d%d%d/%p/%p/%llu/%llu/%p/%u",
+           b->N, b->T, (unsigned long long)b->generation, b->geom.variant, b->want_s, b->want_c,
+           b->want_k, b->want_t, (const void*)b->run_mp, (const void*)b->run_cp,
+           (unsigned long long)b->run_mp_stride, (unsigned long long)b->run_cp_stride,
+           (const void*)b->run_sigma, b->run_sigma_stride);
+  const std::string key = keybuf;
+  if (b->graph == nullptr || b->graph_key != key) {
+    if (b->graph) {
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t le = cudaSuccess;
+    for (uint32_t s = 0; s < b->T && le == cudaSuccess; ++s) {
+      le = launch_rollout(b, s);
+      if (le == cudaSuccess) le = launch_combine(b, s, true);
+    }
+    cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+    if (le != cudaSuccess || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      set_err(err, err_len, std::string("graph capture failed: ") +
+                                cudaGetErrorString(le != cudaSuccess ? le : ce));
+      return MPPI_ERR_CUDA;
+    }
+    cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(ie);
+    b->graph_key = key;
+  }
+  CK(cudaGraphLaunch(b->graph, b->stream));
+  return MPPI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mppi_b200_version(void) { return "mppi_metal_b200 0.1.0 (sm_100a)"; }
+
+int mppi_backend_create(mppi_backend** out) {
+  if (!out) return MPPI_ERR_INVALID;
+  *out = new (std::nothrow) mppi_backend();
+  return *out ? MPPI_OK : MPPI_ERR_INVALID;
+}
+
+void mppi_backend_destroy(mppi_backend* b) {
+  if (!b) return;
+  if (b->initialized) cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  delete b;
+}
+
+int mppi_backend_initialize(mppi_backend* b, const mppi_backend_plugin* plugin,
+                            const mppi_backend_config* cfg, char* err, size_t err_len) {
+  if (!b || !plugin || !cfg) {
+    set_err(err, err_len, "null argument to mppi_backend_initialize.");
+    return MPPI_ERR_INVALID;
+  }
+  if (cfg->state_dim == 0 || cfg->control_dim == 0 || cfg->horizon == 0 ||
+      cfg->sample_count == 0) {
+    set_err(err, err_len, "state_dim, control_dim, horizon and sample_count must be > 0.");
+    return MPPI_ERR_INVALID;
+  }
+  if (cfg->state_dim * 4 > 128) {
+    set_err(err, err_len, "DriverConfig::state_dim (" + std::to_string(cfg->state_dim) +
+                              ") exceeds MPPI_MAX_STATE_BYTES / 4 = 32.");
+    return MPPI_ERR_INVALID;
+  }
+  if (cfg->control_dim > 16) {
+    set_err(err, err_len, "DriverConfig::control_dim (" + std::to_string(cfg->control_dim) +
+                              ") exceeds MPPI_MAX_CONTROL_DIM = 16.");
+    return MPPI_ERR_INVALID;
+  }
+  if (!cfg->sigma || !cfg->u_min || !cfg->u_max || (cfg->control_cost && !cfg->sigma_inv)) {
+    set_err(err, err_len, "sigma, sigma_inv, u_min and u_max must not be null.");
+    return MPPI_ERR_INVALID;
+  }
+  if (!plugin->source_path || !*plugin->source_path) {
+    set_err(err, err_len, "user_metallib_path is empty.");
+    return MPPI_ERR_PLUGIN;
+  }
+  if (!valid_identifier(plugin->dynamics)) {
+    set_err(err, err_len, std::string("Required callable '") +
+                              (plugin->dynamics ? plugin->dynamics : "") +
+                              "' is not a valid identifier.");
+    return MPPI_ERR_CALLABLE;
+  }
+  for (const char* nm : {plugin->stage_cost, plugin->terminal_cost}) {
+    if (nm && *nm && !valid_identifier(nm)) {
+      set_err(err, err_len, std::string("Callable '") + nm + "' is not a valid identifier.");
+      return MPPI_ERR_CALLABLE;
+    }
+  }
+
+  // ---- device (metal_backend.mm:227-231: the default device) ----
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_err(err, err_len, std::string("No CUDA device available: ") +
+                              (e != cudaSuccess ? cudaGetErrorString(e) : "device count is 0"));
+    return MPPI_ERR_NO_DEVICE;
+  }
+  CK(cudaGetDevice(&b->device));
+  cudaDeviceProp prop{};
+  CK(cudaGetDeviceProperties(&prop, b->device));
+  if (prop.major < 10) {
+    set_err(err, err_len, std::string("device '") + prop.name +
+                              "' is not sm_100 (Blackwell); this library is built for sm_100a.");
+    return MPPI_ERR_NO_DEVICE;
+  }
+  b->num_sms = prop.multiProcessorCount;
+  b->max_smem_optin = prop.sharedMemPerBlockOptin;
+
+  b->n = cfg->state_dim;
+  b->m = cfg->control_dim;
+  b->H = cfg->horizon;
+  b->K = cfg->sample_count;
+  b->lambda = cfg->lambda;
+  b->cov_full = cfg->covariance_form == 1;
+  b->control_cost = cfg->control_cost != 0;
+  b->seed = (uint32_t)plugin->seed;  // metal_backend.mm:565
+  b->mp_size = plugin->model_params_size;
+  b->cp_size = plugin->cost_params_size;
+  const uint32_t m = b->m;
+  if (b->cov_full) {
+    if (!cholesky(m, cfg->sigma, &b->sigma_dev)) {
+      set_err(err, err_len, "ControlNoiseConfig::sigma (kFull) is not symmetric positive definite.");
+      return MPPI_ERR_INVALID;
+    }
+  } else {
+    b->sigma_dev.assign(cfg->sigma, cfg->sigma + m);
+  }
+  const size_t sl = b->cov_full ? (size_t)m * m : m;
+  if (cfg->sigma_inv)
+    b->sigma_inv.assign(cfg->sigma_inv, cfg->sigma_inv + sl);
+  else
+    b->sigma_inv.assign(sl, 0.0f);
+  b->u_min.assign(cfg->u_min, cfg->u_min + m);
+  b->u_max.assign(cfg->u_max, cfg->u_max + m);
+
+  // ---- kernel module: plugin + library kernels (metal_backend.mm:278-560) ----
+  mppi_b200::ModuleSpec spec;
+  spec.plugin_path = plugin->source_path;
+  spec.dynamics = plugin->dynamics;
+  spec.stage_cost = plugin->stage_cost ? plugin->stage_cost : "";
+  spec.terminal_cost = plugin->terminal_cost ? plugin->terminal_cost : "";
+  spec.state_dim = b->n;
+  spec.control_dim = m;
+  spec.cov_full = b->cov_full;
+  spec.control_cost = b->control_cost;
+  spec.model_params_bytes = b->mp_size;
+  spec.cost_params_bytes = b->cp_size;
+  std::string merr;
+  const int rc = mppi_b200::load_module(spec, &b->mod, &merr);
+  if (rc != MPPI_OK) {
+    set_err(err, err_len, merr);
+    return rc;
+  }
+
+  if (!b->stream) CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  if (!b->ev0) CK(cudaEventCreate(&b->ev0));
+  if (!b->ev1) CK(cudaEventCreate(&b->ev1));
+
+  // constants: [sigma (m*m)][sigma_inv (m*m)][u_min][u_max]
+  const size_t mm = pad4((size_t)m * m);
+  std::vector<float> consts(2 * mm + 2 * pad4(m), 0.0f);
+  std::copy(b->sigma_dev.begin(), b->sigma_dev.end(), consts.begin());
+  std::copy(b->sigma_inv.begin(), b->sigma_inv.end(), consts.begin() + mm);
+  std::copy(b->u_min.begin(), b->u_min.end(), consts.begin() + 2 * mm);
+  std::copy(b->u_max.begin(), b->u_max.end(), consts.begin() + 2 * mm + pad4(m));
+  CK(b->d_consts.ensure(consts.size() * 4));
+  CK(cudaMemcpy(b->d_consts.p, consts.data(), consts.size() * 4, cudaMemcpyHostToDevice));
+  CK(b->d_zero.ensure(std::max<size_t>(256, pad16(std::max(b->mp_size, b->cp_size)))));
+  CK(cudaMemset(b->d_zero.p, 0, b->d_zero.bytes));
+  b->initialized = true;
+  return MPPI_OK;
+}
+
+int mppi_backend_bind_params(mppi_backend* b, const void* mp, size_t mp_bytes, const void* cp,
+                             size_t cp_bytes, char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  CK(cudaStreamSynchronize(b->stream));
+  if (mp && mp_bytes > 0) {
+    if (mp_bytes != b->mp_size) {
+      set_err(err, err_len, "model_params.bytes does not match ParamLayout::model_params_size.");
+      return MPPI_ERR_INVALID;
+    }
+    std::vector<uint8_t> tmp(pad16(mp_bytes), 0);
+    memcpy(tmp.data(), mp, mp_bytes);
+    CK(b->d_mp_bound.ensure(tmp.size()));
+    CK(cudaMemcpy(b->d_mp_bound.p, tmp.data(), tmp.size(), cudaMemcpyHostToDevice));
+    b->mp_bound = true;
+  } else {
+    b->mp_bound = false;
+  }
+  if (cp && cp_bytes > 0) {
+    if (cp_bytes != b->cp_size) {
+      set_err(err, err_len, "cost_params.bytes does not match ParamLayout::cost_params_size.");
+      return MPPI_ERR_INVALID;
+    }
+    std::vector<uint8_t> tmp(pad16(cp_bytes), 0);
+    memcpy(tmp.data(), cp, cp_bytes);
+    CK(b->d_cp_bound.ensure(tmp.size()));
+    CK(cudaMemcpy(b->d_cp_bound.p, tmp.data(), tmp.size(), cudaMemcpyHostToDevice));
+    b->cp_bound = true;
+  } else {
+    b->cp_bound = false;
+  }
+  return MPPI_OK;
+}
+
+int mppi_backend_dispatch_rollout(mppi_backend* b, uint64_t step_index, const float* x0,
+                                  const float* u_nominal, const void* mp, size_t mp_bytes,
+                                  const void* cp, size_t cp_bytes, float* u_out, float* diag3,
+                                  char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (!x0 || !u_nominal || !u_out) {
+    set_err(err, err_len, "x0, u_nominal and u_out must not be null.");
+    return MPPI_ERR_INVALID;
+  }
+  if (int rc = check_override_sizes(b, mp_bytes, mp, cp_bytes, cp, err, err_len)) return rc;
+  if (int rc = ensure_shape(b, 1, 0, false, false, false, false, err, err_len)) return rc;
+  b->run_mp = pick_params(b, true, mp, mp_bytes);
+  b->run_cp = pick_params(b, false, cp, cp_bytes);
+  b->run_mp_stride = b->run_cp_stride = 0;
+  b->run_sigma = b->c_sigma();
+  b->run_sigma_stride = 0;
+  if (int rc = upload_state(b, step_index, x0, u_nominal, mp, mp_bytes, cp, cp_bytes, err,
+                            err_len))
+    return rc;
+  CK(launch_rollout(b, 0));
+  CK(launch_combine(b, 0, false));
+  float* down = b->h_down.as<float>();
+  const size_t nd = b->off_stats() - b->off_uout();
+  CK(cudaMemcpyAsync(down, b->io() + b->off_uout(), nd * 4, cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  memcpy(u_out, down, b->HM() * 4);
+  if (diag3) memcpy(diag3, down + (b->off_diag() - b->off_uout()), 3 * 4);
+  return MPPI_OK;
+}
+
+int mppi_backend_batch_prepare(mppi_backend* b, uint32_t N, uint32_t T, const float* x0,
+                               const float* u_nom, const mppi_batch_agents* agents,
+                               uint32_t ws, uint32_t wc, uint32_t wk, uint32_t wt, char* err,
+                               size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (N == 0 || T == 0 || !x0) {
+    set_err(err, err_len, "num_agents and num_steps must be > 0 and x0 must not be null.");
+    return MPPI_ERR_INVALID;
+  }
+  if (int rc = ensure_shape(b, N, T, ws, wc, wk, wt, err, err_len)) return rc;
+  b->run_mp = pick_params(b, true, nullptr, 0);
+  b->run_cp = pick_params(b, false, nullptr, 0);
+  b->run_mp_stride = b->run_cp_stride = 0;
+  b->run_sigma = b->c_sigma();
+  b->run_sigma_stride = 0;
+  if (agents) {
+    bool grew = false;
+    if (agents->model_params && b->mp_size > 0) {
+      const size_t st = pad16(b->mp_size);
+      std::vector<uint8_t> tmp(st * N, 0);
+      for (uint32_t a = 0; a < N; ++a)
+        memcpy(tmp.data() + st * a,
+               static_cast<const uint8_t*>(agents->model_params) + agents->model_params_stride * a,
+               b->mp_size);
+      CK(b->d_agent_mp.ensure(tmp.size(), &grew));
+      CK(cudaMemcpy(b->d_agent_mp.p, tmp.data(), tmp.size(), cudaMemcpyHostToDevice));
+      b->run_mp = b->d_agent_mp.as<uint8_t>();
+      b->run_mp_stride = st;
+    }
+    if (agents->cost_params && b->cp_size > 0) {
+      const size_t st = pad16(b->cp_size);
+      std::vector<uint8_t> tmp(st * N, 0);
+      for (uint32_t a = 0; a < N; ++a)
+        memcpy(tmp.data() + st * a,
+               static_cast<const uint8_t*>(agents->cost_params) + agents->cost_params_stride * a,
+               b->cp_size);
+      CK(b->d_agent_cp.ensure(tmp.size(), &grew));
+      CK(cudaMemcpy(b->d_agent_cp.p, tmp.data(), tmp.size(), cudaMemcpyHostToDevice));
+      b->run_cp = b->d_agent_cp.as<uint8_t>();
+      b->run_cp_stride = st;
+    }
+    if (agents->sigma) {
+      const size_t sl = b->sig_len();
+      std::vector<float> tmp(sl * N);
+      for (uint32_t a = 0; a < N; ++a) {
+        const float* src = agents->sigma + sl * a;
+        if (b->cov_full) {
+          std::vector<float> L;
+          if (!cholesky(b->m, src, &L)) {
+            set_err(err, err_len, "per-agent sigma of agent " + std::to_string(a) +
+                                      " is not symmetric positive definite.");
+            return MPPI_ERR_INVALID;
+          }
+          std::copy(L.begin(), L.end(), tmp.begin() + sl * a);
+        } else {
+          std::copy(src, src + sl, tmp.begin() + sl * a);
+        }
+      }
+      CK(b->d_agent_sigma.ensure(tmp.size() * 4, &grew));
+      CK(cudaMemcpy(b->d_agent_sigma.p, tmp.data(), tmp.size() * 4, cudaMemcpyHostToDevice));
+      b->run_sigma = b->d_agent_sigma.as<float>();
+      b->run_sigma_stride = (uint32_t)sl;
+    }
+    if (grew) ++b->generation;
+  }
+  return upload_state(b, 0, x0, u_nom, nullptr, 0, nullptr, 0, err, err_len);
+}
+
+int mppi_backend_batch_run(mppi_backend* b, uint64_t start_step, char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (b->N == 0 || b->T == 0) {
+    set_err(err, err_len, "mppi_backend_batch_run: no batch prepared.");
+    return MPPI_ERR_INVALID;
+  }
+  uint32_t* up = b->h_up.as<uint32_t>();
+  CK(cudaStreamSynchronize(b->stream));  // the pinned word may still feed a copy
+  up[0] = (uint32_t)start_step;
+  CK(cudaMemcpyAsync(b->io(), up, 4, cudaMemcpyHostToDevice, b->stream));
+  return enqueue_closed_loop(b, err, err_len);
+}
+
+int mppi_backend_batch_fetch(mppi_backend* b, float* states, float* controls, float* costs,
+                             float* terminal, float* x_out, float* u_nom_out, char* err,
+                             size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  const size_t N = b->N, T = b->T;
+  if (states && b->want_s)
+    CK(cudaMemcpyAsync(states, b->d_hs.p, T * N * b->n * 4, cudaMemcpyDeviceToHost, b->stream));
+  if (controls && b->want_c)
+    CK(cudaMemcpyAsync(controls, b->d_hc.p, T * N * b->m * 4, cudaMemcpyDeviceToHost, b->stream));
+  if (costs && b->want_k)
+    CK(cudaMemcpyAsync(costs, b->d_hk.p, T * N * 4, cudaMemcpyDeviceToHost, b->stream));
+  if (terminal && b->want_t)
+    CK(cudaMemcpyAsync(terminal, b->d_term.p, N * b->n * 4, cudaMemcpyDeviceToHost, b->stream));
+  if (x_out)
+    CK(cudaMemcpyAsync(x_out, b->io() + b->off_x(), N * b->n * 4, cudaMemcpyDeviceToHost,
+                       b->stream));
+  if (u_nom_out)
+    CK(cudaMemcpyAsync(u_nom_out, b->io() + b->off_unom(), N * b->HM() * 4,
+                       cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return MPPI_OK;
+}
+
+int mppi_backend_dispatch_simulation(mppi_backend* b, uint32_t T, uint64_t start_step,
+                                     const float* x0, const float* u_nom, const void* mp,
+                                     size_t mp_bytes, const void* cp, size_t cp_bytes,
+                                     float* states, float* controls, float* costs, char* err,
+                                     size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (!u_nom) {
+    set_err(err, err_len, "u_nominal must not be null.");
+    return MPPI_ERR_INVALID;
+  }
+  if (int rc = check_override_sizes(b, mp_bytes, mp, cp_bytes, cp, err, err_len)) return rc;
+  if (int rc = mppi_backend_batch_prepare(b, 1, T, x0, u_nom, nullptr, states != nullptr,
+                                          controls != nullptr, costs != nullptr, false, err,
+                                          err_len))
+    return rc;
+  if ((mp && mp_bytes) || (cp && cp_bytes)) {
+    b->run_mp = pick_params(b, true, mp, mp_bytes);
+    b->run_cp = pick_params(b, false, cp, cp_bytes);
+    if (int rc = upload_state(b, 0, x0, u_nom, mp, mp_bytes, cp, cp_bytes, err, err_len))
+      return rc;
+  }
+  if (int rc = mppi_backend_batch_run(b, start_step, err, err_len)) return rc;
+  return mppi_backend_batch_fetch(b, states, controls, costs, nullptr, nullptr, nullptr, err,
+                                  err_len);
+}
+
+int mppi_backend_dispatch_batch_simulation(mppi_backend* b, uint32_t N, uint32_t T,
+                                           uint64_t start_step, const float* x0,
+                                           const float* u_nom, const mppi_batch_agents* agents,
+                                           float* states, float* controls, float* costs,
+                                           float* terminal, char* err, size_t err_len) {
+  if (int rc = mppi_backend_batch_prepare(b, N, T, x0, u_nom, agents, states != nullptr,
+                                          controls != nullptr, costs != nullptr,
+                                          terminal != nullptr, err, err_len))
+    return rc;
+  if (int rc = mppi_backend_batch_run(b, start_step, err, err_len)) return rc;
+  return mppi_backend_batch_fetch(b, states, controls, costs, terminal, nullptr, nullptr, err,
+                                  err_len);
+}
+
+int mppi_backend_reset(mppi_backend* b, char* err, size_t err_len) {
+  if (!b) return MPPI_ERR_INVALID;
+  if (!b->initialized) return MPPI_OK;
+  if (int rc = check_init(b, err, err_len)) return rc;
+  CK(cudaStreamSynchronize(b->stream));
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->graph_key.clear();
+  b->d_io.release();
+  b->d_costs.release();
+  b->d_partials.release();
+  b->d_hs.release();
+  b->d_hc.release();
+  b->d_hk.release();
+  b->d_term.release();
+  b->d_agent_sigma.release();
+  b->d_agent_mp.release();
+  b->d_agent_cp.release();
+  b->N = b->T = 0;
+  ++b->generation;
+  return MPPI_OK;
+}
+
+int mppi_backend_last_costs(mppi_backend* b, uint32_t a0, uint32_t n, float* out, char* err,
+                            size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (!out || a0 + n > b->N) {
+    set_err(err, err_len, "agent range out of bounds.");
+    return MPPI_ERR_INVALID;
+  }
+  CK(cudaMemcpyAsync(out, b->d_costs.as<float>() + (size_t)a0 * b->K, (size_t)n * b->K * 4,
+                     cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return MPPI_OK;
+}
+
+int mppi_backend_last_weights(mppi_backend* b, uint32_t a0, uint32_t n, float* out, char* err,
+                              size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (!out || a0 + n > b->N) {
+    set_err(err, err_len, "agent range out of bounds.");
+    return MPPI_ERR_INVALID;
+  }
+  DevBuf w;
+  CK(w.ensure((size_t)b->N * b->K * 4));
+  MppiWeightsArgs a{};
+  a.num_agents = b->N;
+  a.K = b->K;
+  a.lambda = b->lambda;
+  a.costs = b->d_costs.as<float>();
+  a.stats = b->io() + b->off_stats();
+  a.weights = w.as<float>();
+  void* args[] = {&a};
+  CK(cudaLaunchKernel((const void*)b->mod->weights, dim3((b->K + 255) / 256, b->N), dim3(256),
+                      args, 0, b->stream));
+  CK(cudaMemcpyAsync(out, w.as<float>() + (size_t)a0 * b->K, (size_t)n * b->K * 4,
+                     cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return MPPI_OK;
+}
+
+int mppi_backend_sample_noise(mppi_backend* b, uint64_t step, uint32_t agent, uint32_t k0,
+                              uint32_t count, const float* sigma, float* normals, float* eps,
+                              char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (count == 0) return MPPI_OK;
+  const size_t per = (size_t)count * b->HM();
+  DevBuf dn, de, ds;
+  CK(dn.ensure(per * 4));
+  CK(de.ensure(per * 4));
+  const float* sig = b->c_sigma();
+  if (sigma) {
+    std::vector<float> s;
+    if (b->cov_full) {
+      if (!cholesky(b->m, sigma, &s)) {
+        set_err(err, err_len, "sigma is not symmetric positive definite.");
+        return MPPI_ERR_INVALID;
+      }
+    } else {
+      s.assign(sigma, sigma + b->m);
+    }
+    CK(ds.ensure(s.size() * 4));
+    CK(cudaMemcpy(ds.p, s.data(), s.size() * 4, cudaMemcpyHostToDevice));
+    sig = ds.as<float>();
+  }
+  MppiNoiseArgs a{};
+  a.k0 = k0;
+  a.count = count;
+  a.H = b->H;
+  a.key = b->seed + agent;
+  a.step = (uint32_t)step;
+  a.sigma = sig;
+  a.normals = dn.as<float>();
+  a.eps = de.as<float>();
+  void* args[] = {&a};
+  CK(cudaLaunchKernel((const void*)b->mod->noise, dim3((count + 127) / 128), dim3(128), args, 0,
+                      b->stream));
+  if (normals) CK(cudaMemcpyAsync(normals, dn.p, per * 4, cudaMemcpyDeviceToHost, b->stream));
+  if (eps) CK(cudaMemcpyAsync(eps, de.p, per * 4, cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return MPPI_OK;
+}
+
+int mppi_backend_time_passes(mppi_backend* b, uint32_t iters, float* rollout_ms,
+                             float* combine_ms, char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (b->N == 0 || iters == 0) {
+    set_err(err, err_len, "no batch prepared / iters == 0.");
+    return MPPI_ERR_INVALID;
+  }
+  float ms = 0.0f;
+  CK(cudaEventRecord(b->ev0, b->stream));
+  for (uint32_t i = 0; i < iters; ++i) CK(launch_rollout(b, 0));
+  CK(cudaEventRecord(b->ev1, b->stream));
+  CK(cudaEventSynchronize(b->ev1));
+  CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  if (rollout_ms) *rollout_ms = ms / iters;
+  CK(cudaEventRecord(b->ev0, b->stream));
+  for (uint32_t i = 0; i < iters; ++i) CK(launch_combine(b, 0, false));
+  CK(cudaEventRecord(b->ev1, b->stream));
+  CK(cudaEventSynchronize(b->ev1));
+  CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  if (combine_ms) *combine_ms = ms / iters;
+  return MPPI_OK;
+}
+
+int mppi_compile_check(const mppi_backend_plugin* plugin, const mppi_backend_config* cfg,
+                       char* log, size_t log_len, char* err, size_t err_len) {
+  if (!plugin || !cfg) {
+    set_err(err, err_len, "null argument.");
+    return MPPI_ERR_INVALID;
+  }
+  mppi_b200::ModuleSpec spec;
+  spec.plugin_path = plugin->source_path ? plugin->source_path : "";
+  spec.dynamics = plugin->dynamics ? plugin->dynamics : "";
+  spec.stage_cost = plugin->stage_cost ? plugin->stage_cost : "";
+  spec.terminal_cost = plugin->terminal_cost ? plugin->terminal_cost : "";
+  spec.state_dim = cfg->state_dim;
+  spec.control_dim = cfg->control_dim;
+  spec.cov_full = cfg->covariance_form == 1;
+  spec.control_cost = cfg->control_cost != 0;
+  spec.model_params_bytes = plugin->model_params_size;
+  spec.cost_params_bytes = plugin->cost_params_size;
+  if (!valid_identifier(spec.dynamics.c_str())) {
+    set_err(err, err_len, "Required callable '" + spec.dynamics + "' is not a valid identifier.");
+    return MPPI_ERR_CALLABLE;
+  }
+  std::string lg, e;
+  const int rc = mppi_b200::compile_check(spec, &lg, &e);
+  set_err(log, log_len, lg);
+  if (rc != MPPI_OK) set_err(err, err_len, e);
+  return rc;
+}
+
+int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
+                             uint32_t* stage_rows, uint32_t* smem_bytes,
+                             uint32_t* kernels_per_step) {
+  if (!b || !b->initialized) return MPPI_ERR_NOT_INIT;
+  if (block) *block = b->geom.block;
+  if (nblk) *nblk = b->geom.nblk;
+  if (stage_rows) *stage_rows = b->geom.stage_rows;
+  if (smem_bytes) *smem_bytes = (uint32_t)b->geom.smem;
+  if (kernels_per_step) *kernels_per_step = 2;
+  return MPPI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,469 @@
+// mppi_kernels.cuh — the MPPI hot path for sm_100a, compiled by NVRTC once per
+// driver together with the user's model plugin (csrc/nvrtc_module.cpp), so
+// the dynamics / cost callables inline into the rollout and the state stays
+// in registers.
+//
+// Compile-time configuration (NVRTC -D options set by the backend):
+//   MPPI_STATE_DIM, MPPI_CONTROL_DIM        problem dimensions
+//   MPPI_COV_FULL                           0: sigma = per-dim std-dev
+//                                           1: sigma = Cholesky factor L
+//   MPPI_CONTROL_COST                       1: add lambda * u_nom^T Sigma^-1 eps
+//   MPPI_DYNAMICS_FN / _STAGE_COST_FN / _TERMINAL_COST_FN   callable names
+//   MPPI_MP_BYTES / MPPI_CP_BYTES           ParamLayout blob sizes
+//
+// Kernels (extern "C" names are looked up by the backend):
+//   mppi_rollout_b{64,128,256}  fused rollout + per-CTA softmax partials +
+//                               weighted-noise partial sums
+//   mppi_combine                per-agent combine -> u_out, diagnostics,
+//                               optional propagate & shift (closed loop)
+//   mppi_weights                normalised weights (inspection only)
+//   mppi_noise                  shaped noise of a sample range (inspection)
+//
+// Reference semantics followed (MarshallVielmetti/mppi_metal):
+//   rollout          shaders/mppi_rollout.metal:36-96 and :103-170
+//   weights          shaders/mppi_reduce.metal:14-121  (w = exp(-(c-min)/l)/sum)
+//   update           shaders/mppi_reduce.metal:130-168 (unclamped noise, Q6)
+//   propagate/shift  shaders/mppi_reduce.metal:175-231 and :413-488
+// The reference runs these as four passes and regenerates every noise value
+// in a serial k-loop of the update pass.  Here the rollout CTA keeps its
+// samples' noise in shared memory, and once its costs are known it reduces
+// sum_k e_k * eps_k for its samples with e_k = exp(-(c_k - m_b) / lambda)
+// taken against the CTA's own minimum m_b.  The combine kernel rescales the
+// CTA partials to the global minimum M (e_k * exp(-(m_b - M) / lambda)),
+// which gives the reference's weights exactly in exact arithmetic.
+#pragma once
+
+#include "mppi_launch.h"
+
+#ifndef MPPI_STATE_DIM
+#error "MPPI_STATE_DIM must be defined"
+#endif
+#ifndef MPPI_CONTROL_DIM
+#error "MPPI_CONTROL_DIM must be defined"
+#endif
+#ifndef MPPI_COV_FULL
+#define MPPI_COV_FULL 0
+#endif
+#ifndef MPPI_CONTROL_COST
+#define MPPI_CONTROL_COST 0
+#endif
+#ifndef MPPI_MP_BYTES
+#define MPPI_MP_BYTES 0
+#endif
+#ifndef MPPI_CP_BYTES
+#define MPPI_CP_BYTES 0
+#endif
+#ifndef MPPI_STAGE_COST_FN
+#define MPPI_STAGE_COST_FN mppi_default_stage_cost
+#endif
+#ifndef MPPI_TERMINAL_COST_FN
+#define MPPI_TERMINAL_COST_FN mppi_default_terminal_cost
+#endif
+
+// Parameter blobs up to this size are copied into shared memory once per CTA
+// and the callables read them from there (uniform broadcast loads).
+#define MPPI_PARAM_SMEM_MAX 8192
+#define MPPI_MP_SMEM (MPPI_MP_BYTES > 0 && MPPI_MP_BYTES <= MPPI_PARAM_SMEM_MAX)
+#define MPPI_CP_SMEM (MPPI_CP_BYTES > 0 && MPPI_CP_BYTES <= MPPI_PARAM_SMEM_MAX)
+
+namespace mppi {
+
+constexpr int kN = MPPI_STATE_DIM;
+constexpr int kM = MPPI_CONTROL_DIM;
+constexpr int kP = (kM + 1) / 2;        // Philox pairs per time step
+constexpr int kNPad = (kN + 3) / 4 * 4;  // state buffer, 16-byte multiple
+constexpr int kSig = MPPI_COV_FULL ? kM * kM : kM;
+constexpr unsigned kFull = 0xffffffffu;
+
+static_assert(kN >= 1 && kN * 4 <= MPPI_MAX_STATE_BYTES, "state_dim out of range");
+static_assert(kM >= 1 && kM <= MPPI_MAX_CONTROL_DIM, "control_dim out of range");
+
+typedef typename mppi_first_arg<decltype(&MPPI_DYNAMICS_FN)>::type DynStateT;
+typedef typename mppi_first_arg<decltype(&MPPI_STAGE_COST_FN)>::type StageStateT;
+typedef typename mppi_first_arg<decltype(&MPPI_TERMINAL_COST_FN)>::type TermStateT;
+
+__device__ __forceinline__ float pos_inf() { return __int_as_float(0x7f800000); }
+
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// Block reductions with a fixed combination order (bit-reproducible).
+template <int NW>
+__device__ __forceinline__ float block_min(float v, float* scratch) {
+  v = warp_min(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) scratch[w] = v;
+  __syncthreads();
+  float r = scratch[0];
+#pragma unroll
+  for (int i = 1; i < NW; ++i) r = fminf(r, scratch[i]);
+  return r;
+}
+template <int NW>
+__device__ __forceinline__ void block_sum3(float& a, float& b, float& c, float* scratch) {
+  a = warp_sum(a);
+  b = warp_sum(b);
+  c = warp_sum(c);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+    scratch[3 * w + 0] = a;
+    scratch[3 * w + 1] = b;
+    scratch[3 * w + 2] = c;
+  }
+  __syncthreads();
+  a = scratch[0];
+  b = scratch[1];
+  c = scratch[2];
+#pragma unroll
+  for (int i = 1; i < NW; ++i) {
+    a += scratch[3 * i + 0];
+    b += scratch[3 * i + 1];
+    c += scratch[3 * i + 2];
+  }
+}
+
+__device__ __forceinline__ float clampf(float v, float lo, float hi) {
+  // Metal clamp(x, lo, hi) = min(max(x, lo), hi)
+  return fminf(fmaxf(v, lo), hi);
+}
+
+// Standard normals n[0..m) and shaped noise eps[0..m) of sample k at time t.
+// Pair p of step t uses counter (step, k*H*P + t*P + p); its first normal is
+// dim 2p, its second dim 2p+1 (dropped for odd m).
+__device__ __forceinline__ void sample_noise(uint32_t step, uint32_t key, uint32_t k,
+                                             uint32_t H, uint32_t t, const float (&sig)[kSig],
+                                             float (&n)[2 * kP], float (&eps)[kM]) {
+#pragma unroll
+  for (int p = 0; p < kP; ++p) {
+    const uint2 w = mppi_philox2x32_10(make_uint2(step, mppi_noise_ctr(k, H, kP, t, p)), key);
+    const float2 g = mppi_box_muller(w);
+    n[2 * p] = g.x;
+    n[2 * p + 1] = g.y;
+  }
+#if MPPI_COV_FULL
+#pragma unroll
+  for (int d = 0; d < kM; ++d) {
+    float e = 0.0f;
+#pragma unroll
+    for (int j = 0; j <= d; ++j) e = fmaf(sig[d * kM + j], n[j], e);
+    eps[d] = e;
+  }
+#else
+#pragma unroll
+  for (int d = 0; d < kM; ++d) eps[d] = n[d] * sig[d];
+#endif
+}
+
+__device__ __forceinline__ void load_sigma(const float* g, float (&sig)[kSig]) {
+#pragma unroll
+  for (int i = 0; i < kSig; ++i) sig[i] = g[i];
+}
+
+// Copies `bytes` (a multiple of 4 after padding) from global to shared memory.
+__device__ __forceinline__ void copy_words(uint32_t* dst, const uint8_t* src, int bytes) {
+  const uint32_t* s = reinterpret_cast<const uint32_t*>(src);
+  for (int i = threadIdx.x; i < (bytes + 3) / 4; i += blockDim.x) dst[i] = s[i];
+}
+
+// --------------------------------------------------------------------------
+// Fused rollout.  One thread per sample; grid (nblk, num_agents).
+// Dynamic shared memory: u_nom[H*m] | staging[stage_rows][BLOCK] | e[BLOCK]
+// --------------------------------------------------------------------------
+template <int BLOCK>
+__device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
+  constexpr int NW = BLOCK / 32;
+  constexpr int PER_LANE = BLOCK / 32;
+  extern __shared__ __align__(16) float dsm[];
+  __shared__ float red_s[3 * NW];
+#if MPPI_MP_SMEM
+  __shared__ __align__(16) uint32_t mp_s[(MPPI_MP_BYTES + 3) / 4];
+#endif
+#if MPPI_CP_SMEM
+  __shared__ __align__(16) uint32_t cp_s[(MPPI_CP_BYTES + 3) / 4];
+#endif
+
+  const uint32_t agent = blockIdx.y;
+  const uint32_t blk = blockIdx.x;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t lane = tid & 31, warp = tid >> 5;
+  const uint32_t K = a.K, H = a.H, HM = H * kM;
+  const uint32_t k = blk * BLOCK + tid;
+  const bool active = k < K;
+  const uint32_t step = *a.step_base + a.step_local;
+  const uint32_t key = a.seed + agent;
+  const bool staged = a.stage_rows >= HM;
+
+  float* un_s = dsm;
+  float* stage_s = dsm + ((HM + 3) & ~3u);
+  float* e_s = stage_s + (size_t)a.stage_rows * BLOCK;
+
+  const float* un_g = a.u_nom + (size_t)agent * HM;
+  for (uint32_t i = tid; i < HM; i += BLOCK) un_s[i] = un_g[i];
+  const uint8_t* mp_g = a.model_params + a.model_stride * agent;
+  const uint8_t* cp_g = a.cost_params + a.cost_stride * agent;
+#if MPPI_MP_SMEM
+  copy_words(mp_s, mp_g, MPPI_MP_BYTES);
+  const uint8_t* mp = reinterpret_cast<const uint8_t*>(mp_s);
+#else
+  const uint8_t* mp = mp_g;
+#endif
+#if MPPI_CP_SMEM
+  copy_words(cp_s, cp_g, MPPI_CP_BYTES);
+  const uint8_t* cp = reinterpret_cast<const uint8_t*>(cp_s);
+#else
+  const uint8_t* cp = cp_g;
+#endif
+  float sig[kSig], lo[kM], hi[kM];
+  load_sigma(a.sigma + (size_t)a.sigma_stride * agent, sig);
+#pragma unroll
+  for (int d = 0; d < kM; ++d) {
+    lo[d] = a.u_min[d];
+    hi[d] = a.u_max[d];
+  }
+#if MPPI_CONTROL_COST
+  float sinv[kSig];
+  load_sigma(a.sigma_inv + (size_t)a.sigma_inv_stride * agent, sinv);
+#endif
+  __syncthreads();
+
+  // ---- rollout: noise -> clamp -> dynamics -> stage cost; terminal cost ----
+  float J = 0.0f;
+  if (active) {
+    __align__(16) float st[kNPad];
+    const float* xg = a.x + (size_t)agent * kN;
+#pragma unroll
+    for (int d = 0; d < kN; ++d) st[d] = xg[d];
+#pragma unroll
+    for (int d = kN; d < kNPad; ++d) st[d] = 0.0f;
+    for (uint32_t t = 0; t < H; ++t) {
+      float n[2 * kP], eps[kM], u[kM];
+      sample_noise(step, key, k, H, t, sig, n, eps);
+#pragma unroll
+      for (int d = 0; d < kM; ++d) u[d] = clampf(un_s[t * kM + d] + eps[d], lo[d], hi[d]);
+#if MPPI_CONTROL_COST
+      {
+        float cc = 0.0f;
+#if MPPI_COV_FULL
+#pragma unroll
+        for (int i = 0; i < kM; ++i) {
+          float r = 0.0f;
+#pragma unroll
+          for (int j = 0; j < kM; ++j) r = fmaf(sinv[i * kM + j], eps[j], r);
+          cc = fmaf(un_s[t * kM + i], r, cc);
+        }
+#else
+#pragma unroll
+        for (int i = 0; i < kM; ++i) cc = fmaf(un_s[t * kM + i], sinv[i] * eps[i], cc);
+#endif
+        J = fmaf(a.lambda, cc, J);
+      }
+#endif
+      if (staged) {
+#pragma unroll
+        for (int d = 0; d < kM; ++d) stage_s[(size_t)(t * kM + d) * BLOCK + tid] = eps[d];
+      }
+      MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u, mp,
+                       make_uint2(step, mppi_dyn_ctr(k, H, kP, t)), key);
+      J += MPPI_STAGE_COST_FN(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u,
+                              mp, cp);
+    }
+    J += MPPI_TERMINAL_COST_FN(reinterpret_cast<TermStateT>(reinterpret_cast<void*>(st)), mp, cp);
+    if (a.costs) a.costs[(size_t)agent * K + k] = J;
+  } else if (staged) {
+    for (uint32_t j = 0; j < HM; ++j) stage_s[(size_t)j * BLOCK + tid] = 0.0f;
+  }
+
+  // ---- CTA softmax statistics against the CTA minimum ----
+  const float bmin = block_min<NW>(active ? J : pos_inf(), red_s);
+  const float e = active ? expf(-(J - bmin) / a.lambda) : 0.0f;
+  float s_e = e, s_e2 = e * e, s_c = active ? J : 0.0f;
+  block_sum3<NW>(s_e, s_e2, s_c, red_s);
+  e_s[tid] = e;
+  float* part = a.partials + ((size_t)agent * a.nblk + blk) * a.pstride;
+  if (tid == 0) {
+    part[0] = bmin;
+    part[1] = s_e;
+    part[2] = s_e2;
+    part[3] = s_c;
+  }
+  __syncthreads();
+  float e_r[PER_LANE];
+#pragma unroll
+  for (int i = 0; i < PER_LANE; ++i) e_r[i] = e_s[lane + 32 * i];
+
+  // ---- weighted noise sums V[j] = sum_k e_k eps_k[j] over this CTA ----
+  const uint32_t R = staged ? HM : a.stage_rows;  // rows per chunk (multiple of m)
+  for (uint32_t r0 = 0; r0 < HM; r0 += R) {
+    const uint32_t rows = min(R, HM - r0);
+    const float* base = stage_s;
+    if (!staged) {
+      // regenerate this chunk's noise (same counters, same values)
+      __syncthreads();
+      const uint32_t t0 = r0 / kM, t1 = (r0 + rows) / kM;
+      for (uint32_t t = t0; t < t1; ++t) {
+        float n[2 * kP], eps[kM];
+        if (active) {
+          sample_noise(step, key, k, H, t, sig, n, eps);
+        } else {
+#pragma unroll
+          for (int d = 0; d < kM; ++d) eps[d] = 0.0f;
+        }
+#pragma unroll
+        for (int d = 0; d < kM; ++d)
+          stage_s[(size_t)((t - t0) * kM + d) * BLOCK + tid] = eps[d];
+      }
+      __syncthreads();
+    } else {
+      base = stage_s + (size_t)r0 * BLOCK;
+    }
+    for (uint32_t r = warp; r < rows; r += NW) {
+      const float* row = base + (size_t)r * BLOCK;
+      float s = 0.0f;
+#pragma unroll
+      for (int i = 0; i < PER_LANE; ++i) s = fmaf(e_r[i], row[lane + 32 * i], s);
+      s = warp_sum(s);
+      if (lane == 0) part[MPPI_PARTIAL_HEAD + r0 + r] = s;
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// Combine: one CTA per agent.  Dynamic shared memory: scale[nblk] | u[H*m].
+// --------------------------------------------------------------------------
+constexpr int kCombineBlock = 256;
+
+__device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
+  constexpr int NW = kCombineBlock / 32;
+  extern __shared__ __align__(16) float dsm[];
+  __shared__ float red_s[3 * NW];
+  const uint32_t agent = blockIdx.x;
+  const uint32_t tid = threadIdx.x;
+  const uint32_t H = a.H, HM = H * kM, nblk = a.nblk, ps = a.pstride;
+  float* scale_s = dsm;
+  float* u_s = dsm + ((nblk + 3) & ~3u);
+  const float* P = a.partials + (size_t)agent * nblk * ps;
+
+  float lm = pos_inf();
+  for (uint32_t b = tid; b < nblk; b += kCombineBlock) lm = fminf(lm, P[(size_t)b * ps]);
+  const float M = block_min<NW>(lm, red_s);
+  float S = 0.0f, Q = 0.0f, C = 0.0f;
+  for (uint32_t b = tid; b < nblk; b += kCombineBlock) {
+    const float* pb = P + (size_t)b * ps;
+    const float sc = expf(-(pb[0] - M) / a.lambda);
+    scale_s[b] = sc;
+    S = fmaf(sc, pb[1], S);
+    Q = fmaf(sc * sc, pb[2], Q);
+    C += pb[3];
+  }
+  block_sum3<NW>(S, Q, C, red_s);  // ends with a barrier: scale_s visible
+
+  const float invS = 1.0f / S;
+  float* un = a.u_nom + (size_t)agent * HM;
+  float* uo = a.u_out + (size_t)agent * HM;
+  for (uint32_t j = tid; j < HM; j += kCombineBlock) {
+    float v = 0.0f;
+    for (uint32_t b = 0; b < nblk; ++b)
+      v = fmaf(scale_s[b], P[(size_t)b * ps + MPPI_PARTIAL_HEAD + j], v);
+    const uint32_t d = j % kM;
+    const float u = clampf(un[j] + v * invS, a.u_min[d], a.u_max[d]);
+    u_s[j] = u;
+    uo[j] = u;
+  }
+  if (tid == 0) {
+    a.diag[agent * 3 + 0] = M;
+    a.diag[agent * 3 + 1] = C / (float)a.K;
+    a.diag[agent * 3 + 2] = S * S / Q;  // 1 / sum w^2 with w = e / S
+    if (a.stats) {
+      a.stats[agent * 4 + 0] = M;
+      a.stats[agent * 4 + 1] = S;
+      a.stats[agent * 4 + 2] = Q;
+      a.stats[agent * 4 + 3] = C;
+    }
+  }
+  if (!a.propagate) return;
+  __syncthreads();  // u_s complete, all reads of un done
+
+  // ---- propagate & shift (shaders/mppi_reduce.metal:175-231, 413-488) ----
+  if (tid == 0) {
+    const uint32_t step = *a.step_base + a.step_local;
+    const uint32_t row = a.step_local * a.num_agents + agent;
+    float* xg = a.x + (size_t)agent * kN;
+    __align__(16) float st[kNPad];
+    float u0[kM];
+#pragma unroll
+    for (int d = 0; d < kN; ++d) st[d] = xg[d];
+#pragma unroll
+    for (int d = kN; d < kNPad; ++d) st[d] = 0.0f;
+#pragma unroll
+    for (int d = 0; d < kM; ++d) u0[d] = u_s[d];
+    if (a.hist_states)
+      for (int d = 0; d < kN; ++d) a.hist_states[(size_t)row * kN + d] = st[d];
+    if (a.hist_controls)
+      for (int d = 0; d < kM; ++d) a.hist_controls[(size_t)row * kM + d] = u0[d];
+    if (a.hist_costs) a.hist_costs[row] = M;
+    // counter (step, 0x80000000); seed = agent index (0 for a single agent)
+    MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u0,
+                     a.model_params + a.model_stride * agent, make_uint2(step, 0x80000000u),
+                     agent);
+#pragma unroll
+    for (int d = 0; d < kN; ++d) xg[d] = st[d];
+    if (a.terminal)
+      for (int d = 0; d < kN; ++d) a.terminal[(size_t)agent * kN + d] = st[d];
+  }
+  for (uint32_t j = tid; j < HM; j += kCombineBlock) {
+    const uint32_t t = j / kM, d = j % kM;
+    un[j] = (t + 1 < H) ? u_s[j + kM] : u_s[(H - 1) * kM + d];  // shift left, hold last
+  }
+}
+
+}  // namespace mppi
+
+#define MPPI_ROLLOUT_ENTRY(B)                                                      \
+  extern "C" __global__ void __launch_bounds__(B) mppi_rollout_b##B(const MppiRolloutArgs a) { \
+    mppi::rollout_body<B>(a);                                                     \
+  }
+MPPI_ROLLOUT_ENTRY(64)
+MPPI_ROLLOUT_ENTRY(128)
+MPPI_ROLLOUT_ENTRY(256)
+
+extern "C" __global__ void __launch_bounds__(mppi::kCombineBlock)
+    mppi_combine(const MppiCombineArgs a) {
+  mppi::combine_body(a);
+}
+
+extern "C" __global__ void __launch_bounds__(256) mppi_weights(const MppiWeightsArgs a) {
+  const uint32_t agent = blockIdx.y;
+  const uint32_t k = blockIdx.x * 256 + threadIdx.x;
+  if (k >= a.K) return;
+  const float M = a.stats[agent * 4 + 0], S = a.stats[agent * 4 + 1];
+  const float c = a.costs[(size_t)agent * a.K + k];
+  a.weights[(size_t)agent * a.K + k] = expf(-(c - M) / a.lambda) / S;
+}
+
+extern "C" __global__ void __launch_bounds__(128) mppi_noise(const MppiNoiseArgs a) {
+  const uint32_t i = blockIdx.x * 128 + threadIdx.x;
+  if (i >= a.count) return;
+  float sig[mppi::kSig];
+  mppi::load_sigma(a.sigma, sig);
+  const uint32_t k = a.k0 + i;
+  for (uint32_t t = 0; t < a.H; ++t) {
+    float n[2 * mppi::kP], eps[mppi::kM];
+    mppi::sample_noise(a.step, a.key, k, a.H, t, sig, n, eps);
+    const size_t o = ((size_t)i * a.H + t) * mppi::kM;
+#pragma unroll
+    for (int d = 0; d < mppi::kM; ++d) {
+      if (a.normals) a.normals[o + d] = n[d];
+      if (a.eps) a.eps[o + d] = eps[d];
+    }
+  }
+}

@@ -1,0 +1,98 @@
+// mppi_launch.h — kernel argument records shared by the host backend
+// (csrc/backend.cpp) and the NVRTC-compiled kernels (mppi_kernels.cuh).
+// Plain C layout: only pointers, 32/64-bit integers and floats, so the
+// struct is identical under g++, nvcc and NVRTC.
+#pragma once
+
+#if !defined(__CUDACC_RTC__)
+#include <cstdint>
+#endif
+
+// Floats in front of the weighted-noise sums of one partial record:
+// [block min cost, sum e, sum e^2, sum cost].
+#define MPPI_PARTIAL_HEAD 4
+
+// One launch of the fused rollout kernel: every agent of the batch, every
+// sample of every agent.  Grid = (nblk, num_agents), one thread per sample.
+struct MppiRolloutArgs {
+  uint32_t num_agents;
+  uint32_t K;           // samples per agent
+  uint32_t H;           // horizon
+  uint32_t nblk;        // CTAs per agent = ceil(K / block)
+  uint32_t stage_rows;  // rows of the per-CTA noise staging buffer; >= H*m
+                        // stages the whole horizon during the rollout,
+                        // fewer regenerates it chunk by chunk afterwards
+  uint32_t seed;        // agent a draws with key seed + a
+  uint32_t step_local;  // absolute step index = *step_base + step_local
+  uint32_t pstride;     // floats per partial record (head + H*m, padded)
+  float lambda;
+  uint32_t sigma_stride;      // floats between agents' sigma rows (0: shared)
+  uint32_t sigma_inv_stride;  // same for sigma_inv
+  uint32_t pad0;
+  const uint32_t* step_base;  // device word
+  const float* x;             // [N][n] current states
+  const float* u_nom;         // [N][H*m] nominal controls
+  const float* sigma;         // std-devs (diagonal) or Cholesky factor (full)
+  const float* sigma_inv;     // Sigma^-1 (diagonal or full) for the control cost
+  const float* u_min;         // [m]
+  const float* u_max;         // [m]
+  const uint8_t* model_params;  // agent a at + a * model_stride
+  const uint8_t* cost_params;
+  uint64_t model_stride;
+  uint64_t cost_stride;
+  float* costs;     // [N][K] per-sample costs (may be null)
+  float* partials;  // [N][nblk][pstride]
+};
+
+// One launch of the combine (+ optional propagate & shift) kernel.
+// Grid = num_agents, one CTA per agent.
+struct MppiCombineArgs {
+  uint32_t num_agents;
+  uint32_t K;
+  uint32_t H;
+  uint32_t nblk;
+  uint32_t pstride;
+  uint32_t step_local;  // history row written by the propagate stage
+  float lambda;
+  uint32_t propagate;   // 1: propagate x with u*[0], write history, shift u_nom
+  const uint32_t* step_base;
+  const float* partials;
+  const float* u_min;
+  const float* u_max;
+  const uint8_t* model_params;
+  uint64_t model_stride;
+  float* u_nom;        // [N][H*m] read; shifted in place when propagating
+  float* u_out;        // [N][H*m]
+  float* diag;         // [N][3]: best cost, mean cost, effective sample size
+  float* stats;        // [N][4]: min, sum e, sum e^2, sum cost (may be null)
+  float* x;            // [N][n] state, propagated in place
+  float* hist_states;  // [T][N][n] (may be null)
+  float* hist_controls;  // [T][N][m] (may be null)
+  float* hist_costs;   // [T][N] (may be null)
+  float* terminal;     // [N][n] (may be null)
+};
+
+// Normalised weights from the per-sample costs and the combine statistics
+// (inspection path; the control update does not need them materialised).
+struct MppiWeightsArgs {
+  uint32_t num_agents;
+  uint32_t K;
+  float lambda;
+  uint32_t pad0;
+  const float* costs;  // [N][K]
+  const float* stats;  // [N][4]
+  float* weights;      // [N][K]
+};
+
+// Noise of samples [k0, k0 + count) of one agent, every time step.
+struct MppiNoiseArgs {
+  uint32_t k0;
+  uint32_t count;
+  uint32_t H;
+  uint32_t key;
+  uint32_t step;
+  uint32_t pad0;
+  const float* sigma;  // this agent's sigma row
+  float* normals;      // [count][H*m] (may be null)
+  float* eps;          // [count][H*m] (may be null)
+};

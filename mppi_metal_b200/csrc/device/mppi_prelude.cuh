@@ -1,0 +1,143 @@
+// mppi_prelude.cuh — device-side basics shared by every kernel of the library
+// and by user model plugins.
+//
+// Compiled two ways:
+//   * by NVRTC, as the first part of the per-driver translation unit
+//     (prelude + user plugin + mppi_kernels.cuh), see csrc/nvrtc_module.cpp;
+//   * by nvcc, inside csrc/static_kernels.cu (Philox known-answer kernels).
+//
+// Contents
+//   - fixed-width integer types under NVRTC (no libc headers there);
+//   - the plugin callable ABI: the CUDA form of the reference's
+//     shaders/mppi_core.h:11-42 (same argument order and meaning; the
+//     reference's `thread` / `device` address spaces become plain pointers);
+//   - Philox-2x32-10, the uint -> (0,1) map and Box-Muller, the CUDA form of
+//     shaders/philox.h:19-50.  Words are bit-exact with the reference.  The
+//     normals use correctly-rounded float ops for the uniform map (identical
+//     bits to the reference) and CUDA's accurate logf / sqrtf / sincospif
+//     for the transcendental part.
+#pragma once
+
+#if defined(__CUDACC_RTC__)
+typedef unsigned char uint8_t;
+typedef signed char int8_t;
+typedef unsigned short uint16_t;
+typedef unsigned int uint32_t;
+typedef int int32_t;
+typedef unsigned long long uint64_t;
+typedef long long int64_t;
+#else
+#include <cstdint>
+#endif
+
+#ifndef MPPI_MAX_STATE_BYTES
+// Thread-local state buffer limit (shaders/mppi_core.h:32).
+#define MPPI_MAX_STATE_BYTES 128
+#endif
+#ifndef MPPI_MAX_CONTROL_DIM
+// Control dimension limit (shaders/mppi_core.h:33).
+#define MPPI_MAX_CONTROL_DIM 16
+#endif
+
+// ---------------------------------------------------------------------------
+// Callable ABI (shaders/mppi_core.h:11-26).  A plugin defines __device__
+// functions with these shapes; the names are chosen in ModelPluginSpec.
+//   dynamics      : in-place state update; rng_counter / rng_seed let a
+//                   stochastic model draw its own Philox numbers.
+//   stage cost    : running cost on (post-dynamics state, clamped control).
+//   terminal cost : cost on the final state.
+// The state pointer may be declared as uint8_t* (as in the reference) or as
+// float* / a struct pointer: the library casts to the declared type.
+// ---------------------------------------------------------------------------
+typedef void (*MppiDynamicsFn)(uint8_t* state, const float* control,
+                               const uint8_t* model_params, uint2 rng_counter,
+                               uint32_t rng_seed);
+typedef float (*MppiStageCostFn)(const uint8_t* state, const float* control,
+                                 const uint8_t* model_params,
+                                 const uint8_t* cost_params);
+typedef float (*MppiTerminalCostFn)(const uint8_t* state,
+                                    const uint8_t* model_params,
+                                    const uint8_t* cost_params);
+
+// Default costs used when a cost callable is not named
+// (shaders/mppi_rollout.metal:11-28): both return zero.
+__device__ __forceinline__ float mppi_default_stage_cost(const uint8_t*, const float*,
+                                                         const uint8_t*, const uint8_t*) {
+  return 0.0f;
+}
+__device__ __forceinline__ float mppi_default_terminal_cost(const uint8_t*, const uint8_t*,
+                                                            const uint8_t*) {
+  return 0.0f;
+}
+
+// First-parameter type of a plain function, so the library can hand a
+// plugin its state in whatever pointer type the plugin declared.
+template <class F>
+struct mppi_first_arg;
+template <class R, class A0, class... As>
+struct mppi_first_arg<R (*)(A0, As...)> {
+  typedef A0 type;
+};
+
+// ---------------------------------------------------------------------------
+// Philox-2x32-10 (shaders/philox.h:19-36).
+//   round: (c0, c1) -> (hi(c0 * M) ^ key ^ c1, lo(c0 * M)),  M = 0xD256D193
+//   key  : += 0x9E3779B9 after each of the 10 rounds
+// ---------------------------------------------------------------------------
+#define MPPI_PHILOX_M 0xD256D193u
+#define MPPI_PHILOX_W 0x9E3779B9u
+
+__device__ __forceinline__ uint2 mppi_philox2x32_10(uint2 ctr, uint32_t key) {
+  uint32_t c0 = ctr.x, c1 = ctr.y;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    const uint32_t hi = __umulhi(c0, MPPI_PHILOX_M);
+    const uint32_t lo = c0 * MPPI_PHILOX_M;
+    c0 = hi ^ key ^ c1;
+    c1 = lo;
+    key += MPPI_PHILOX_W;
+  }
+  return make_uint2(c0, c1);
+}
+
+// (float(x) + 0.5f) * 2^-32 (shaders/philox.h:39-41): two correctly rounded
+// float operations, so the result is bit-identical to the reference's.
+__device__ __forceinline__ float mppi_uint_to_01(uint32_t x) {
+  const float f = __fadd_rn(__uint2float_rn(x), 0.5f);
+  return __fmul_rn(f, 2.3283064365386962890625e-10f);
+}
+
+// Box-Muller (shaders/philox.h:44-50): r = sqrt(-2 ln u1), theta = 2 pi u2.
+// sincospif(2 u2) evaluates sin/cos(2 pi u2) without rounding 2 pi u2 to a
+// float first, so it stays closer to the exact value the oracle computes.
+__device__ __forceinline__ float2 mppi_box_muller(uint2 w) {
+  const float u1 = mppi_uint_to_01(w.x);
+  const float u2 = mppi_uint_to_01(w.y);
+  const float r = sqrtf(-2.0f * logf(u1));
+  float s, c;
+  sincospif(2.0f * u2, &s, &c);
+  return make_float2(r * c, r * s);
+}
+
+// Reference-compatible spellings for plugins ported from MSL
+// (examples/wez_environment_batch/wez_environment.metal:166-173 draws with
+// philox2x32_10 / uint_to_01 inside its dynamics).
+__device__ __forceinline__ uint2 philox2x32_10(uint2 ctr, uint32_t key) {
+  return mppi_philox2x32_10(ctr, key);
+}
+__device__ __forceinline__ float uint_to_01(uint32_t x) { return mppi_uint_to_01(x); }
+__device__ __forceinline__ float2 box_muller(uint2 w) { return mppi_box_muller(w); }
+
+// Counter layout of the reference (shaders/mppi_rollout.metal:66-90):
+//   noise pair  (step, k*H*P + t*P + d/2)          P = ceil(m/2)
+//   dynamics    (step, k*H*P + t + 0x80000000)
+//   propagate   (step, 0x80000000)                  (mppi_reduce.metal:212)
+// All arithmetic wraps modulo 2^32 exactly as the reference's uint math.
+__device__ __forceinline__ uint32_t mppi_noise_ctr(uint32_t k, uint32_t H, uint32_t P,
+                                                   uint32_t t, uint32_t pair) {
+  return k * H * P + t * P + pair;
+}
+__device__ __forceinline__ uint32_t mppi_dyn_ctr(uint32_t k, uint32_t H, uint32_t P,
+                                                 uint32_t t) {
+  return k * H * P + t + 0x80000000u;
+}

@@ -1,0 +1,59 @@
+// nvrtc_module.hpp — per-driver kernel module: the library kernel template
+// (csrc/device/*.cuh, embedded in this library) compiled together with the
+// user's plugin source by NVRTC for sm_100a, loaded with cudaLibraryLoadData.
+//
+// Replaces the reference's pipeline construction (src/metal_backend.mm:233-560:
+// load the library metallib and the user metallib, look the callables up by
+// name, link them into the rollout pipelines through visible function
+// tables).  Here the callables are bound by name at compile time, so they
+// inline into the rollout kernel.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace mppi_b200 {
+
+struct ModuleSpec {
+  std::string plugin_path;    // CUDA source of the callables
+  std::string dynamics;       // required
+  std::string stage_cost;     // "" = library default
+  std::string terminal_cost;  // "" = library default
+  uint32_t state_dim = 0;
+  uint32_t control_dim = 0;
+  bool cov_full = false;
+  bool control_cost = false;
+  uint64_t model_params_bytes = 0;
+  uint64_t cost_params_bytes = 0;
+};
+
+// Rollout block sizes compiled into every module (mppi_rollout_b<N>).
+constexpr int kRolloutBlocks[3] = {64, 128, 256};
+
+struct KernelModule {
+  cudaLibrary_t library = nullptr;
+  cudaKernel_t rollout[3] = {nullptr, nullptr, nullptr};
+  cudaKernel_t combine = nullptr;
+  cudaKernel_t weights = nullptr;
+  cudaKernel_t noise = nullptr;
+  std::string build_log;  // NVRTC log of the compile (warnings, ptxas info)
+};
+
+// Status codes mirror include/mppi_b200/mppi_backend.h.
+// Returns 0 and a shared module (cached per process and, when a cache
+// directory is usable, on disk) or an error code with a message.
+int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out,
+                std::string* error);
+
+// Compiles the module without loading it (no GPU needed); `log` receives the
+// NVRTC log including ptxas resource usage.
+int compile_check(const ModuleSpec& spec, std::string* log, std::string* error);
+
+// The embedded device sources (generated at build time).
+const char* embedded_source(const char* name);
+
+}  // namespace mppi_b200

@@ -1,0 +1,171 @@
+"""Parameter blobs of the shipped model plugins and the seeded workloads.
+
+``ctypes`` mirrors of mppi_metal_b200/plugins/model_params.h, plus builders
+for the benchmark problems.  No public benchmark data is involved: every
+workload is drawn from numpy's PCG64 generator with a fixed seed, with the
+shapes, sizes and value ranges of the configurations it stands for.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+UNICYCLE_MAX_OBS = 16
+BICYCLE_MAX_SEGMENTS = 32
+QUAD_MAX_OBS = 32
+
+_f = ctypes.c_float
+_u = ctypes.c_uint32
+
+
+class NonholonomicModelParams(ctypes.Structure):
+    _fields_ = [("v_max", _f), ("dt", _f)]
+
+
+class NonholonomicCostParams(ctypes.Structure):
+    _fields_ = [("x_goal", _f), ("y_goal", _f), ("goal_radius", _f), ("pos_weight", _f),
+                ("heading_weight", _f), ("control_weight", _f)]
+
+
+class UnicycleModelParams(ctypes.Structure):
+    _fields_ = [("dt", _f), ("pad0", _f), ("pad1", _f), ("pad2", _f)]
+
+
+class UnicycleCostParams(ctypes.Structure):
+    _fields_ = [("goal_x", _f), ("goal_y", _f), ("w_goal", _f), ("w_obs", _f),
+                ("w_terminal", _f), ("num_obs", _u), ("pad0", _f), ("pad1", _f),
+                ("obs_cx", _f * UNICYCLE_MAX_OBS), ("obs_cy", _f * UNICYCLE_MAX_OBS),
+                ("obs_vx", _f * UNICYCLE_MAX_OBS), ("obs_vy", _f * UNICYCLE_MAX_OBS),
+                ("obs_r", _f * UNICYCLE_MAX_OBS)]
+
+
+class BicycleModelParams(ctypes.Structure):
+    _fields_ = [("dt", _f), ("wheelbase", _f), ("delta_max", _f), ("pad0", _f)]
+
+
+class BicycleCostParams(ctypes.Structure):
+    _fields_ = [("x0", _f), ("knot_dx", _f), ("num_segments", _u), ("v_ref", _f),
+                ("w_lat", _f), ("w_head", _f), ("w_speed", _f), ("w_terminal", _f),
+                ("coef", (_f * 4) * BICYCLE_MAX_SEGMENTS)]
+
+
+class QuadrotorModelParams(ctypes.Structure):
+    _fields_ = [("dt", _f), ("mass", _f), ("gravity", _f), ("arm", _f), ("yaw_coef", _f),
+                ("jx", _f), ("jy", _f), ("jz", _f)]
+
+
+class QuadrotorCostParams(ctypes.Structure):
+    _fields_ = [("wp_x", _f), ("wp_y", _f), ("wp_z", _f), ("w_pos", _f), ("w_vel", _f),
+                ("w_att", _f), ("w_rate", _f), ("w_obs", _f), ("w_terminal", _f),
+                ("num_obs", _u), ("pad0", _f), ("pad1", _f),
+                ("obs_cx", _f * QUAD_MAX_OBS), ("obs_cy", _f * QUAD_MAX_OBS),
+                ("obs_cz", _f * QUAD_MAX_OBS), ("obs_r", _f * QUAD_MAX_OBS)]
+
+
+def blob(s: ctypes.Structure) -> bytes:
+    return ctypes.string_at(ctypes.addressof(s), ctypes.sizeof(s))
+
+
+@dataclass
+class Workload:
+    """One benchmark / parity problem, in driver terms."""
+    name: str
+    plugin: str
+    oracle_model: str
+    state_dim: int
+    control_dim: int
+    horizon: int
+    sample_count: int
+    lam: float
+    sigma: np.ndarray            # shared sigma (std-devs) or covariance
+    sigma_inv: np.ndarray
+    u_min: np.ndarray
+    u_max: np.ndarray
+    num_agents: int
+    num_steps: int
+    x0: np.ndarray               # [N][n]
+    model_params: bytes
+    cost_params: list = field(default_factory=list)   # per-agent blobs
+    agent_sigma: np.ndarray | None = None             # [N][m] or None
+    cov_full: bool = False
+    control_cost: bool = False
+    seed: int = 0
+
+    @property
+    def cost_params_packed(self) -> bytes:
+        return b"".join(self.cost_params)
+
+    @property
+    def cost_stride(self) -> int:
+        return len(self.cost_params[0]) if self.cost_params else 0
+
+    @property
+    def rollout_steps_per_control_step(self) -> int:
+        return self.num_agents * self.sample_count * self.horizon
+
+
+def _unicycle_cost(rng: np.random.Generator, n_obs: int, moving: bool) -> UnicycleCostParams:
+    c = UnicycleCostParams()
+    gx, gy = rng.uniform(-10.0, 10.0, size=2)
+    c.goal_x, c.goal_y = float(gx), float(gy)
+    c.w_goal = 1.0
+    c.w_obs = 1.0e3
+    c.w_terminal = 10.0
+    c.num_obs = n_obs
+    cx = rng.uniform(-10.0, 10.0, size=n_obs)
+    cy = rng.uniform(-10.0, 10.0, size=n_obs)
+    r = rng.uniform(0.3, 1.0, size=n_obs)
+    v = rng.uniform(-0.5, 0.5, size=(n_obs, 2)) if moving else np.zeros((n_obs, 2))
+    for i in range(n_obs):
+        c.obs_cx[i], c.obs_cy[i] = float(cx[i]), float(cy[i])
+        c.obs_vx[i], c.obs_vy[i] = float(v[i, 0]), float(v[i, 1])
+        c.obs_r[i] = float(r[i])
+    return c
+
+
+def unicycle_single(seed: int = 0, K: int = 1024, H: int = 30, T: int = 200) -> Workload:
+    """Single-agent plain MPPI, kinematic unicycle: dt 0.05, H 30, K 1024,
+    lambda 1, sigma [0.5, 0.5], v in [-1, 2], omega in [-1.5, 1.5], goal and 8
+    static circles (centres U[-10,10]^2, radii U[0.3,1.0]), control cost on,
+    Philox seed 0, 200 closed-loop steps from x0 = 0."""
+    rng = np.random.default_rng(seed)
+    mp = UnicycleModelParams(0.05, 0.0, 0.0, 0.0)
+    cp = _unicycle_cost(rng, 8, moving=False)
+    sigma = np.array([0.5, 0.5], np.float32)
+    return Workload("unicycle_single", "unicycle_obstacles", "unicycle_obstacles", 4, 2, H, K,
+                    1.0, sigma, (1.0 / sigma ** 2).astype(np.float32),
+                    np.array([-1.0, -1.5], np.float32), np.array([2.0, 1.5], np.float32),
+                    1, T, np.zeros((1, 4), np.float32), blob(mp), [blob(cp)], None,
+                    control_cost=True, seed=seed)
+
+
+def unicycle_batch(seed: int = 0, N: int = 256, K: int = 4096, H: int = 50, T: int = 300,
+                   n_obs: int = 16) -> Workload:
+    """Batched plain MPPI: N unicycle agents, each with its own seeded start,
+    goal, 16 moving circular keep-out regions (velocities U[-0.5,0.5]^2) and
+    per-dimension sigma U[0.2, 0.8]; K 4096, H 50, 300 closed-loop steps."""
+    rng = np.random.default_rng(seed)
+    mp = UnicycleModelParams(0.05, 0.0, 0.0, 0.0)
+    x0 = np.zeros((N, 4), np.float32)
+    x0[:, 0:2] = rng.uniform(-10.0, 10.0, size=(N, 2))
+    x0[:, 2] = rng.uniform(-np.pi, np.pi, size=N)
+    cps = [blob(_unicycle_cost(rng, n_obs, moving=True)) for _ in range(N)]
+    agent_sigma = rng.uniform(0.2, 0.8, size=(N, 2)).astype(np.float32)
+    sigma = np.array([0.5, 0.5], np.float32)
+    return Workload("unicycle_batch", "unicycle_obstacles", "unicycle_obstacles", 4, 2, H, K,
+                    1.0, sigma, (1.0 / sigma ** 2).astype(np.float32),
+                    np.array([-1.0, -1.5], np.float32), np.array([2.0, 1.5], np.float32),
+                    N, T, x0, blob(mp), cps, agent_sigma, control_cost=False, seed=seed)
+
+
+def double_integrator_test(K: int = 64, H: int = 10) -> Workload:
+    """The reference test fixture (tests/mppi_driver_tests.cpp:42-72):
+    n 4, m 2, H 10, K 64, lambda 1, sigma [1, 1], bounds [-1, 1]; stage cost
+    px^2 + py^2 and the default (zero) terminal cost; x0 = (1, 1, 0, 0)."""
+    sigma = np.ones(2, np.float32)
+    return Workload("double_integrator_test", "double_integrator", "double_integrator", 4, 2, H,
+                    K, 1.0, sigma, sigma.copy(), -np.ones(2, np.float32),
+                    np.ones(2, np.float32), 1, 5, np.array([[1.0, 1.0, 0.0, 0.0]], np.float32),
+                    b"", [], None)

@@ -1,0 +1,119 @@
+"""The C ABI boundary, without a GPU: the library loads, exports every
+function the public headers declare, and every shipped plugin compiles with
+the library kernels for sm_100a through NVRTC."""
+from __future__ import annotations
+
+import re
+from pathlib import Path
+
+import pytest
+
+from mppi_metal_b200 import _lib
+from mppi_metal_b200.backend import compile_check
+
+INCLUDE = Path(_lib.INCLUDE_DIR)
+
+
+def declared_c_functions() -> set[str]:
+    names = set()
+    for h in (INCLUDE / "mppi_b200").glob("*.h"):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(mppi_[a-z0-9_]+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_loads(lib):
+    assert b"sm_100a" in lib.mppi_b200_version()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_c_functions()
+    assert len(names) >= 25
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_ctypes_signatures_cover_the_headers():
+    assert declared_c_functions() == set(_lib.SIGNATURES)
+
+
+def test_cpp_driver_symbols_exported(lib):
+    import subprocess
+    out = subprocess.run(["nm", "-D", "--defined-only", "-C", str(_lib.LIB_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    for sym in ["mppi_metal::MPPIDriver::MPPIDriver(mppi_metal::DriverConfig const&)",
+                "mppi_metal::MPPIDriver::initialize(",
+                "mppi_metal::MPPIDriver::set_problem_params(",
+                "mppi_metal::MPPIDriver::step(",
+                "mppi_metal::MPPIDriver::reset(std::",
+                "mppi_metal::MPPIDriver::reset(mppi_metal::ControlSequenceView const&",
+                "mppi_metal::MPPIDriver::simulate(",
+                "mppi_metal::MPPIDriver::simulate_batch("]:
+        assert sym in out, sym
+
+
+PLUGINS = [
+    ("double_integrator", 4, 2, 0, 0),
+    ("nonholonomic_vehicle", 4, 2, 8, 24),
+    ("unicycle_obstacles", 4, 2, 16, 352),
+]
+
+
+@pytest.mark.parametrize("plugin,n,m,mp,cp", PLUGINS)
+@pytest.mark.parametrize("cov_full,control_cost", [(False, False), (True, True)])
+def test_plugins_compile_for_sm100a(plugin, n, m, mp, cp, cov_full, control_cost):
+    rc, err, log = compile_check(plugin, n, m, cov_full=cov_full, control_cost=control_cost,
+                                 model_params_size=mp, cost_params_size=cp)
+    assert rc == 0, err
+    assert "mppi_rollout_b128" in log and "sm_100a" in log
+    # no register spills in the benchmark model's hot kernel
+    block = log.split("Function properties for mppi_rollout_b128")[1].split("Compile time")[0]
+    if plugin == "unicycle_obstacles":
+        assert "0 bytes spill stores" in block
+
+
+def test_missing_callable_is_named():
+    rc, err, _ = compile_check("double_integrator", 4, 2, dynamics="nonexistent_fn")
+    assert rc == _lib.MPPI_ERR_CALLABLE
+    assert "nonexistent_fn" in err
+
+
+def test_missing_cost_callable_is_named():
+    rc, err, _ = compile_check("double_integrator", 4, 2, stage_cost="no_such_cost")
+    assert rc == _lib.MPPI_ERR_CALLABLE
+    assert "no_such_cost" in err
+
+
+def test_unreadable_plugin_is_reported():
+    rc, err, _ = compile_check("/nonexistent/plugin.cu", 4, 2)
+    assert rc == _lib.MPPI_ERR_PLUGIN
+    assert "/nonexistent/plugin.cu" in err
+
+
+def test_plugin_compile_error_is_reported(tmp_path):
+    bad = tmp_path / "bad.cu"
+    bad.write_text('#include "mppi_core.h"\n__device__ void mppi_dynamics(uint8_t* s, '
+                   'const float* u, const uint8_t* p, uint2 c, uint32_t k) { this is not C++ }\n')
+    rc, err, _ = compile_check(str(bad), 4, 2, stage_cost="", terminal_cost="")
+    assert rc == _lib.MPPI_ERR_PLUGIN
+    assert "bad.cu" in err
+
+
+def test_reference_style_plugin_includes_resolve(tmp_path):
+    """A plugin written like the reference's (includes "mppi_core.h" and
+    "philox.h", declares state as uint8_t*, draws Philox numbers in its
+    dynamics) compiles unchanged apart from the address-space keywords."""
+    src = tmp_path / "stochastic.cu"
+    src.write_text(
+        '#include "mppi_core.h"\n#include "philox.h"\n'
+        "__device__ void mppi_dynamics(uint8_t* state_raw, const float* control,\n"
+        "    const uint8_t* mp, uint2 rng_counter, uint32_t rng_seed) {\n"
+        "  float* s = (float*)state_raw;\n"
+        "  uint2 c = make_uint2(rng_counter.x, rng_counter.y + 0x1000u);\n"
+        "  float u = uint_to_01(philox2x32_10(c, rng_seed).x);\n"
+        "  s[0] += 0.1f * control[0] + 0.01f * u;\n"
+        "  s[1] += 0.1f * control[1];\n}\n")
+    rc, err, _ = compile_check(str(src), 2, 2, stage_cost="", terminal_cost="")
+    assert rc == 0, err

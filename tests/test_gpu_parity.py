@@ -1,0 +1,221 @@
+"""GPU parity: the CUDA path against the FP64 oracle and the reference's own
+kernels (golden vectors), pass by pass and end to end.
+
+Tolerances (FP32 device arithmetic against an FP64 restatement):
+  Philox words              bit-exact
+  standard normals          2e-6 absolute
+  per-sample costs          1e-5 relative
+  weights / ESS             1e-5 (weights absolute, ESS relative), given the
+                            same per-sample costs
+  u_next                    1e-4 absolute
+The end-to-end u_next comparisons use well-conditioned problems (small
+costs, or lambda large against the cost spread): with lambda = 1 and costs
+of order 1e3-1e4 the softmax amplifies the unavoidable FP32 rounding of the
+costs, so there the update is checked stage-isolated (oracle weights and
+update evaluated on the device's own costs).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from helpers import abs_err, backend_for, nonholonomic_example, oracle_problem, rel_err
+from mppi_metal_b200 import models
+from mppi_metal_b200.backend import Backend, device_philox
+
+pytestmark = pytest.mark.gpu
+
+TOL_NORMAL = 2e-6
+TOL_COST_REL = 1e-5
+TOL_WEIGHT = 1e-5
+TOL_U = 1e-4
+
+
+def test_device_philox_matches_reference_words(golden):
+    g = golden("philox_ref.npz")
+    words = device_philox(g["ctr0"], g["ctr1"], g["key"])
+    assert np.array_equal(words, g["words"])
+
+
+def test_device_philox_matches_oracle_large(oracle):
+    rng = np.random.default_rng(5)
+    c = rng.integers(0, 2 ** 32, size=(3, 1 << 16), dtype=np.uint64).astype(np.uint32)
+    assert np.array_equal(device_philox(c[0], c[1], c[2]), oracle.philox(c[0], c[1], c[2]))
+
+
+def test_noise_normals_match_oracle(oracle):
+    w = models.double_integrator_test(K=128, H=10)
+    b = backend_for(w, use_terminal=False)
+    p = oracle_problem(w, use_terminal=False)
+    nrm, eps = b.sample_noise(step=3, agent=0, k0=0, count=128)
+    worst = 0.0
+    for k in range(0, 128, 7):
+        n_o, e_o = oracle.noise(p, 3, w.seed, k)
+        worst = max(worst, abs_err(nrm[k], n_o), abs_err(eps[k], e_o))
+    assert worst < TOL_NORMAL
+
+
+def test_noise_per_agent_key_and_sigma(oracle):
+    # agent a draws with key seed + a and its own sigma row
+    w = models.unicycle_batch(seed=3, N=4, K=64, H=12, T=2)
+    b = backend_for(w, seed=11)
+    p = oracle_problem(w)
+    for agent in (0, 3):
+        sig = w.agent_sigma[agent]
+        nrm, eps = b.sample_noise(step=9, agent=agent, k0=5, count=4, sigma=sig)
+        for i in range(4):
+            n_o, e_o = oracle.noise(p, 9, 11 + agent, 5 + i, sigma=sig.astype(float))
+            assert abs_err(nrm[i], n_o) < TOL_NORMAL
+            assert abs_err(eps[i], e_o) < TOL_NORMAL
+
+
+@pytest.mark.parametrize("K,H", [(64, 10), (1000, 7), (4096, 30)])
+def test_rollout_costs_double_integrator(oracle, K, H):
+    w = models.double_integrator_test(K=K, H=H)
+    b = backend_for(w, use_terminal=False)
+    p = oracle_problem(w, use_terminal=False)
+    un = np.random.default_rng(K).uniform(-0.5, 0.5, H * 2).astype(np.float32)
+    b.dispatch_rollout(4, w.x0[0], un)
+    costs = b.last_costs()[0]
+    ref = oracle.rollout(p, 4, 0, w.x0[0], un)
+    assert rel_err(costs, ref) < TOL_COST_REL
+
+
+def test_rollout_costs_unicycle_control_cost(oracle):
+    w = models.unicycle_single(seed=2, K=2048, H=30)
+    b = backend_for(w)
+    p = oracle_problem(w)
+    un = np.random.default_rng(0).uniform(-0.5, 0.5, 60).astype(np.float32)
+    x0 = np.array([1.0, -2.0, 0.3, 0.0], np.float32)
+    b.dispatch_rollout(0, x0, un)
+    costs = b.last_costs()[0]
+    ref = oracle.rollout(p, 0, w.seed, x0, un)
+    assert rel_err(costs, ref) < TOL_COST_REL
+
+
+def test_weights_and_ess_on_device_costs(oracle):
+    w = models.unicycle_single(seed=1, K=4096, H=30)
+    w.lam = 20.0
+    b = backend_for(w)
+    un = np.zeros(60, np.float32)
+    _, diag = b.dispatch_rollout(0, w.x0[0], un)
+    costs = b.last_costs()[0]
+    weights = b.last_weights()[0]
+    w_o, d_o = oracle.weights(costs, w.lam)
+    assert abs_err(weights, w_o) < TOL_WEIGHT
+    assert abs(diag[0] - d_o[0]) <= 1e-6 * max(1.0, abs(d_o[0]))
+    assert rel_err(diag[1:], d_o[1:]) < TOL_WEIGHT
+
+
+def test_update_stage_isolated_lambda_one(oracle):
+    """Benchmark conditioning (lambda 1, costs ~1e3): oracle weights and
+    update evaluated on the device's own costs reproduce u_next."""
+    w = models.unicycle_batch(seed=0, N=1, K=4096, H=50, T=1)
+    b = backend_for(w)
+    b.bind_params(w.model_params, w.cost_params[0])
+    p = oracle_problem(w)
+    un = np.random.default_rng(1).uniform(-0.3, 0.3, 100).astype(np.float32)
+    u_out, diag = b.dispatch_rollout(2, w.x0[0], un)
+    costs = b.last_costs()[0]
+    w_o, d_o = oracle.weights(costs, w.lam)
+    u_o = oracle.update(p, 2, w.seed, w_o, un)
+    assert abs_err(u_out, u_o) < TOL_U
+    assert rel_err([diag[2]], [d_o[2]]) < TOL_WEIGHT
+
+
+def test_u_next_double_integrator_matches_oracle_and_reference(oracle, golden):
+    g = golden("step_double_integrator.npz")
+    w = models.double_integrator_test()
+    b = backend_for(w, use_terminal=False)
+    p = oracle_problem(w, use_terminal=False)
+    u_out, diag = b.dispatch_rollout(0, g["x0"], g["u_nom"])
+    o = oracle.step(p, 0, 0, g["x0"], g["u_nom"])
+    assert abs_err(u_out, o["u_out"]) < TOL_U
+    assert rel_err(b.last_costs()[0], o["costs"]) < TOL_COST_REL
+    assert rel_err(diag, o["diag"]) < TOL_WEIGHT
+    # the reference's own kernels (FP32, CPU) on the same inputs
+    assert abs_err(u_out, g["u_out"]) < TOL_U
+    assert rel_err(b.last_costs()[0], g["costs"]) < 1e-5
+    # behaviour pinned by tests/mppi_driver_tests.cpp:632-667
+    assert u_out[0] < 0 and u_out[1] < 0
+    assert diag[0] > 0 and diag[1] >= diag[0] and diag[2] > 0
+
+
+def test_u_next_nonholonomic_matches_oracle_and_reference(oracle, golden):
+    g = golden("step_nonholonomic.npz")
+    w = nonholonomic_example()
+    w.seed = int(g["seed"])
+    b = backend_for(w)
+    p = oracle_problem(w)
+    u_out, diag = b.dispatch_rollout(int(g["step"]), g["x0"], g["u_nom"])
+    o = oracle.step(p, int(g["step"]), int(g["seed"]), g["x0"], g["u_nom"])
+    assert rel_err(b.last_costs()[0], o["costs"]) < TOL_COST_REL
+    assert abs_err(u_out, o["u_out"]) < TOL_U
+    assert abs_err(u_out, g["u_out"]) < TOL_U
+
+
+def test_u_next_unicycle_matches_reference_golden(oracle, golden):
+    g = golden("step_unicycle.npz")
+    w = models.unicycle_single(seed=0, K=int(g["K"]), H=int(g["H"]))
+    w.lam = float(g["lam"])
+    w.control_cost = False  # the reference has no control-cost term
+    b = backend_for(w)
+    u_out, diag = b.dispatch_rollout(0, g["x0"], g["u_nom"])
+    assert rel_err(b.last_costs()[0], g["costs"]) < 1e-5
+    assert abs_err(u_out, g["u_out"]) < TOL_U
+    o = oracle.step(oracle_problem(w), 0, 0, g["x0"], g["u_nom"])
+    assert abs_err(u_out, o["u_out"]) < TOL_U
+
+
+def test_same_seed_is_bit_identical():
+    w = models.unicycle_single(seed=4, K=4096, H=30)
+    a = backend_for(w)
+    b = backend_for(w)
+    un = np.zeros(60, np.float32)
+    ua, da = a.dispatch_rollout(5, w.x0[0], un)
+    ub, db = b.dispatch_rollout(5, w.x0[0], un)
+    assert np.array_equal(ua, ub) and np.array_equal(da, db)
+    assert np.array_equal(a.last_costs(), b.last_costs())
+
+
+def test_simulate_matches_oracle_closed_loop(oracle, golden):
+    g = golden("step_double_integrator.npz")
+    w = models.double_integrator_test()
+    b = backend_for(w, use_terminal=False)
+    p = oracle_problem(w, use_terminal=False)
+    r = b.simulate(5, 0, g["x0"], np.zeros(20, np.float32))
+    o = oracle.simulate(p, 5, 0, 0, g["x0"], np.zeros(20))
+    assert abs_err(r["states"], o["states"]) < TOL_U
+    assert abs_err(r["controls"], o["controls"]) < TOL_U
+    assert abs_err(r["costs"], o["costs"]) < TOL_U * max(1.0, float(np.max(o["costs"])))
+    assert abs_err(r["controls"], g["sim_controls"]) < TOL_U
+    assert abs_err(r["states"], g["sim_states"]) < TOL_U
+
+
+def test_simulate_batch_matches_oracle(oracle, golden):
+    g = golden("step_double_integrator.npz")
+    w = models.double_integrator_test()
+    b = backend_for(w, use_terminal=False)
+    p = oracle_problem(w, use_terminal=False)
+    x0 = g["batch_x0"]
+    r = b.simulate_batch(4, 5, 0, x0)
+    o = oracle.simulate_batch(p, 4, 5, 0, 0, x0)
+    assert abs_err(r["states"], o["states"]) < TOL_U
+    assert abs_err(r["controls"], o["controls"]) < TOL_U
+    assert abs_err(r["terminal"], o["terminal"]) < TOL_U
+    assert abs_err(r["controls"], g["batch_controls"]) < TOL_U
+    assert abs_err(r["terminal"], g["batch_terminal"]) < TOL_U
+
+
+def test_batch_per_agent_params_match_oracle(oracle):
+    w = models.unicycle_batch(seed=7, N=6, K=512, H=20, T=3)
+    w.lam = 200.0
+    b = backend_for(w)
+    p = oracle_problem(w)
+    r = b.simulate_batch(w.num_agents, w.num_steps, 0, w.x0, cost_params=w.cost_params_packed,
+                         cost_stride=w.cost_stride, sigma=w.agent_sigma)
+    o = oracle.simulate_batch(p, w.num_agents, w.num_steps, 0, w.seed, w.x0,
+                              cost_params_packed=w.cost_params_packed, cost_stride=w.cost_stride,
+                              sigma_packed=w.agent_sigma.astype(float))
+    assert abs_err(r["controls"], o["controls"]) < TOL_U
+    assert abs_err(r["states"], o["states"]) < TOL_U
