@@ -1,0 +1,421 @@
+"""MPPI rollout throughput on B200 — one JSON line.
+
+Workload (the batched configuration): 256 independent kinematic-unicycle
+agents per GPU in one launch per pass, K = 4096 samples, horizon H = 50,
+FP32, each agent with its own seeded start, goal, 16 moving circular
+keep-out regions and per-dimension sigma U[0.2, 0.8]; 300 closed-loop
+control steps.  One benchmark step = one such closed loop
+(MPPIDriver::simulate_batch): 256 x 300 control steps of
+rollout -> weights -> update -> propagate & shift.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+value : rollout-steps/s over all ranks, inputs resident in HBM (device
+        time, CUDA events on the library's stream, max over ranks)
+e2e   : the same metric through the public C ABI call with host buffers
+        (host->device inputs and device->host histories inside the timing)
+--impl reference : the reference's own kernels (its Metal shader sources
+        compiled for the CPU, oracle/_ref) on the host cores, on a bounded
+        sample of the same workload.
+Multi-GPU: agents are independent, so ranks run disjoint agent sets with no
+collective on the data path (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "rollout-steps/s and control steps/s per B200 at matched closed-loop cost"
+AGENTS_PER_GPU = 256
+K_SAMPLES = 4096
+HORIZON = 50
+CLOSED_LOOP_STEPS = 300
+L2_FLUSH_BYTES = 256 << 20
+
+# Rollout-kernel instruction count per rollout-step (warp-level instructions
+# issued per sample-timestep / 32 lanes), from an ncu capture of the same
+# kernel build: profiles/rollout_unicycle_batch.txt.  Used only to express
+# the live-timed kernel against the SM issue-rate roofline.
+ROLLOUT_WARP_INST_PER_ROLLOUT_STEP = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["full", "kernels"], default="full",
+                    help="kernels: only launch the rollout and combine kernels of the "
+                         "workload `--iters` times each (small capture target for ncu)")
+    ap.add_argument("--iters", type=int, default=3)
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def workload_for_rank(rank: int):
+    from mppi_metal_b200 import models
+    return models.unicycle_batch(seed=1000 + rank, N=AGENTS_PER_GPU, K=K_SAMPLES, H=HORIZON,
+                                 T=CLOSED_LOOP_STEPS)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.idx), "-lms", "100"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return False
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+        return False
+
+    def summary(self) -> dict:
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[5 + i].lower() == "active"})
+        loaded = [s for s in sm if s >= 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def physical_gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return int(ids[local_rank])
+    return local_rank
+
+
+# ---------------------------------------------------------------------------
+# the reference's CPU implementation, bounded sample
+# ---------------------------------------------------------------------------
+def reference_sample_run(w, agents: int, steps: int, nthreads: int):
+    """Runs `agents` x `steps` closed-loop control steps of the workload with
+    the reference's kernels on the CPU; returns (seconds, rollout-steps,
+    executed closed-loop cost of the sampled agents over those steps)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    from mppi_metal_b200 import models
+    ref = pyoracle.RefKernels("unicycle_obstacles")
+    p = pyoracle.Problem("unicycle_obstacles", w.state_dim, w.control_dim, w.horizon,
+                         w.sample_count, w.lam, w.sigma.astype(float), w.u_min.astype(float),
+                         w.u_max.astype(float), sigma_inv=w.sigma_inv.astype(float),
+                         model_params=w.model_params)
+    blobs = w.cost_params[:agents]
+    t0 = time.perf_counter()
+    r = ref.simulate_batch(p, agents, steps, 0, w.seed, w.x0[:agents],
+                           sigma_packed=w.agent_sigma[:agents],
+                           cost_params_packed=b"".join(blobs), cost_stride=w.cost_stride,
+                           model_params_packed=w.model_params, model_stride=0,
+                           nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    cost = models.unicycle_executed_cost(r["states"], r["controls"], r["terminal"], blobs)
+    return dt, agents * steps * w.sample_count * w.horizon, float(cost.mean())
+
+
+def choose_reference_sample(w, nthreads: int, target_s: float):
+    """Sizes the CPU sample (agents at full K and H, 2 closed-loop steps) so one
+    reference step takes about target_s seconds."""
+    dt, rs, _ = reference_sample_run(w, 1, 1, nthreads)
+    per_rs = dt / rs
+    agents = int(max(1, min(AGENTS_PER_GPU, target_s / (per_rs * w.sample_count * w.horizon * 2))))
+    return agents, 2
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = workload_for_rank(0)
+    nthreads = os.cpu_count() or 1
+    lib = ROOT / "oracle" / "_ref" / "libmppi_ref_unicycle_obstacles.so"
+    if not lib.exists():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref (the reference's kernels built for the CPU) is missing; "
+                          "build it with `make -C oracle ref` where the reference tree exists"}))
+        return 0
+    agents, steps = choose_reference_sample(w, nthreads, target_s=4.0)
+    for _ in range(args.warmup):
+        reference_sample_run(w, agents, steps, nthreads)
+    times, costs = [], []
+    rs = 0
+    for _ in range(args.steps):
+        dt, rs, c = reference_sample_run(w, agents, steps, nthreads)
+        times.append(dt)
+        costs.append(c)
+    total = sum(times)
+    value = rs * len(times) / total
+    sample = (f"{agents} of {AGENTS_PER_GPU} agents x {steps} of {CLOSED_LOOP_STEPS} closed-loop "
+              f"steps at full K={K_SAMPLES}, H={HORIZON} per step")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "rollout-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": config_block(),
+        "control_steps_per_s": value / (K_SAMPLES * HORIZON),
+        "closed_loop_cost": {"mean": float(np.mean(costs)), "agents": agents, "steps": steps},
+        "cpu_baseline": {"value": value, "unit": "rollout-steps/s", "cores": nthreads,
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "rollout-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def config_block():
+    return {
+        "workload": (f"unicycle_batch: {AGENTS_PER_GPU} agents per GPU, K={K_SAMPLES}, H={HORIZON}, "
+                     f"{CLOSED_LOOP_STEPS} closed-loop steps, 16 moving circular obstacles and "
+                     "per-dimension sigma U[0.2,0.8] per agent, lambda=1, dt=0.05"),
+        "agents_per_gpu": AGENTS_PER_GPU, "samples": K_SAMPLES, "horizon": HORIZON,
+        "closed_loop_steps": CLOSED_LOOP_STEPS,
+        "step": "one simulate_batch closed loop (300 control steps for every agent)",
+        "l2": "flushed between timed iterations (256 MiB device write)",
+        "parallelism": "agent-sharded replicas, no data-path collective",
+    }
+
+
+# ---------------------------------------------------------------------------
+# the B200 path
+# ---------------------------------------------------------------------------
+def run_b200(args):
+    import torch
+    rank, world, local_rank = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    from mppi_metal_b200 import driver as D
+    from mppi_metal_b200 import models
+    from mppi_metal_b200._lib import plugin_path
+    from mppi_metal_b200.backend import Backend
+
+    w = workload_for_rank(rank)
+    N, T = w.num_agents, w.num_steps
+    rs_per_step = N * w.sample_count * w.horizon * T  # rollout-steps per bench step (this rank)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- value: device-resident closed loop ---------------------------------
+    b = Backend(w.plugin, w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam, w.sigma,
+                w.u_min, w.u_max, sigma_inv=w.sigma_inv, control_cost=w.control_cost,
+                model_params_size=len(w.model_params), cost_params_size=w.cost_stride,
+                seed=w.seed)
+    b.bind_params(w.model_params, w.cost_params[0])
+    b.prepare(N, T, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+              sigma=w.agent_sigma)
+    for _ in range(args.warmup):
+        b.run(0)
+        b.last_run_ms()
+    times = []
+    barrier()
+    with ClockSampler(physical_gpu_index(local_rank)) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            b.run(0)
+            times.append(b.last_run_ms())
+    barrier()
+    total_ms = max_over_ranks(sum(times))
+    value = world * rs_per_step * args.steps / (total_ms / 1e3)
+
+    # ---- kernel-level timing for the roofline --------------------------------
+    rollout_ms, combine_ms = b.time_passes(20)
+    geom = b.launch_info()
+    b.close()
+
+    # ---- e2e: public API, host buffers ---------------------------------------
+    cfg = D.DriverConfig(w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam,
+                         D.ControlNoiseConfig(D.CovarianceForm.kDiagonal, w.sigma, w.sigma_inv, 2),
+                         D.ControlBounds(w.u_min, w.u_max, 2))
+    drv = D.MPPIDriver(cfg, D.DriverOptions(control_cost=w.control_cost))
+    err = D.ErrorRef()
+    spec = D.ModelPluginSpec(plugin_path(w.plugin),
+                             D.CallableNames("mppi_dynamics", "mppi_stage_cost",
+                                             "mppi_terminal_cost"),
+                             D.ParamLayout(len(w.model_params), 4, w.cost_stride, 4),
+                             D.RngConfig(w.seed))
+    assert drv.initialize(spec, err), err.value
+    assert drv.set_problem_params(D.ProblemParams(D.ByteView.of(w.model_params),
+                                                  D.ByteView.of(w.cost_params[0])), err), err.value
+    agent_params = D.BatchAgentParams(cost_params=w.cost_params_packed,
+                                      cost_params_stride=w.cost_stride, sigma=w.agent_sigma)
+    outs = D.BatchSimulationResults(np.zeros((T, N, w.state_dim), np.float32),
+                                    np.zeros((T, N, w.control_dim), np.float32),
+                                    np.zeros((T, N), np.float32),
+                                    np.zeros((N, w.state_dim), np.float32), N, T)
+    for _ in range(args.warmup):
+        assert drv.reset(None, err)
+        assert drv.simulate_batch(N, T, w.x0, outs, agent_params, err), err.value
+    e2e_times = []
+    barrier()
+    for _ in range(args.steps):
+        assert drv.reset(None, err)
+        t0 = time.perf_counter()
+        assert drv.simulate_batch(N, T, w.x0, outs, agent_params, err), err.value
+        e2e_times.append(time.perf_counter() - t0)
+    barrier()
+    e2e_total = max_over_ranks(sum(e2e_times))
+    # executed closed-loop cost of the last API call (from x0, step index 0)
+    cost = models.unicycle_executed_cost(outs.states_out, outs.controls_out,
+                                         outs.terminal_states_out, w.cost_params)
+    e2e_value = world * rs_per_step * args.steps / e2e_total
+    HM = w.horizon * w.control_dim
+    h2d = (N * w.state_dim + N * HM + 4) * 4 + N * ((w.cost_stride + 15) // 16 * 16) \
+        + N * w.control_dim * 4
+    d2h = (T * N * (w.state_dim + w.control_dim + 1) + N * w.state_dim) * 4
+
+    # ---- CPU baseline (rank 0, N = 1 only) ------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        lib = ROOT / "oracle" / "_ref" / "libmppi_ref_unicycle_obstacles.so"
+        if lib.exists():
+            nthreads = os.cpu_count() or 1
+            agents, steps = choose_reference_sample(w, nthreads, target_s=5.0)
+            dt, rs, c = reference_sample_run(w, agents, steps, nthreads)
+            # the GPU's executed cost on the same agents over the same steps
+            gpu_c = models.unicycle_executed_cost(
+                outs.states_out[:steps, :agents], outs.controls_out[:steps, :agents],
+                outs.states_out[steps, :agents], w.cost_params[:agents])
+            cpu = {"value": rs / dt, "unit": "rollout-steps/s", "cores": nthreads,
+                   "kind": "reference",
+                   "sample": f"{agents} agents x {steps} closed-loop steps at full K={K_SAMPLES}, "
+                             f"H={HORIZON} (reference kernels compiled for the CPU)",
+                   "closed_loop_cost_sample": c,
+                   "gpu_closed_loop_cost_same_sample": float(gpu_c.mean())}
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+
+    rollout_units = N * w.sample_count * w.horizon  # rollout-steps per rollout launch
+    roof = {"kernel": "mppi_rollout_b%d" % geom["block"], "bound": "issue",
+            "launch_ms": rollout_ms, "combine_launch_ms": combine_ms,
+            "rollout_steps_per_launch": rollout_units,
+            "traffic": None, "unit": "Gwarp-inst/s"}
+    clk = clocks.summary()
+    if ROLLOUT_WARP_INST_PER_ROLLOUT_STEP is not None:
+        achieved = ROLLOUT_WARP_INST_PER_ROLLOUT_STEP * rollout_units / (rollout_ms / 1e3) / 1e9
+        mhz = clk.get("sm_mhz") or 1965.0
+        peak = 148 * 4 * mhz * 1e6 / 1e9
+        roof.update({"achieved": achieved, "peak": peak, "frac": achieved / peak,
+                     "peak_basis": f"148 SMs x 4 warp-inst/clk x {mhz:.0f} MHz (sampled)"})
+    line = {
+        "metric": METRIC, "value": value, "unit": "rollout-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "data": "synthetic (seeded PCG64 workload generator, mppi_metal_b200/models.py)",
+        "config": config_block(),
+        "control_steps_per_s": value / (w.sample_count * w.horizon),
+        "closed_loop_cost": {"mean": float(cost.mean()), "agents": N,
+                             "mean_first_agents": float(cost[:8].mean())},
+        "e2e": {"value": e2e_value, "unit": "rollout-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e2e_total / args.steps},
+        "gpu_launches": 2 * T * args.steps,
+        "launch_geometry": geom,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_kernels_only(args):
+    """Prepares the workload and launches the rollout and combine kernels
+    `iters` times each (no closed loop, no host copies in between)."""
+    from mppi_metal_b200.backend import Backend
+    w = workload_for_rank(0)
+    b = Backend(w.plugin, w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam, w.sigma,
+                w.u_min, w.u_max, sigma_inv=w.sigma_inv, control_cost=w.control_cost,
+                model_params_size=len(w.model_params), cost_params_size=w.cost_stride,
+                seed=w.seed)
+    b.bind_params(w.model_params, w.cost_params[0])
+    b.prepare(w.num_agents, 1, w.x0, cost_params=w.cost_params_packed,
+              cost_stride=w.cost_stride, sigma=w.agent_sigma)
+    r, c = b.time_passes(args.iters)
+    print(json.dumps({"mode": "kernels", "rollout_ms": r, "combine_ms": c,
+                      "geometry": b.launch_info()}))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    if args.mode == "kernels":
+        return run_kernels_only(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -137,6 +137,9 @@ int mppi_backend_batch_prepare(mppi_backend* b, uint32_t num_agents, uint32_t nu
                                uint32_t want_terminal, char* err, size_t err_len);
 int mppi_backend_batch_run(mppi_backend* b, uint64_t start_step_index, char* err,
                            size_t err_len);
+/* Device time (ms) of the last batch_run: CUDA events recorded on the
+ * backend's stream around the closed-loop graph (waits for it to finish). */
+int mppi_backend_last_run_ms(mppi_backend* b, float* ms, char* err, size_t err_len);
 int mppi_backend_batch_fetch(mppi_backend* b, float* states_out, float* controls_out,
                              float* costs_out, float* terminal_states_out, float* x_out,
                              float* u_nominal_out, char* err, size_t err_len);

@@ -100,6 +100,7 @@ SIGNATURES = {
                                                   ctypes.POINTER(BatchAgents), c_u32, c_u32,
                                                   c_u32, c_u32] + _ERR),
     "mppi_backend_batch_run": (ctypes.c_int, [c_ptr, c_u64] + _ERR),
+    "mppi_backend_last_run_ms": (ctypes.c_int, [c_ptr, ctypes.POINTER(c_f32)] + _ERR),
     "mppi_backend_batch_fetch": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr,
                                                 c_ptr] + _ERR),
     "mppi_backend_last_costs": (ctypes.c_int, [c_ptr, c_u32, c_u32, c_ptr] + _ERR),

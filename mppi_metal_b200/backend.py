@@ -145,6 +145,13 @@ class Backend:
         eb = _lib.err_buf()
         _check(self.lib.mppi_backend_batch_run(self.h, start_step, eb, len(eb)), eb)
 
+    def last_run_ms(self) -> float:
+        """Device time of the last run() (CUDA events on the backend stream)."""
+        ms = ctypes.c_float()
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_last_run_ms(self.h, ctypes.byref(ms), eb, len(eb)), eb)
+        return ms.value
+
     def fetch(self):
         N, T = self.N, self.T
         ws, wc, wk, wt = self._flags

@@ -169,6 +169,7 @@ struct mppi_backend {
   uint64_t generation = 0;  // bumps whenever a device buffer is reallocated
 
   PinnedBuf h_up, h_down;
+  bool run_timed = false;  // ev0 / ev1 bracket the last closed-loop run
 
   // ---- closed-loop graph cache ----
   cudaGraphExec_t graph = nullptr;
@@ -770,7 +771,22 @@ int mppi_backend_batch_run(mppi_backend* b, uint64_t start_step, char* err, size
   CK(cudaStreamSynchronize(b->stream));  // the pinned word may still feed a copy
   up[0] = (uint32_t)start_step;
   CK(cudaMemcpyAsync(b->io(), up, 4, cudaMemcpyHostToDevice, b->stream));
-  return enqueue_closed_loop(b, err, err_len);
+  CK(cudaEventRecord(b->ev0, b->stream));
+  if (int rc = enqueue_closed_loop(b, err, err_len)) return rc;
+  CK(cudaEventRecord(b->ev1, b->stream));
+  b->run_timed = true;
+  return MPPI_OK;
+}
+
+int mppi_backend_last_run_ms(mppi_backend* b, float* ms, char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (!b->run_timed || !ms) {
+    set_err(err, err_len, "no closed-loop run has been issued.");
+    return MPPI_ERR_INVALID;
+  }
+  CK(cudaEventSynchronize(b->ev1));
+  CK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+  return MPPI_OK;
 }
 
 int mppi_backend_batch_fetch(mppi_backend* b, float* states, float* controls, float* costs,

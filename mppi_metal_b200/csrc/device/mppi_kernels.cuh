@@ -237,50 +237,73 @@ __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   __syncthreads();
 
   // ---- rollout: noise -> clamp -> dynamics -> stage cost; terminal cost ----
+  // Time is processed in chunks of TC steps (the whole horizon when the
+  // staging buffer holds it).  Phase A draws the chunk's noise into this
+  // thread's own staging column: Philox chains of different steps are
+  // independent, so they overlap.  Phase B runs the state recurrence, reading
+  // the noise back.  No thread touches another's column until the weighted
+  // sums, so neither phase needs a barrier.
   float J = 0.0f;
+  __align__(16) float st[kNPad];
   if (active) {
-    __align__(16) float st[kNPad];
     const float* xg = a.x + (size_t)agent * kN;
 #pragma unroll
     for (int d = 0; d < kN; ++d) st[d] = xg[d];
+  }
 #pragma unroll
-    for (int d = kN; d < kNPad; ++d) st[d] = 0.0f;
-    for (uint32_t t = 0; t < H; ++t) {
-      float n[2 * kP], eps[kM], u[kM];
-      sample_noise(step, key, k, H, t, sig, n, eps);
+  for (int d = kN; d < kNPad; ++d) st[d] = 0.0f;
+  const uint32_t TC = staged ? H : a.stage_rows / kM;
+  for (uint32_t t0 = 0; t0 < H; t0 += TC) {
+    const uint32_t t1 = min(H, t0 + TC);
+    const uint32_t row0 = staged ? 0u : t0;  // staging row of step t is (t - row0) * m + d
+#pragma unroll 2
+    for (uint32_t t = t0; t < t1; ++t) {
+      float n[2 * kP], eps[kM];
+      if (active) {
+        sample_noise(step, key, k, H, t, sig, n, eps);
+      } else {
 #pragma unroll
-      for (int d = 0; d < kM; ++d) u[d] = clampf(un_s[t * kM + d] + eps[d], lo[d], hi[d]);
+        for (int d = 0; d < kM; ++d) eps[d] = 0.0f;
+      }
+#pragma unroll
+      for (int d = 0; d < kM; ++d) stage_s[(size_t)((t - row0) * kM + d) * BLOCK + tid] = eps[d];
+    }
+    if (active) {
+      for (uint32_t t = t0; t < t1; ++t) {
+        float eps[kM], u[kM];
+#pragma unroll
+        for (int d = 0; d < kM; ++d) {
+          eps[d] = stage_s[(size_t)((t - row0) * kM + d) * BLOCK + tid];
+          u[d] = clampf(un_s[t * kM + d] + eps[d], lo[d], hi[d]);
+        }
 #if MPPI_CONTROL_COST
-      {
-        float cc = 0.0f;
+        {
+          float cc = 0.0f;
 #if MPPI_COV_FULL
 #pragma unroll
-        for (int i = 0; i < kM; ++i) {
-          float r = 0.0f;
+          for (int i = 0; i < kM; ++i) {
+            float r = 0.0f;
 #pragma unroll
-          for (int j = 0; j < kM; ++j) r = fmaf(sinv[i * kM + j], eps[j], r);
-          cc = fmaf(un_s[t * kM + i], r, cc);
-        }
+            for (int j = 0; j < kM; ++j) r = fmaf(sinv[i * kM + j], eps[j], r);
+            cc = fmaf(un_s[t * kM + i], r, cc);
+          }
 #else
 #pragma unroll
-        for (int i = 0; i < kM; ++i) cc = fmaf(un_s[t * kM + i], sinv[i] * eps[i], cc);
+          for (int i = 0; i < kM; ++i) cc = fmaf(un_s[t * kM + i], sinv[i] * eps[i], cc);
 #endif
-        J = fmaf(a.lambda, cc, J);
-      }
+          J = fmaf(a.lambda, cc, J);
+        }
 #endif
-      if (staged) {
-#pragma unroll
-        for (int d = 0; d < kM; ++d) stage_s[(size_t)(t * kM + d) * BLOCK + tid] = eps[d];
+        MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u, mp,
+                         make_uint2(step, mppi_dyn_ctr(k, H, kP, t)), key);
+        J += MPPI_STAGE_COST_FN(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u,
+                                mp, cp);
       }
-      MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u, mp,
-                       make_uint2(step, mppi_dyn_ctr(k, H, kP, t)), key);
-      J += MPPI_STAGE_COST_FN(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u,
-                              mp, cp);
     }
+  }
+  if (active) {
     J += MPPI_TERMINAL_COST_FN(reinterpret_cast<TermStateT>(reinterpret_cast<void*>(st)), mp, cp);
     if (a.costs) a.costs[(size_t)agent * K + k] = J;
-  } else if (staged) {
-    for (uint32_t j = 0; j < HM; ++j) stage_s[(size_t)j * BLOCK + tid] = 0.0f;
   }
 
   // ---- CTA softmax statistics against the CTA minimum ----
@@ -428,8 +451,12 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
 
 }  // namespace mppi
 
+// Residency is bounded by the noise staging buffer (H*m floats per thread),
+// not by registers: 512 resident threads per SM lets the compiler use up to
+// 128 registers for instruction-level parallelism.
 #define MPPI_ROLLOUT_ENTRY(B)                                                      \
-  extern "C" __global__ void __launch_bounds__(B) mppi_rollout_b##B(const MppiRolloutArgs a) { \
+  extern "C" __global__ void __launch_bounds__(B, 512 / B)                        \
+      mppi_rollout_b##B(const MppiRolloutArgs a) {                                \
     mppi::rollout_body<B>(a);                                                     \
   }
 MPPI_ROLLOUT_ENTRY(64)

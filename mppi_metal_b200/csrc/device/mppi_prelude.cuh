@@ -119,6 +119,15 @@ __device__ __forceinline__ float2 mppi_box_muller(uint2 w) {
   return make_float2(r * c, r * s);
 }
 
+// Square root by the SM's approximate square-root instruction (PTX
+// sqrt.approx.f32, relative error of order 2^-23): one instruction, exact
+// zero at zero.  For plugin cost terms where a few ulps do not matter.
+__device__ __forceinline__ float mppi_sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // Reference-compatible spellings for plugins ported from MSL
 // (examples/wez_environment_batch/wez_environment.metal:166-173 draws with
 // philox2x32_10 / uint_to_01 inside its dynamics).

@@ -169,3 +169,30 @@ def double_integrator_test(K: int = 64, H: int = 10) -> Workload:
                     K, 1.0, sigma, sigma.copy(), -np.ones(2, np.float32),
                     np.ones(2, np.float32), 1, 5, np.array([[1.0, 1.0, 0.0, 0.0]], np.float32),
                     b"", [], None)
+
+
+def unicycle_executed_cost(states: np.ndarray, controls: np.ndarray, terminal: np.ndarray,
+                           cost_blobs: list[bytes]) -> np.ndarray:
+    """Closed-loop cost of executed unicycle trajectories, per agent.
+
+    states [T][N][4] are the pre-step states, controls [T][N][2] the applied
+    u*[0], terminal [N][4] the state after the last step.  The cost is the
+    model's stage cost (goal distance + obstacle penetration at the model
+    time) summed over the visited states x_1..x_T, plus the terminal cost of
+    x_T -- what the controller actually incurred, not a sampled rollout cost.
+    """
+    T, N, _ = states.shape
+    nxt = np.concatenate([states[1:], terminal[None]], axis=0).astype(np.float64)  # x_1..x_T
+    out = np.zeros(N)
+    for a in range(N):
+        c = UnicycleCostParams.from_buffer_copy(cost_blobs[a])
+        n_obs = min(int(c.num_obs), UNICYCLE_MAX_OBS)
+        p = nxt[:, a, :]
+        goal = c.w_goal * ((p[:, 0] - c.goal_x) ** 2 + (p[:, 1] - c.goal_y) ** 2)
+        t = p[:, 3:4]
+        cx = np.array(c.obs_cx[:n_obs]) + np.array(c.obs_vx[:n_obs]) * t
+        cy = np.array(c.obs_cy[:n_obs]) + np.array(c.obs_vy[:n_obs]) * t
+        d = np.sqrt((p[:, 0:1] - cx) ** 2 + (p[:, 1:2] - cy) ** 2)
+        pen = np.maximum(np.array(c.obs_r[:n_obs]) - d, 0.0).sum(axis=1)
+        out[a] = float(np.sum(goal + c.w_obs * pen) + c.w_terminal * goal[-1])
+    return out
