@@ -47,7 +47,11 @@ L2_FLUSH_BYTES = 256 << 20
 # issued per sample-timestep / 32 lanes), from an ncu capture of the same
 # kernel build: profiles/rollout_unicycle_batch.txt.  Used only to express
 # the live-timed kernel against the SM issue-rate roofline.
-ROLLOUT_WARP_INST_PER_ROLLOUT_STEP = None
+ROLLOUT_WARP_INST_PER_ROLLOUT_STEP = 732651532 / 52428800  # 13.97
+
+
+# DRAM bytes (read + write) per rollout launch of the same capture.
+ROLLOUT_DRAM_BYTES_PER_LAUNCH = 240128
 
 
 def parse():
@@ -359,7 +363,10 @@ def run_b200(args):
     roof = {"kernel": "mppi_rollout_b%d" % geom["block"], "bound": "issue",
             "launch_ms": rollout_ms, "combine_launch_ms": combine_ms,
             "rollout_steps_per_launch": rollout_units,
-            "traffic": None, "unit": "Gwarp-inst/s"}
+            "traffic": ROLLOUT_DRAM_BYTES_PER_LAUNCH, "unit": "Gwarp-inst/s",
+            "note": "issue-bound kernel (no HBM or tensor-core bound applies): "
+                    "achieved = ncu-counted warp-instructions per rollout-step x "
+                    "rollout-steps per launch / live CUDA-event launch time"}
     clk = clocks.summary()
     if ROLLOUT_WARP_INST_PER_ROLLOUT_STEP is not None:
         achieved = ROLLOUT_WARP_INST_PER_ROLLOUT_STEP * rollout_units / (rollout_ms / 1e3) / 1e9

@@ -52,6 +52,10 @@ def build_oracle() -> None:
     ref_root = Path(os.environ.get("MPPI_REF_ROOT", "/root/reference"))
     if (ref_root / "shaders" / "mppi_rollout.metal").exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={ref_root}"], check=True)
+        product = HERE.parent / "mppi_metal_b200" / "lib" / "libmppi_b200.so"
+        if product.exists():
+            subprocess.run(["make", "-s", "-C", str(HERE), "ref_suite", f"REF_ROOT={ref_root}"],
+                           check=True)
 
 
 def _ptr(a: np.ndarray | None):
