@@ -171,6 +171,27 @@ int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
 int mppi_device_philox(uint64_t n, const uint32_t* ctr0, const uint32_t* ctr1,
                        const uint32_t* key, uint32_t* out_pairs, char* err, size_t err_len);
 
+/* ---- allocation-free control step --------------------------------------
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory once running (a fixed-rate control loop, where cudaMalloc /
+ * cudaFree can stall and synchronise the device; an application whose device
+ * memory is owned and budgeted by another allocator): one control step for
+ * one agent, like mppi_backend_dispatch_rollout, but x0 [state_dim],
+ * u_nominal [horizon * control_dim], the two parameter blobs (NULL = zeros),
+ * u_out [horizon * control_dim] and diag3 [3] are DEVICE pointers the caller
+ * owns, and the step's temporary data lives in one static device array of
+ * MPPI_NOALLOC_SCRATCH_BYTES that every GPU loading this library keeps
+ * until exit.  The call allocates nothing, blocks until the step is done,
+ * and rejects problems whose scratch (about 4 * (sample_count + blocks *
+ * (4 + horizon * control_dim)) bytes) exceeds the array.  The first call on
+ * a device looks the array's device address up (make it before any stream
+ * capture).  Calls share the array: calls that overlap on the GPU race. */
+#define MPPI_NOALLOC_SCRATCH_BYTES (2u << 20)
+int mppi_backend_dispatch_rollout_noalloc(mppi_backend* b, uint64_t step_index, const float* x0,
+                                          const float* u_nominal, const void* model_params,
+                                          const void* cost_params, float* u_out, float* diag3,
+                                          char* err, size_t err_len);
+
 /* Compiles a plugin with the library kernels for sm_100a without loading
  * the result (needs no GPU).  log receives the NVRTC log, including ptxas's
  * register / shared-memory / spill report for every kernel. */

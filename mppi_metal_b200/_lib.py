@@ -111,6 +111,8 @@ SIGNATURES = {
                                                 ctypes.POINTER(c_f32)] + _ERR),
     "mppi_backend_launch_info": (ctypes.c_int, [c_ptr] + [ctypes.POINTER(c_u32)] * 5),
     "mppi_device_philox": (ctypes.c_int, [c_u64, c_ptr, c_ptr, c_ptr, c_ptr] + _ERR),
+    "mppi_backend_dispatch_rollout_noalloc": (ctypes.c_int, [c_ptr, c_u64, c_ptr, c_ptr, c_ptr,
+                                                             c_ptr, c_ptr, c_ptr] + _ERR),
     "mppi_compile_check": (ctypes.c_int, [ctypes.POINTER(BackendPlugin),
                                           ctypes.POINTER(BackendConfig), ctypes.c_char_p,
                                           c_size] + _ERR),

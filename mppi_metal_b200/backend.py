@@ -105,6 +105,14 @@ class Backend:
         self.N, self.T = 1, 0
         return u_out, diag
 
+    def dispatch_rollout_noalloc(self, step: int, d_x0: int, d_u_nom: int, d_model_params,
+                                 d_cost_params, d_u_out: int, d_diag: int) -> None:
+        """Allocation-free step on caller-owned DEVICE buffers (raw addresses)."""
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_dispatch_rollout_noalloc(
+            self.h, step, d_x0, d_u_nom, d_model_params, d_cost_params, d_u_out, d_diag, eb,
+            len(eb)), eb)
+
     def simulate(self, T: int, start_step: int, x0, u_nom):
         x0, u_nom = _f32(x0), _f32(u_nom)
         st = np.zeros((T, self.n), np.float32)

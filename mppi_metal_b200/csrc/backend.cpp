@@ -1019,3 +1019,120 @@ int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Single-agent step on caller memory + a caller scratch area (used by the
+// allocation-free entry point in csrc/noalloc.cu).  Scratch layout (floats):
+//   [0, 16)              zero block: the step_base word reads 0, the step index
+//                        travels in step_local
+//   [16, 16 + K)         per-sample costs
+//   [.., + nblk * ps)    per-CTA partial records
+//   [.., + 4)            combine statistics
+// ---------------------------------------------------------------------------
+#include "step_scratch.hpp"
+
+namespace mppi_b200 {
+
+size_t step_scratch_floats(const mppi_backend* b) {
+  const LaunchGeom g = choose_geometry(b);
+  return 16 + pad4(b->K) + (size_t)g.nblk * g.pstride + 4;
+}
+
+int backend_device(const mppi_backend* b) { return b->device; }
+cudaStream_t backend_stream(const mppi_backend* b) { return b->stream; }
+bool backend_initialized(const mppi_backend* b) { return b != nullptr && b->initialized; }
+
+int launch_step_with_scratch(mppi_backend* b, uint64_t step_index, const float* x0,
+                             const float* u_nominal, const void* model_params,
+                             const void* cost_params, float* u_out, float* diag3,
+                             float* scratch, size_t scratch_floats, cudaStream_t stream,
+                             std::string* error) {
+  char ebuf[512] = {0};
+  char* err = ebuf;
+  const size_t err_len = sizeof(ebuf);
+  auto fail = [&](int rc) {
+    *error = ebuf;
+    return rc;
+  };
+  const LaunchGeom g = choose_geometry(b);
+  const size_t need = step_scratch_floats(b);
+  if (scratch_floats < need) {
+    *error = "scratch too small";
+    return MPPI_ERR_INVALID;
+  }
+  float* zero = scratch;
+  float* costs = scratch + 16;
+  float* partials = costs + pad4(b->K);
+  float* stats = partials + (size_t)g.nblk * g.pstride;
+  const void* rk = (const void*)b->mod->rollout[g.variant];
+  if (g.smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(rk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)g.smem);
+    if (e != cudaSuccess) {
+      set_err(err, err_len, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+      return fail(MPPI_ERR_CUDA);
+    }
+  }
+  cudaError_t e = cudaMemsetAsync(zero, 0, 16 * sizeof(float), stream);
+  if (e != cudaSuccess) {
+    set_err(err, err_len, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+    return fail(MPPI_ERR_CUDA);
+  }
+  MppiRolloutArgs a{};
+  a.num_agents = 1;
+  a.K = b->K;
+  a.H = b->H;
+  a.nblk = g.nblk;
+  a.stage_rows = g.stage_rows;
+  a.seed = b->seed;
+  a.step_local = (uint32_t)step_index;
+  a.pstride = g.pstride;
+  a.lambda = b->lambda;
+  a.step_base = reinterpret_cast<const uint32_t*>(zero);
+  a.x = x0;
+  a.u_nom = u_nominal;
+  a.sigma = b->c_sigma();
+  a.sigma_inv = b->c_sigma_inv();
+  a.u_min = b->c_umin();
+  a.u_max = b->c_umax();
+  a.model_params = model_params ? static_cast<const uint8_t*>(model_params)
+                                : b->d_zero.as<uint8_t>();
+  a.cost_params = cost_params ? static_cast<const uint8_t*>(cost_params)
+                              : b->d_zero.as<uint8_t>();
+  a.costs = costs;
+  a.partials = partials;
+  void* ra[] = {&a};
+  e = cudaLaunchKernel(rk, dim3(g.nblk, 1), dim3(g.block), ra, g.smem, stream);
+  if (e != cudaSuccess) {
+    set_err(err, err_len, std::string("rollout launch: ") + cudaGetErrorString(e));
+    return fail(MPPI_ERR_CUDA);
+  }
+  MppiCombineArgs c{};
+  c.num_agents = 1;
+  c.K = b->K;
+  c.H = b->H;
+  c.nblk = g.nblk;
+  c.pstride = g.pstride;
+  c.step_local = (uint32_t)step_index;
+  c.lambda = b->lambda;
+  c.propagate = 0;
+  c.step_base = reinterpret_cast<const uint32_t*>(zero);
+  c.partials = partials;
+  c.u_min = b->c_umin();
+  c.u_max = b->c_umax();
+  c.model_params = a.model_params;
+  c.u_nom = const_cast<float*>(u_nominal);  // read only: propagate == 0
+  c.u_out = u_out;
+  c.diag = diag3;
+  c.stats = stats;
+  void* ca[] = {&c};
+  e = cudaLaunchKernel((const void*)b->mod->combine, dim3(1), dim3(256), ca,
+                       (pad4(g.nblk) + pad4(b->HM())) * 4, stream);
+  if (e != cudaSuccess) {
+    set_err(err, err_len, std::string("combine launch: ") + cudaGetErrorString(e));
+    return fail(MPPI_ERR_CUDA);
+  }
+  return MPPI_OK;
+}
+
+}  // namespace mppi_b200
