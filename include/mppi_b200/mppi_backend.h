@@ -70,6 +70,14 @@ typedef struct mppi_batch_agents {
   const void* cost_params;
   uint64_t cost_params_stride;
   const float* sigma;           /* [N][control_dim] or [N][control_dim^2] */
+  /* Uneven batches: per-agent sample count (1..sample_count) and horizon
+   * (1..horizon); NULL = the configured value for every agent.  Nominals
+   * keep the stride horizon * control_dim.  An uneven batch runs as one
+   * persistent launch per pass whose grid size and noise staging are chosen
+   * by timing candidates on the first run of each shape (the choice does not
+   * change any result bit). */
+  const uint32_t* sample_counts;
+  const uint32_t* horizons;
 } mppi_batch_agents;
 
 /* Constructs an empty backend (MetalBackend::MetalBackend, metal_backend.mm:215). */
@@ -166,6 +174,13 @@ int mppi_backend_time_passes(mppi_backend* b, uint32_t iters, float* rollout_ms,
 int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
                              uint32_t* stage_rows, uint32_t* smem_bytes,
                              uint32_t* kernels_per_step);
+
+/* Autotuner result for the prepared uneven batch: persistent grid size
+ * (0 = one CTA per work item), number of work items, noise staging rows and
+ * the tuned rollout time (ms).  Returns MPPI_ERR_INVALID for uniform batches
+ * or before the first run. */
+int mppi_backend_tuning_info(mppi_backend* b, uint32_t* grid, uint32_t* num_work,
+                             uint32_t* stage_rows, float* rollout_ms);
 
 /* Philox-2x32-10 words computed on the device (known-answer tests). */
 int mppi_device_philox(uint64_t n, const uint32_t* ctr0, const uint32_t* ctr1,

@@ -85,7 +85,7 @@ int mppi_driver_simulate(mppi_driver* d, uint32_t num_steps, const float* x0, ui
                          size_t err_len);
 
 /* MPPIDriver::simulate_batch (shared params) and its per-agent overload
- * (any of the per-agent pointers may be NULL). */
+ * (BatchAgentParams; any of the per-agent pointers may be NULL). */
 int mppi_driver_simulate_batch(mppi_driver* d, uint32_t num_agents, uint32_t num_steps,
                                const float* x0_packed, float* states_out, float* controls_out,
                                float* costs_out, float* terminal_states_out,
@@ -95,6 +95,7 @@ int mppi_driver_simulate_batch_agents(mppi_driver* d, uint32_t num_agents, uint3
                                       const float* x0_packed, const void* model_params,
                                       size_t model_params_stride, const void* cost_params,
                                       size_t cost_params_stride, const float* sigma,
+                                      const uint32_t* sample_counts, const uint32_t* horizons,
                                       float* states_out, float* controls_out,
                                       float* costs_out, float* terminal_states_out,
                                       uint32_t results_num_agents,

@@ -182,6 +182,13 @@ struct BatchAgentParams {
 	const void* cost_params = nullptr;
 	size_t cost_params_stride = 0;
 	const float* sigma = nullptr;
+	// Uneven batches: per-agent sample count (1..sample_count) and horizon
+	// (1..horizon).  Null = the DriverConfig value for every agent.  An uneven
+	// batch runs as one persistent launch per pass; its grid size and noise
+	// staging are tuned on the first run of each shape without changing any
+	// result.
+	const uint32_t* sample_counts = nullptr;
+	const uint32_t* horizons = nullptr;
 };
 
 }  // namespace mppi_metal

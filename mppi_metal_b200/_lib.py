@@ -54,6 +54,7 @@ class BatchAgents(ctypes.Structure):
     _fields_ = [
         ("model_params", c_ptr), ("model_params_stride", c_u64),
         ("cost_params", c_ptr), ("cost_params_stride", c_u64), ("sigma", c_ptr),
+        ("sample_counts", c_ptr), ("horizons", c_ptr),
     ]
 
 
@@ -110,6 +111,8 @@ SIGNATURES = {
     "mppi_backend_time_passes": (ctypes.c_int, [c_ptr, c_u32, ctypes.POINTER(c_f32),
                                                 ctypes.POINTER(c_f32)] + _ERR),
     "mppi_backend_launch_info": (ctypes.c_int, [c_ptr] + [ctypes.POINTER(c_u32)] * 5),
+    "mppi_backend_tuning_info": (ctypes.c_int, [c_ptr] + [ctypes.POINTER(c_u32)] * 3
+                                 + [ctypes.POINTER(c_f32)]),
     "mppi_device_philox": (ctypes.c_int, [c_u64, c_ptr, c_ptr, c_ptr, c_ptr] + _ERR),
     "mppi_backend_dispatch_rollout_noalloc": (ctypes.c_int, [c_ptr, c_u64, c_ptr, c_ptr, c_ptr,
                                                              c_ptr, c_ptr, c_ptr] + _ERR),
@@ -133,8 +136,8 @@ SIGNATURES = {
                                                   c_ptr, c_ptr, c_u32, c_u32] + _ERR),
     "mppi_driver_simulate_batch_agents": (ctypes.c_int, [c_ptr, c_u32, c_u32, c_ptr, c_ptr,
                                                          c_size, c_ptr, c_size, c_ptr, c_ptr,
-                                                         c_ptr, c_ptr, c_ptr, c_u32, c_u32]
-                                          + _ERR),
+                                                         c_ptr, c_ptr, c_ptr, c_ptr, c_ptr,
+                                                         c_u32, c_u32] + _ERR),
 }
 
 _lib = None

@@ -126,21 +126,26 @@ class Backend:
         return dict(states=st, controls=ct, costs=co)
 
     def _agents(self, cost_params=None, cost_stride=0, model_params=None, model_stride=0,
-                sigma=None):
-        if cost_params is None and model_params is None and sigma is None:
+                sigma=None, sample_counts=None, horizons=None):
+        if cost_params is None and model_params is None and sigma is None \
+                and sample_counts is None and horizons is None:
             return None, []
         mp = _blob(model_params)
         cp = _blob(cost_params)
         sg = _f32(sigma)
-        ag = _lib.BatchAgents(mp[0], model_stride, cp[0], cost_stride, _p(sg))
-        return ag, [mp, cp, sg]
+        ks = None if sample_counts is None else np.ascontiguousarray(sample_counts, np.uint32)
+        hs = None if horizons is None else np.ascontiguousarray(horizons, np.uint32)
+        ag = _lib.BatchAgents(mp[0], model_stride, cp[0], cost_stride, _p(sg), _p(ks), _p(hs))
+        return ag, [mp, cp, sg, ks, hs]
 
     def prepare(self, N: int, T: int, x0_packed, u_nom_packed=None, cost_params=None,
                 cost_stride: int = 0, model_params=None, model_stride: int = 0, sigma=None,
-                want_states=True, want_controls=True, want_costs=True, want_terminal=True):
+                want_states=True, want_controls=True, want_costs=True, want_terminal=True,
+                sample_counts=None, horizons=None):
         x0 = _f32(x0_packed)
         un = _f32(u_nom_packed)
-        ag, keep = self._agents(cost_params, cost_stride, model_params, model_stride, sigma)
+        ag, keep = self._agents(cost_params, cost_stride, model_params, model_stride, sigma,
+                                sample_counts, horizons)
         eb = _lib.err_buf()
         _check(self.lib.mppi_backend_batch_prepare(
             self.h, N, T, _p(x0), _p(un), ctypes.byref(ag) if ag is not None else None,
@@ -176,10 +181,11 @@ class Backend:
 
     def simulate_batch(self, N: int, T: int, start_step: int, x0_packed, u_nom_packed=None,
                        cost_params=None, cost_stride: int = 0, model_params=None,
-                       model_stride: int = 0, sigma=None):
+                       model_stride: int = 0, sigma=None, sample_counts=None, horizons=None):
         x0 = _f32(x0_packed)
         un = _f32(u_nom_packed)
-        ag, keep = self._agents(cost_params, cost_stride, model_params, model_stride, sigma)
+        ag, keep = self._agents(cost_params, cost_stride, model_params, model_stride, sigma,
+                                sample_counts, horizons)
         st = np.zeros((T, N, self.n), np.float32)
         ct = np.zeros((T, N, self.m), np.float32)
         co = np.zeros((T, N), np.float32)
@@ -223,6 +229,17 @@ class Backend:
         _check(self.lib.mppi_backend_time_passes(self.h, iters, ctypes.byref(r), ctypes.byref(c),
                                                  eb, len(eb)), eb)
         return r.value, c.value
+
+    def tuning_info(self) -> dict:
+        """Autotuner choice for the prepared uneven batch (after a run)."""
+        g, n, r = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        ms = ctypes.c_float()
+        rc = self.lib.mppi_backend_tuning_info(self.h, ctypes.byref(g), ctypes.byref(n),
+                                               ctypes.byref(r), ctypes.byref(ms))
+        if rc != _lib.MPPI_OK:
+            return {}
+        return {"grid": g.value, "num_work": n.value, "stage_rows": r.value,
+                "rollout_ms": ms.value}
 
     def launch_info(self) -> dict:
         vals = [ctypes.c_uint32() for _ in range(5)]

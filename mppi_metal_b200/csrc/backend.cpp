@@ -171,6 +171,18 @@ struct mppi_backend {
   PinnedBuf h_up, h_down;
   bool run_timed = false;  // ev0 / ev1 bracket the last closed-loop run
 
+  // ---- uneven batch (per-agent K and H) ----
+  bool ragged = false;
+  std::vector<uint32_t> agent_K, agent_H, agent_blk0;
+  uint32_t num_work = 0;     // work items (agent, CTA-of-agent)
+  uint32_t total_records = 0;
+  uint32_t grid = 0;         // persistent grid size; 0 = one CTA per item
+  DevBuf d_agent_info;       // [K N][H N][blk0 N] uint32
+  DevBuf d_work;             // [num_work] uint2, longest horizons first
+  DevBuf d_queue;            // atomic work counter
+  std::string tuned_key;
+  float tuned_ms = 0.0f;
+
   // ---- closed-loop graph cache ----
   cudaGraphExec_t graph = nullptr;
   std::string graph_key;
@@ -266,9 +278,28 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
   b->N = N;
   b->T = T;
   b->geom = choose_geometry(b);
+  if (b->ragged) {
+    // uneven batches: 128-thread CTAs (results independent of tuning)
+    LaunchGeom g = b->geom;
+    if (g.block != 128) {
+      const size_t HM = b->HM();
+      g.variant = 1;
+      g.block = 128;
+      uint32_t rows = 32768 / (128 * 4);
+      rows = std::min<uint32_t>(std::max<uint32_t>(b->m, rows / b->m * b->m), (uint32_t)HM);
+      g.stage_rows = rows;
+      g.smem = pad4(HM) * 4 + (size_t)128 * 4 + (size_t)rows * 128 * 4;
+      g.pstride = (uint32_t)pad4(MPPI_PARTIAL_HEAD + HM);
+    }
+    uint32_t maxblk = 0;
+    for (uint32_t a = 0; a < N; ++a) maxblk = std::max(maxblk, (b->agent_K[a] + 127) / 128);
+    g.nblk = maxblk;  // the largest agent's CTA count (combine shared memory)
+    b->geom = g;
+  }
   CK(b->d_io.ensure(b->io_floats() * 4, &grew));
   CK(b->d_costs.ensure((size_t)N * b->K * 4, &grew));
-  CK(b->d_partials.ensure((size_t)N * b->geom.nblk * b->geom.pstride * 4, &grew));
+  const size_t records = b->ragged ? b->total_records : (size_t)N * b->geom.nblk;
+  CK(b->d_partials.ensure(records * b->geom.pstride * 4, &grew));
   b->want_s = ws;
   b->want_c = wc;
   b->want_k = wk;
@@ -280,7 +311,8 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
   CK(b->h_up.ensure((b->off_uout() + 64) * 4 + 2 * pad16(b->mp_size + b->cp_size) + 64));
   CK(b->h_down.ensure((b->io_floats() + 64) * 4));
   if (grew) ++b->generation;
-  const void* k = (const void*)b->mod->rollout[b->geom.variant];
+  const void* k = b->ragged ? (const void*)b->mod->rollout_work
+                            : (const void*)b->mod->rollout[b->geom.variant];
   if (b->geom.smem > 48 * 1024)
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem));
   return MPPI_OK;
@@ -312,6 +344,15 @@ MppiRolloutArgs rollout_args(const mppi_backend* b, uint32_t step_local) {
   a.cost_stride = b->run_cp_stride;
   a.costs = b->d_costs.as<float>();
   a.partials = b->d_partials.as<float>();
+  if (b->ragged) {
+    const uint32_t* info = b->d_agent_info.as<uint32_t>();
+    a.agent_K = info;
+    a.agent_H = info + b->N;
+    a.agent_blk0 = info + 2 * b->N;
+    a.work = b->d_work.as<uint2>();
+    a.work_counter = b->grid ? b->d_queue.as<uint32_t>() : nullptr;
+    a.num_work = b->num_work;
+  }
   return a;
 }
 
@@ -340,6 +381,13 @@ MppiCombineArgs combine_args(const mppi_backend* b, uint32_t step_local, bool pr
   c.hist_controls = b->want_c ? b->d_hc.as<float>() : nullptr;
   c.hist_costs = b->want_k ? b->d_hk.as<float>() : nullptr;
   c.terminal = b->want_t ? b->d_term.as<float>() : nullptr;
+  if (b->ragged) {
+    const uint32_t* info = b->d_agent_info.as<uint32_t>();
+    c.agent_K = info;
+    c.agent_H = info + b->N;
+    c.agent_blk0 = info + 2 * b->N;
+    c.block = 128;
+  }
   return c;
 }
 
@@ -350,9 +398,86 @@ size_t combine_smem(const mppi_backend* b) {
 cudaError_t launch_rollout(mppi_backend* b, uint32_t step_local) {
   MppiRolloutArgs a = rollout_args(b, step_local);
   void* args[] = {&a};
+  if (b->ragged) {
+    if (b->grid) {
+      cudaError_t e = cudaMemsetAsync(b->d_queue.p, 0, 4, b->stream);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaLaunchKernel((const void*)b->mod->rollout_work,
+                            dim3(b->grid ? b->grid : b->num_work), dim3(128), args,
+                            b->geom.smem, b->stream);
+  }
   return cudaLaunchKernel((const void*)b->mod->rollout[b->geom.variant],
                           dim3(b->geom.nblk, b->N), dim3(b->geom.block), args, b->geom.smem,
                           b->stream);
+}
+
+// Uneven batches: times candidate (grid size, noise staging) pairs on the
+// prepared data and keeps the fastest.  Every candidate computes the same
+// bits (same 128-thread partition of samples, same summation orders).
+int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
+  const size_t HM = b->HM();
+  const size_t budget = std::min<size_t>(b->max_smem_optin ? b->max_smem_optin : 232448, 232448);
+  std::vector<uint32_t> stage_options;
+  const size_t full = pad4(HM) * 4 + 128 * 4 + HM * 128 * 4;
+  if (full <= budget - 2048) stage_options.push_back((uint32_t)HM);
+  uint32_t chunk = std::max<uint32_t>(b->m, (32768 / 512) / b->m * b->m);
+  stage_options.push_back(std::min<uint32_t>(chunk, (uint32_t)HM));
+  std::vector<uint32_t> grids = {0};
+  for (uint32_t c = 1; c <= 4; ++c) grids.push_back(c * (uint32_t)b->num_sms);
+  // MPPI_B200_UNEVEN_GRID / MPPI_B200_UNEVEN_STAGE_ROWS pin a candidate
+  // (reproducible profiling; the result bits are the same either way)
+  if (const char* g = getenv("MPPI_B200_UNEVEN_GRID"); g && *g) {
+    grids.assign(1, (uint32_t)strtoul(g, nullptr, 10));
+  }
+  if (const char* r = getenv("MPPI_B200_UNEVEN_STAGE_ROWS"); r && *r) {
+    const uint32_t rows = (uint32_t)strtoul(r, nullptr, 10);
+    if (rows >= b->m && rows % b->m == 0) {
+      const size_t sm = pad4(HM) * 4 + 128 * 4 + (size_t)std::min<size_t>(rows, HM) * 128 * 4;
+      if (sm <= budget) stage_options.assign(1, (uint32_t)std::min<size_t>(rows, HM));
+    }
+  }
+  const LaunchGeom base = b->geom;
+  float best = 1e30f;
+  LaunchGeom best_g = base;
+  uint32_t best_grid = 0;
+  for (uint32_t rows : stage_options) {
+    LaunchGeom g = base;
+    g.stage_rows = rows;
+    g.smem = pad4(HM) * 4 + 128 * 4 + (size_t)rows * 128 * 4;
+    b->geom = g;
+    CK(cudaFuncSetAttribute((const void*)b->mod->rollout_work,
+                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
+    for (uint32_t grid : grids) {
+      b->grid = grid;
+      CK(launch_rollout(b, 0));  // warm-up
+      CK(cudaEventRecord(b->ev0, b->stream));
+      for (int i = 0; i < 3; ++i) CK(launch_rollout(b, 0));
+      CK(cudaEventRecord(b->ev1, b->stream));
+      CK(cudaEventSynchronize(b->ev1));
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+      ms /= 3.0f;
+      if (ms < best) {
+        best = ms;
+        best_g = g;
+        best_grid = grid;
+      }
+    }
+  }
+  b->geom = best_g;
+  b->grid = best_grid;
+  b->tuned_ms = best;
+  CK(cudaFuncSetAttribute((const void*)b->mod->rollout_work,
+                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)best_g.smem));
+  return MPPI_OK;
+}
+
+std::string ragged_key(const mppi_backend* b) {
+  std::string k = std::to_string(b->N) + ":";
+  for (uint32_t a = 0; a < b->N; ++a)
+    k += std::to_string(b->agent_K[a]) + "," + std::to_string(b->agent_H[a]) + ";";
+  return k;
 }
 
 cudaError_t launch_combine(mppi_backend* b, uint32_t step_local, bool propagate) {
@@ -454,7 +579,17 @@ int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
            b->want_k, b->want_t, (const void*)b->run_mp, (const void*)b->run_cp,
            (unsigned long long)b->run_mp_stride, (unsigned long long)b->run_cp_stride,
            (const void*)b->run_sigma, b->run_sigma_stride);
-  const std::string key = keybuf;
+  if (b->ragged) {
+    const std::string rk = ragged_key(b);
+    if (b->tuned_key != rk) {
+      if (int rc = tune_ragged(b, err, err_len)) return rc;
+      b->tuned_key = rk;
+    }
+  }
+  const std::string key = std::string(keybuf) + (b->ragged ? "/r" + std::to_string(b->grid) + "/" +
+                                                                 std::to_string(b->geom.stage_rows) +
+                                                                 "/" + b->tuned_key
+                                                           : std::string());
   if (b->graph == nullptr || b->graph_key != key) {
     if (b->graph) {
       cudaGraphExecDestroy(b->graph);
@@ -673,6 +808,7 @@ int mppi_backend_dispatch_rollout(mppi_backend* b, uint64_t step_index, const fl
     return MPPI_ERR_INVALID;
   }
   if (int rc = check_override_sizes(b, mp_bytes, mp, cp_bytes, cp, err, err_len)) return rc;
+  b->ragged = false;
   if (int rc = ensure_shape(b, 1, 0, false, false, false, false, err, err_len)) return rc;
   b->run_mp = pick_params(b, true, mp, mp_bytes);
   b->run_cp = pick_params(b, false, cp, cp_bytes);
@@ -701,6 +837,66 @@ int mppi_backend_batch_prepare(mppi_backend* b, uint32_t N, uint32_t T, const fl
   if (N == 0 || T == 0 || !x0) {
     set_err(err, err_len, "num_agents and num_steps must be > 0 and x0 must not be null.");
     return MPPI_ERR_INVALID;
+  }
+  b->ragged = agents && (agents->sample_counts || agents->horizons);
+  if (b->ragged) {
+    CK(cudaStreamSynchronize(b->stream));  // the tables below may be in use
+    b->agent_K.assign(N, b->K);
+    b->agent_H.assign(N, b->H);
+    for (uint32_t a = 0; a < N; ++a) {
+      if (agents->sample_counts) b->agent_K[a] = agents->sample_counts[a];
+      if (agents->horizons) b->agent_H[a] = agents->horizons[a];
+      if (b->agent_K[a] == 0 || b->agent_K[a] > b->K) {
+        set_err(err, err_len, "sample_counts[" + std::to_string(a) + "] (" +
+                                  std::to_string(b->agent_K[a]) +
+                                  ") must be in [1, DriverConfig::sample_count = " +
+                                  std::to_string(b->K) + "].");
+        b->ragged = false;
+        return MPPI_ERR_INVALID;
+      }
+      if (b->agent_H[a] == 0 || b->agent_H[a] > b->H) {
+        set_err(err, err_len, "horizons[" + std::to_string(a) + "] (" +
+                                  std::to_string(b->agent_H[a]) +
+                                  ") must be in [1, DriverConfig::horizon = " +
+                                  std::to_string(b->H) + "].");
+        b->ragged = false;
+        return MPPI_ERR_INVALID;
+      }
+    }
+    // work items, longest horizon first (then more samples first), so the
+    // longest items start earliest: list scheduling by decreasing work
+    b->agent_blk0.assign(N, 0);
+    uint32_t rec = 0;
+    std::vector<uint32_t> order(N);
+    for (uint32_t a = 0; a < N; ++a) {
+      b->agent_blk0[a] = rec;
+      rec += (b->agent_K[a] + 127) / 128;
+      order[a] = a;
+    }
+    b->total_records = rec;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+      if (b->agent_H[x] != b->agent_H[y]) return b->agent_H[x] > b->agent_H[y];
+      return b->agent_K[x] > b->agent_K[y];
+    });
+    std::vector<uint32_t> work;
+    work.reserve(2 * (size_t)rec);
+    for (uint32_t a : order)
+      for (uint32_t k = 0; k < (b->agent_K[a] + 127) / 128; ++k) {
+        work.push_back(a);
+        work.push_back(k);
+      }
+    b->num_work = rec;
+    std::vector<uint32_t> info(3 * (size_t)N);
+    std::copy(b->agent_K.begin(), b->agent_K.end(), info.begin());
+    std::copy(b->agent_H.begin(), b->agent_H.end(), info.begin() + N);
+    std::copy(b->agent_blk0.begin(), b->agent_blk0.end(), info.begin() + 2 * N);
+    bool grew = false;
+    CK(b->d_agent_info.ensure(info.size() * 4, &grew));
+    CK(b->d_work.ensure(work.size() * 4, &grew));
+    CK(b->d_queue.ensure(16, &grew));
+    if (grew) ++b->generation;
+    CK(cudaMemcpy(b->d_agent_info.p, info.data(), info.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_work.p, work.data(), work.size() * 4, cudaMemcpyHostToDevice));
   }
   if (int rc = ensure_shape(b, N, T, ws, wc, wk, wt, err, err_len)) return rc;
   b->run_mp = pick_params(b, true, nullptr, 0);
@@ -1004,6 +1200,17 @@ int mppi_compile_check(const mppi_backend_plugin* plugin, const mppi_backend_con
   set_err(log, log_len, lg);
   if (rc != MPPI_OK) set_err(err, err_len, e);
   return rc;
+}
+
+int mppi_backend_tuning_info(mppi_backend* b, uint32_t* grid, uint32_t* num_work,
+                             uint32_t* stage_rows, float* rollout_ms) {
+  if (!b || !b->initialized) return MPPI_ERR_NOT_INIT;
+  if (!b->ragged || b->tuned_key.empty()) return MPPI_ERR_INVALID;
+  if (grid) *grid = b->grid;
+  if (num_work) *num_work = b->num_work;
+  if (stage_rows) *stage_rows = b->geom.stage_rows;
+  if (rollout_ms) *rollout_ms = b->tuned_ms;
+  return MPPI_OK;
 }
 
 int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,

@@ -176,11 +176,15 @@ __device__ __forceinline__ void copy_words(uint32_t* dst, const uint8_t* src, in
 }
 
 // --------------------------------------------------------------------------
-// Fused rollout.  One thread per sample; grid (nblk, num_agents).
-// Dynamic shared memory: u_nom[H*m] | staging[stage_rows][BLOCK] | e[BLOCK]
+// Fused rollout of one work item: CTA `blk` of agent `agent` (K samples,
+// horizon H, nominal at un_g, partial record at part).  One thread per
+// sample.  Dynamic shared memory: u_nom[H*m] | staging[stage_rows][BLOCK] |
+// e[BLOCK] (sized for the launch's largest horizon).
 // --------------------------------------------------------------------------
 template <int BLOCK>
-__device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
+__device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t agent,
+                                             uint32_t blk, uint32_t K, uint32_t H,
+                                             const float* un_g, float* part) {
   constexpr int NW = BLOCK / 32;
   constexpr int PER_LANE = BLOCK / 32;
   extern __shared__ __align__(16) float dsm[];
@@ -192,11 +196,9 @@ __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   __shared__ __align__(16) uint32_t cp_s[(MPPI_CP_BYTES + 3) / 4];
 #endif
 
-  const uint32_t agent = blockIdx.y;
-  const uint32_t blk = blockIdx.x;
   const uint32_t tid = threadIdx.x;
   const uint32_t lane = tid & 31, warp = tid >> 5;
-  const uint32_t K = a.K, H = a.H, HM = H * kM;
+  const uint32_t HM = H * kM;
   const uint32_t k = blk * BLOCK + tid;
   const bool active = k < K;
   const uint32_t step = *a.step_base + a.step_local;
@@ -204,10 +206,9 @@ __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   const bool staged = a.stage_rows >= HM;
 
   float* un_s = dsm;
-  float* stage_s = dsm + ((HM + 3) & ~3u);
+  float* stage_s = dsm + ((a.H * kM + 3) & ~3u);
   float* e_s = stage_s + (size_t)a.stage_rows * BLOCK;
 
-  const float* un_g = a.u_nom + (size_t)agent * HM;
   for (uint32_t i = tid; i < HM; i += BLOCK) un_s[i] = un_g[i];
   const uint8_t* mp_g = a.model_params + a.model_stride * agent;
   const uint8_t* cp_g = a.cost_params + a.cost_stride * agent;
@@ -303,7 +304,7 @@ __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   }
   if (active) {
     J += MPPI_TERMINAL_COST_FN(reinterpret_cast<TermStateT>(reinterpret_cast<void*>(st)), mp, cp);
-    if (a.costs) a.costs[(size_t)agent * K + k] = J;
+    if (a.costs) a.costs[(size_t)agent * a.K + k] = J;  // agent stride: the largest K
   }
 
   // ---- CTA softmax statistics against the CTA minimum ----
@@ -312,7 +313,6 @@ __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   float s_e = e, s_e2 = e * e, s_c = active ? J : 0.0f;
   block_sum3<NW>(s_e, s_e2, s_c, red_s);
   e_s[tid] = e;
-  float* part = a.partials + ((size_t)agent * a.nblk + blk) * a.pstride;
   if (tid == 0) {
     part[0] = bmin;
     part[1] = s_e;
@@ -360,6 +360,35 @@ __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   }
 }
 
+// Uniform batch: grid (nblk, num_agents), every agent K samples, horizon H.
+template <int BLOCK>
+__device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
+  const uint32_t agent = blockIdx.y, blk = blockIdx.x;
+  rollout_item<BLOCK>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
+                      a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
+}
+
+// Uneven batch: work items (agent, CTA-of-agent), longest horizons first.
+// A persistent grid pulls items from an atomic queue (no CTA ever waits on
+// another); without a queue each CTA runs item blockIdx.x.
+template <int BLOCK>
+__device__ __forceinline__ void rollout_work(const MppiRolloutArgs& a) {
+  __shared__ uint32_t item_s;
+  for (uint32_t pass = 0;; ++pass) {
+    __syncthreads();  // the previous item is done with shared memory
+    if (threadIdx.x == 0)
+      item_s = a.work_counter ? atomicAdd(a.work_counter, 1u) : (pass == 0 ? blockIdx.x : ~0u);
+    __syncthreads();
+    const uint32_t item = item_s;
+    if (item >= a.num_work) return;
+    const uint2 w = a.work[item];
+    const uint32_t agent = w.x, blk = w.y;
+    rollout_item<BLOCK>(a, agent, blk, a.agent_K[agent], a.agent_H[agent],
+                        a.u_nom + (size_t)agent * a.H * kM,
+                        a.partials + ((size_t)a.agent_blk0[agent] + blk) * a.pstride);
+  }
+}
+
 // --------------------------------------------------------------------------
 // Combine: one CTA per agent.  Dynamic shared memory: scale[nblk] | u[H*m].
 // --------------------------------------------------------------------------
@@ -371,10 +400,15 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
   __shared__ float red_s[3 * NW];
   const uint32_t agent = blockIdx.x;
   const uint32_t tid = threadIdx.x;
-  const uint32_t H = a.H, HM = H * kM, nblk = a.nblk, ps = a.pstride;
+  const bool ragged = a.agent_K != nullptr;
+  const uint32_t K = ragged ? a.agent_K[agent] : a.K;
+  const uint32_t H = ragged ? a.agent_H[agent] : a.H;
+  const uint32_t HM = H * kM, ps = a.pstride;
+  const uint32_t nblk = ragged ? (K + a.block - 1) / a.block : a.nblk;
+  const size_t blk0 = ragged ? (size_t)a.agent_blk0[agent] : (size_t)agent * a.nblk;
   float* scale_s = dsm;
-  float* u_s = dsm + ((nblk + 3) & ~3u);
-  const float* P = a.partials + (size_t)agent * nblk * ps;
+  float* u_s = dsm + ((a.nblk + 3) & ~3u);  // a.nblk: the largest agent's CTA count
+  const float* P = a.partials + blk0 * ps;
 
   float lm = pos_inf();
   for (uint32_t b = tid; b < nblk; b += kCombineBlock) lm = fminf(lm, P[(size_t)b * ps]);
@@ -391,8 +425,8 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
   block_sum3<NW>(S, Q, C, red_s);  // ends with a barrier: scale_s visible
 
   const float invS = 1.0f / S;
-  float* un = a.u_nom + (size_t)agent * HM;
-  float* uo = a.u_out + (size_t)agent * HM;
+  float* un = a.u_nom + (size_t)agent * a.H * kM;  // agent stride: the largest horizon
+  float* uo = a.u_out + (size_t)agent * a.H * kM;
   for (uint32_t j = tid; j < HM; j += kCombineBlock) {
     float v = 0.0f;
     for (uint32_t b = 0; b < nblk; ++b)
@@ -404,7 +438,7 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
   }
   if (tid == 0) {
     a.diag[agent * 3 + 0] = M;
-    a.diag[agent * 3 + 1] = C / (float)a.K;
+    a.diag[agent * 3 + 1] = C / (float)K;
     a.diag[agent * 3 + 2] = S * S / Q;  // 1 / sum w^2 with w = e / S
     if (a.stats) {
       a.stats[agent * 4 + 0] = M;
@@ -462,6 +496,13 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
 MPPI_ROLLOUT_ENTRY(64)
 MPPI_ROLLOUT_ENTRY(128)
 MPPI_ROLLOUT_ENTRY(256)
+
+// Uneven batches always use 128-thread CTAs, so the partition of samples into
+// CTAs -- and therefore every floating-point sum -- does not depend on the
+// tuned grid size or staging mode.
+extern "C" __global__ void __launch_bounds__(128, 4) mppi_rollout_work_b128(const MppiRolloutArgs a) {
+  mppi::rollout_work<128>(a);
+}
 
 extern "C" __global__ void __launch_bounds__(mppi::kCombineBlock)
     mppi_combine(const MppiCombineArgs a) {

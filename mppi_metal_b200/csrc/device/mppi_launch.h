@@ -42,6 +42,19 @@ struct MppiRolloutArgs {
   uint64_t cost_stride;
   float* costs;     // [N][K] per-sample costs (may be null)
   float* partials;  // [N][nblk][pstride]
+  // Uneven batches (all null for a uniform batch).  Agent a has agent_K[a]
+  // samples, horizon agent_H[a] <= H (nominals keep the stride H*m) and its
+  // partial records start at record agent_blk0[a].  The launch walks `work`
+  // items (agent, CTA-of-agent): taken from an atomic queue (work_counter,
+  // zero at launch) by a persistent grid, or one item per CTA when
+  // work_counter is null.
+  const uint32_t* agent_K;
+  const uint32_t* agent_H;
+  const uint32_t* agent_blk0;
+  const uint2* work;
+  uint32_t* work_counter;
+  uint32_t num_work;
+  uint32_t pad1;
 };
 
 // One launch of the combine (+ optional propagate & shift) kernel.
@@ -70,6 +83,13 @@ struct MppiCombineArgs {
   float* hist_controls;  // [T][N][m] (may be null)
   float* hist_costs;   // [T][N] (may be null)
   float* terminal;     // [N][n] (may be null)
+  // Uneven batches (null for a uniform batch): per-agent sample count,
+  // horizon and first partial record; `block` = rollout CTA size.
+  const uint32_t* agent_K;
+  const uint32_t* agent_H;
+  const uint32_t* agent_blk0;
+  uint32_t block;
+  uint32_t pad0;
 };
 
 // Normalised weights from the per-sample costs and the combine statistics

@@ -374,7 +374,10 @@ bool MPPIDriver::simulate_batch(
 	ag.cost_params = agent_params.cost_params;
 	ag.cost_params_stride = agent_params.cost_params_stride;
 	ag.sigma = agent_params.sigma;
-	const bool any = ag.model_params || ag.cost_params || ag.sigma;
+	ag.sample_counts = agent_params.sample_counts;
+	ag.horizons = agent_params.horizons;
+	const bool any = ag.model_params || ag.cost_params || ag.sigma || ag.sample_counts ||
+		ag.horizons;
 	std::vector<char> err(kErrLen, '\0');
 	if (mppi_backend_dispatch_batch_simulation(impl_->backend, num_agents, num_steps,
 			impl_->step_index, x0_packed, nullptr, any ? &ag : nullptr, results.states_out,

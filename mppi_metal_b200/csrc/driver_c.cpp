@@ -164,7 +164,8 @@ int mppi_driver_simulate_batch(mppi_driver* d, uint32_t N, uint32_t T, const flo
 
 int mppi_driver_simulate_batch_agents(mppi_driver* d, uint32_t N, uint32_t T, const float* x0,
                                       const void* mp, size_t mps, const void* cp, size_t cps,
-                                      const float* sigma, float* states, float* controls,
+                                      const float* sigma, const uint32_t* sample_counts,
+                                      const uint32_t* horizons, float* states, float* controls,
                                       float* costs, float* terminal, uint32_t res_agents,
                                       uint32_t res_steps, char* err, size_t err_len) {
   ErrSink e{err, err_len, {}};
@@ -174,6 +175,8 @@ int mppi_driver_simulate_batch_agents(mppi_driver* d, uint32_t N, uint32_t T, co
   ap.cost_params = cp;
   ap.cost_params_stride = cps;
   ap.sigma = sigma;
+  ap.sample_counts = sample_counts;
+  ap.horizons = horizons;
   BatchSimulationResults r;
   r.states_out = states;
   r.controls_out = controls;

@@ -267,6 +267,8 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
     ce = cudaLibraryGetKernel(&mod->rollout[i], mod->library, names[i]);
     if (ce != cudaSuccess) break;
   }
+  if (ce == cudaSuccess)
+    ce = cudaLibraryGetKernel(&mod->rollout_work, mod->library, "mppi_rollout_work_b128");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->combine, mod->library, "mppi_combine");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->weights, mod->library, "mppi_weights");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->noise, mod->library, "mppi_noise");

@@ -37,6 +37,7 @@ constexpr int kRolloutBlocks[3] = {64, 128, 256};
 struct KernelModule {
   cudaLibrary_t library = nullptr;
   cudaKernel_t rollout[3] = {nullptr, nullptr, nullptr};
+  cudaKernel_t rollout_work = nullptr;  // uneven batches (128-thread CTAs)
   cudaKernel_t combine = nullptr;
   cudaKernel_t weights = nullptr;
   cudaKernel_t noise = nullptr;

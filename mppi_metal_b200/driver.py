@@ -196,6 +196,8 @@ class BatchAgentParams:
     cost_params: Optional[bytes] = None
     cost_params_stride: int = 0
     sigma: Optional[np.ndarray] = None
+    sample_counts: Optional[np.ndarray] = None  # uneven batches (uint32 per agent)
+    horizons: Optional[np.ndarray] = None
 
 
 def _out_array(a: Optional[np.ndarray]) -> Optional[np.ndarray]:
@@ -336,11 +338,15 @@ class MPPIDriver:
             mp, _ = _blob(agent_params.model_params)
             cp, _ = _blob(agent_params.cost_params)
             sg = _f32(agent_params.sigma)
+            ks = None if agent_params.sample_counts is None else \
+                np.ascontiguousarray(agent_params.sample_counts, dtype=np.uint32)
+            hs = None if agent_params.horizons is None else \
+                np.ascontiguousarray(agent_params.horizons, dtype=np.uint32)
             rc = self._lib.mppi_driver_simulate_batch_agents(
                 self._h, num_agents, num_steps, _ptr(x0),
                 ctypes.cast(mp, ctypes.c_void_p) if mp is not None else None,
                 agent_params.model_params_stride,
                 ctypes.cast(cp, ctypes.c_void_p) if cp is not None else None,
-                agent_params.cost_params_stride, _ptr(sg), *outs, results.num_agents,
-                results.num_steps, eb, len(eb))
+                agent_params.cost_params_stride, _ptr(sg), _ptr(ks), _ptr(hs), *outs,
+                results.num_agents, results.num_steps, eb, len(eb))
         return self._done(rc, eb, error)

@@ -196,3 +196,70 @@ def unicycle_executed_cost(states: np.ndarray, controls: np.ndarray, terminal: n
         pen = np.maximum(np.array(c.obs_r[:n_obs]) - d, 0.0).sum(axis=1)
         out[a] = float(np.sum(goal + c.w_obs * pen) + c.w_terminal * goal[-1])
     return out
+
+
+def natural_cubic_spline(x0: float, dx: float, ys: np.ndarray) -> np.ndarray:
+    """Per-segment coefficients [c0, c1, c2, c3] (in s = x - x_i) of the
+    natural cubic spline through (x0 + i dx, ys[i])."""
+    n = len(ys) - 1
+    a = np.zeros((n + 1, n + 1))
+    rhs = np.zeros(n + 1)
+    a[0, 0] = a[n, n] = 1.0
+    for i in range(1, n):
+        a[i, i - 1], a[i, i], a[i, i + 1] = dx, 4.0 * dx, dx
+        rhs[i] = 3.0 * ((ys[i + 1] - ys[i]) - (ys[i] - ys[i - 1])) / dx
+    c = np.linalg.solve(a, rhs)
+    coef = np.zeros((n, 4))
+    for i in range(n):
+        coef[i, 0] = ys[i]
+        coef[i, 1] = (ys[i + 1] - ys[i]) / dx - dx * (2.0 * c[i] + c[i + 1]) / 3.0
+        coef[i, 2] = c[i]
+        coef[i, 3] = (c[i + 1] - c[i]) / (3.0 * dx)
+    return coef
+
+
+def _random_spd(rng: np.random.Generator, lo: float, hi: float) -> np.ndarray:
+    th = rng.uniform(0.0, np.pi)
+    rot = np.array([[np.cos(th), -np.sin(th)], [np.sin(th), np.cos(th)]])
+    return rot @ np.diag(rng.uniform(lo, hi, size=2)) @ rot.T
+
+
+def bicycle_uneven(seed: int = 0, N: int = 64, T: int = 100, k_range=(1024, 16384),
+                   h_range=(16, 96)) -> Workload:
+    """Uneven batch: N kinematic-bicycle instances (state [x,y,theta,v,delta],
+    control [accel, steer_rate]) with K log-uniform in k_range and H
+    log-uniform in h_range per instance, a full 2x2 noise covariance per
+    instance (random SPD, eigenvalues U[0.05, 0.5]) and a lane-keeping cost on
+    a seeded natural cubic-spline centreline (32 segments of 5 m)."""
+    rng = np.random.default_rng(seed)
+    mp = BicycleModelParams(0.05, 2.5, 0.6, 0.0)
+    nseg, dx = BICYCLE_MAX_SEGMENTS, 5.0
+    ys = np.cumsum(rng.uniform(-1.0, 1.0, size=nseg + 1))
+    coef = natural_cubic_spline(0.0, dx, ys)
+    cp = BicycleCostParams()
+    cp.x0, cp.knot_dx, cp.num_segments, cp.v_ref = 0.0, dx, nseg, 5.0
+    cp.w_lat, cp.w_head, cp.w_speed, cp.w_terminal = 1.0, 2.0, 0.2, 10.0
+    for i in range(nseg):
+        for j in range(4):
+            cp.coef[i][j] = float(coef[i, j])
+    lk = rng.uniform(np.log(k_range[0]), np.log(k_range[1]), size=N)
+    lh = rng.uniform(np.log(h_range[0]), np.log(h_range[1]), size=N)
+    Ks = np.round(np.exp(lk)).astype(np.uint32)
+    Hs = np.round(np.exp(lh)).astype(np.uint32)
+    x0 = np.zeros((N, 5), np.float32)
+    x0[:, 0] = rng.uniform(0.0, 20.0, size=N)
+    for a in range(N):
+        i = min(int(x0[a, 0] // dx), nseg - 1)
+        sg = x0[a, 0] - i * dx
+        x0[a, 1] = coef[i, 0] + sg * (coef[i, 1] + sg * (coef[i, 2] + sg * coef[i, 3])) \
+            + rng.uniform(-1.0, 1.0)
+        x0[a, 3] = rng.uniform(2.0, 6.0)
+    covs = np.stack([_random_spd(rng, 0.05, 0.5) for _ in range(N)]).astype(np.float32)
+    shared = np.diag([0.25, 0.25]).astype(np.float32)
+    w = Workload("bicycle_uneven", "bicycle_lane", "bicycle_lane", 5, 2, int(Hs.max()),
+                 int(Ks.max()), 1.0, shared, np.linalg.inv(shared).astype(np.float32),
+                 np.array([-3.0, -0.5], np.float32), np.array([3.0, 0.5], np.float32), N, T,
+                 x0, blob(mp), [blob(cp)] * N, covs.reshape(N, 4), cov_full=True, seed=seed)
+    w.agent_K = Ks
+    w.agent_H = Hs
+    return w
