@@ -65,6 +65,8 @@ def parse():
                     help="kernels: only launch the rollout and combine kernels of the "
                          "workload `--iters` times each (small capture target for ncu)")
     ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--workload", choices=WORKLOADS, default="batch",
+                    help="batch (default, the headline configuration), uneven, single")
     return ap.parse_args()
 
 
@@ -73,10 +75,35 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
-def workload_for_rank(rank: int):
+WORKLOADS = ("batch", "uneven", "single")
+
+
+def workload_for_rank(rank: int, name: str = "batch"):
+    """batch  : 256 unicycle agents per GPU, K 4096, H 50, 300 closed-loop steps
+                (the headline configuration);
+    uneven : 64 kinematic-bicycle instances per GPU, K log-uniform [1024, 16384],
+                H log-uniform [16, 96], full 2x2 covariance, 100 closed-loop steps;
+    single : one unicycle agent, K 1024, H 30, 8 static obstacles, control
+                cost on, 200 closed-loop steps from x0 = 0, Philox seed 0."""
     from mppi_metal_b200 import models
+    if name == "uneven":
+        return models.bicycle_uneven(seed=2000 + rank, N=64, T=100)
+    if name == "single":
+        return models.unicycle_single(seed=0, K=1024, H=30, T=200)
     return models.unicycle_batch(seed=1000 + rank, N=AGENTS_PER_GPU, K=K_SAMPLES, H=HORIZON,
                                  T=CLOSED_LOOP_STEPS)
+
+
+def agent_shapes(w):
+    """(sample counts, horizons) per agent, or (None, None) for a uniform batch."""
+    return getattr(w, "agent_K", None), getattr(w, "agent_H", None)
+
+
+def rollout_steps_per_control_step(w) -> int:
+    ks, hs = agent_shapes(w)
+    if ks is None:
+        return w.num_agents * w.sample_count * w.horizon
+    return int(np.sum(ks.astype(np.int64) * hs.astype(np.int64)))
 
 
 # ---------------------------------------------------------------------------
@@ -218,7 +245,28 @@ def run_reference(args):
     return 0
 
 
-def config_block():
+def config_block(name: str = "batch", w=None):
+    if name == "uneven":
+        return {
+            "workload": ("bicycle_uneven: 64 kinematic-bicycle instances per GPU, K log-uniform "
+                         "[1024,16384], H log-uniform [16,96], full 2x2 covariance per instance "
+                         "(eigenvalues U[0.05,0.5]), cubic-spline lane keeping, 100 closed-loop "
+                         "steps; one persistent launch per pass, autotuned"),
+            "agents_per_gpu": w.num_agents, "rollout_steps_per_control_step":
+                rollout_steps_per_control_step(w), "closed_loop_steps": w.num_steps,
+            "step": "one simulate_batch closed loop (100 control steps for every agent)",
+            "l2": "flushed between timed iterations (256 MiB device write)",
+            "parallelism": "agent-sharded replicas, no data-path collective",
+        }
+    if name == "single":
+        return {
+            "workload": ("unicycle_single: 1 agent, K=1024, H=30, 8 static obstacles, control "
+                         "cost on, 200 closed-loop steps from x0=0, Philox seed 0"),
+            "agents_per_gpu": 1, "samples": 1024, "horizon": 30, "closed_loop_steps": 200,
+            "step": "one simulate closed loop of 200 control steps",
+            "l2": "flushed between timed iterations (256 MiB device write)",
+            "parallelism": "replicas only",
+        }
     return {
         "workload": (f"unicycle_batch: {AGENTS_PER_GPU} agents per GPU, K={K_SAMPLES}, H={HORIZON}, "
                      f"{CLOSED_LOOP_STEPS} closed-loop steps, 16 moving circular obstacles and "
@@ -249,9 +297,10 @@ def run_b200(args):
     from mppi_metal_b200._lib import plugin_path
     from mppi_metal_b200.backend import Backend
 
-    w = workload_for_rank(rank)
+    w = workload_for_rank(rank, args.workload)
     N, T = w.num_agents, w.num_steps
-    rs_per_step = N * w.sample_count * w.horizon * T  # rollout-steps per bench step (this rank)
+    ks, hs = agent_shapes(w)
+    rs_per_step = rollout_steps_per_control_step(w) * T  # per bench step (this rank)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def barrier():
@@ -268,12 +317,12 @@ def run_b200(args):
 
     # ---- value: device-resident closed loop ---------------------------------
     b = Backend(w.plugin, w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam, w.sigma,
-                w.u_min, w.u_max, sigma_inv=w.sigma_inv, control_cost=w.control_cost,
-                model_params_size=len(w.model_params), cost_params_size=w.cost_stride,
-                seed=w.seed)
+                w.u_min, w.u_max, sigma_inv=w.sigma_inv, cov_full=w.cov_full,
+                control_cost=w.control_cost, model_params_size=len(w.model_params),
+                cost_params_size=w.cost_stride, seed=w.seed)
     b.bind_params(w.model_params, w.cost_params[0])
     b.prepare(N, T, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
-              sigma=w.agent_sigma)
+              sigma=w.agent_sigma, sample_counts=ks, horizons=hs)
     for _ in range(args.warmup):
         b.run(0)
         b.last_run_ms()
@@ -292,12 +341,14 @@ def run_b200(args):
     # ---- kernel-level timing for the roofline --------------------------------
     rollout_ms, combine_ms = b.time_passes(20)
     geom = b.launch_info()
+    tuning = b.tuning_info()
     b.close()
 
     # ---- e2e: public API, host buffers ---------------------------------------
+    form = D.CovarianceForm.kFull if w.cov_full else D.CovarianceForm.kDiagonal
     cfg = D.DriverConfig(w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam,
-                         D.ControlNoiseConfig(D.CovarianceForm.kDiagonal, w.sigma, w.sigma_inv, 2),
-                         D.ControlBounds(w.u_min, w.u_max, 2))
+                         D.ControlNoiseConfig(form, w.sigma, w.sigma_inv, w.control_dim),
+                         D.ControlBounds(w.u_min, w.u_max, w.control_dim))
     drv = D.MPPIDriver(cfg, D.DriverOptions(control_cost=w.control_cost))
     err = D.ErrorRef()
     spec = D.ModelPluginSpec(plugin_path(w.plugin),
@@ -309,7 +360,8 @@ def run_b200(args):
     assert drv.set_problem_params(D.ProblemParams(D.ByteView.of(w.model_params),
                                                   D.ByteView.of(w.cost_params[0])), err), err.value
     agent_params = D.BatchAgentParams(cost_params=w.cost_params_packed,
-                                      cost_params_stride=w.cost_stride, sigma=w.agent_sigma)
+                                      cost_params_stride=w.cost_stride, sigma=w.agent_sigma,
+                                      sample_counts=ks, horizons=hs)
     outs = D.BatchSimulationResults(np.zeros((T, N, w.state_dim), np.float32),
                                     np.zeros((T, N, w.control_dim), np.float32),
                                     np.zeros((T, N), np.float32),
@@ -327,17 +379,21 @@ def run_b200(args):
     barrier()
     e2e_total = max_over_ranks(sum(e2e_times))
     # executed closed-loop cost of the last API call (from x0, step index 0)
-    cost = models.unicycle_executed_cost(outs.states_out, outs.controls_out,
-                                         outs.terminal_states_out, w.cost_params)
+    cost = models.executed_cost(w, outs.states_out, outs.controls_out,
+                                outs.terminal_states_out)
     e2e_value = world * rs_per_step * args.steps / e2e_total
     HM = w.horizon * w.control_dim
+    sig_len = w.control_dim * w.control_dim if w.cov_full else w.control_dim
     h2d = (N * w.state_dim + N * HM + 4) * 4 + N * ((w.cost_stride + 15) // 16 * 16) \
-        + N * w.control_dim * 4
+        + N * sig_len * 4
+    if ks is not None:
+        work_items = int(sum((int(k) + 127) // 128 for k in ks))
+        h2d += 12 * N + 8 * work_items  # per-agent K / H / offsets and the work list
     d2h = (T * N * (w.state_dim + w.control_dim + 1) + N * w.state_dim) * 4
 
     # ---- CPU baseline (rank 0, N = 1 only) ------------------------------------
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "batch":
         lib = ROOT / "oracle" / "_ref" / "libmppi_ref_unicycle_obstacles.so"
         if lib.exists():
             nthreads = os.cpu_count() or 1
@@ -359,8 +415,9 @@ def run_b200(args):
             torch.distributed.destroy_process_group()
         return 0
 
-    rollout_units = N * w.sample_count * w.horizon  # rollout-steps per rollout launch
-    roof = {"kernel": "mppi_rollout_b%d" % geom["block"], "bound": "issue",
+    rollout_units = rollout_steps_per_control_step(w)  # rollout-steps per rollout launch
+    kname = "mppi_rollout_work_b128" if ks is not None else "mppi_rollout_b%d" % geom["block"]
+    roof = {"kernel": kname, "bound": "issue",
             "launch_ms": rollout_ms, "combine_launch_ms": combine_ms,
             "rollout_steps_per_launch": rollout_units,
             "traffic": ROLLOUT_DRAM_BYTES_PER_LAUNCH, "unit": "Gwarp-inst/s",
@@ -368,7 +425,7 @@ def run_b200(args):
                     "achieved = ncu-counted warp-instructions per rollout-step x "
                     "rollout-steps per launch / live CUDA-event launch time"}
     clk = clocks.summary()
-    if ROLLOUT_WARP_INST_PER_ROLLOUT_STEP is not None:
+    if ROLLOUT_WARP_INST_PER_ROLLOUT_STEP is not None and args.workload == "batch":
         achieved = ROLLOUT_WARP_INST_PER_ROLLOUT_STEP * rollout_units / (rollout_ms / 1e3) / 1e9
         mhz = clk.get("sm_mhz") or 1965.0
         peak = 148 * 4 * mhz * 1e6 / 1e9
@@ -379,14 +436,15 @@ def run_b200(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
         "data": "synthetic (seeded PCG64 workload generator, mppi_metal_b200/models.py)",
-        "config": config_block(),
-        "control_steps_per_s": value / (w.sample_count * w.horizon),
+        "config": config_block(args.workload, w),
+        "control_steps_per_s": value * N / rollout_steps_per_control_step(w),
         "closed_loop_cost": {"mean": float(cost.mean()), "agents": N,
                              "mean_first_agents": float(cost[:8].mean())},
         "e2e": {"value": e2e_value, "unit": "rollout-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e2e_total / args.steps},
         "gpu_launches": 2 * T * args.steps,
         "launch_geometry": geom,
+        "autotuner": tuning or None,
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clk,

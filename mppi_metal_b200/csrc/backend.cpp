@@ -182,6 +182,8 @@ struct mppi_backend {
   DevBuf d_queue;            // atomic work counter
   std::string tuned_key;
   float tuned_ms = 0.0f;
+  LaunchGeom tuned_geom;     // the autotuner's choice for tuned_key
+  uint32_t tuned_grid = 0;
 
   // ---- closed-loop graph cache ----
   cudaGraphExec_t graph = nullptr;
@@ -468,6 +470,8 @@ int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
   b->geom = best_g;
   b->grid = best_grid;
   b->tuned_ms = best;
+  b->tuned_geom = best_g;
+  b->tuned_grid = best_grid;
   CK(cudaFuncSetAttribute((const void*)b->mod->rollout_work,
                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)best_g.smem));
   return MPPI_OK;
@@ -584,6 +588,12 @@ int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
     if (b->tuned_key != rk) {
       if (int rc = tune_ragged(b, err, err_len)) return rc;
       b->tuned_key = rk;
+    } else {
+      // prepare() re-derived the default geometry; restore the tuned one
+      b->geom = b->tuned_geom;
+      b->grid = b->tuned_grid;
+      CK(cudaFuncSetAttribute((const void*)b->mod->rollout_work,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem));
     }
   }
   const std::string key = std::string(keybuf) + (b->ragged ? "/r" + std::to_string(b->grid) + "/" +

@@ -263,3 +263,31 @@ def bicycle_uneven(seed: int = 0, N: int = 64, T: int = 100, k_range=(1024, 1638
     w.agent_K = Ks
     w.agent_H = Hs
     return w
+
+
+def bicycle_executed_cost(states: np.ndarray, terminal: np.ndarray, cost_blob: bytes) -> np.ndarray:
+    """Closed-loop lane-keeping cost of executed bicycle trajectories, per
+    agent: the stage cost over x_1..x_T plus the terminal cost of x_T."""
+    c = BicycleCostParams.from_buffer_copy(cost_blob)
+    coef = np.array([[c.coef[i][j] for j in range(4)] for i in range(c.num_segments)])
+    nxt = np.concatenate([states[1:], terminal[None]], axis=0).astype(np.float64)
+    x = np.clip(nxt[..., 0], c.x0, c.x0 + c.knot_dx * c.num_segments)
+    i = np.clip(np.floor((x - c.x0) / c.knot_dx).astype(int), 0, c.num_segments - 1)
+    sg = x - (c.x0 + c.knot_dx * i)
+    k = coef[i]
+    yc = k[..., 0] + sg * (k[..., 1] + sg * (k[..., 2] + sg * k[..., 3]))
+    slope = k[..., 1] + sg * (2.0 * k[..., 2] + sg * 3.0 * k[..., 3])
+    st = (c.w_lat * (nxt[..., 1] - yc) ** 2 + c.w_head * (nxt[..., 2] - np.arctan(slope)) ** 2
+          + c.w_speed * (nxt[..., 3] - c.v_ref) ** 2)
+    return st.sum(axis=0) + c.w_terminal * st[-1]
+
+
+def executed_cost(w: Workload, states, controls, terminal) -> np.ndarray:
+    """Executed closed-loop cost per agent for the shipped benchmark models."""
+    if w.plugin == "unicycle_obstacles":
+        blobs = w.cost_params if len(w.cost_params) == states.shape[1] else \
+            [w.cost_params[0]] * states.shape[1]
+        return unicycle_executed_cost(states, controls, terminal, blobs)
+    if w.plugin == "bicycle_lane":
+        return bicycle_executed_cost(states, terminal, w.cost_params[0])
+    return np.full(states.shape[1], np.nan)
