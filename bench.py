@@ -66,7 +66,10 @@ def parse():
                          "workload `--iters` times each (small capture target for ncu)")
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--workload", choices=WORKLOADS, default="batch",
-                    help="batch (default, the headline configuration), uneven, single")
+                    help="batch (default, the headline configuration), uneven, single, "
+                         "quadrotor")
+    ap.add_argument("--numeric", choices=["fp32", "mixed"], default="fp32",
+                    help="numeric mode of the quadrotor workload")
     return ap.parse_args()
 
 
@@ -75,17 +78,24 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
-WORKLOADS = ("batch", "uneven", "single")
+WORKLOADS = ("batch", "uneven", "single", "quadrotor")
 
 
-def workload_for_rank(rank: int, name: str = "batch"):
+def workload_for_rank(rank: int, name: str = "batch", numeric: str = "fp32"):
     """batch  : 256 unicycle agents per GPU, K 4096, H 50, 300 closed-loop steps
                 (the headline configuration);
     uneven : 64 kinematic-bicycle instances per GPU, K log-uniform [1024, 16384],
                 H log-uniform [16, 96], full 2x2 covariance, 100 closed-loop steps;
     single : one unicycle agent, K 1024, H 30, 8 static obstacles, control
-                cost on, 200 closed-loop steps from x0 = 0, Philox seed 0."""
+                cost on, 200 closed-loop steps from x0 = 0, Philox seed 0;
+    quadrotor : 32 quadrotors, n 12, m 4, dt 0.01, H 100, K 65536, 32
+                spherical obstacles each, 20 closed-loop steps, in the numeric
+                mode `numeric` (fp32, or mixed: FP16 noise)."""
     from mppi_metal_b200 import models
+    if name == "quadrotor":
+        w = models.quadrotor_batch(seed=3000 + rank, N=32, K=65536, H=100, T=20)
+        w.numeric_mode = 2 if numeric == "mixed" else 0
+        return w
     if name == "uneven":
         return models.bicycle_uneven(seed=2000 + rank, N=64, T=100)
     if name == "single":
@@ -246,6 +256,17 @@ def run_reference(args):
 
 
 def config_block(name: str = "batch", w=None):
+    if name == "quadrotor":
+        return {
+            "workload": ("quadrotor_batch: 32 quadrotors per GPU (n=12, m=4 rotor thrusts in "
+                         "[0, 2*hover]), dt=0.01, H=100, K=65536, waypoint tracking + 32 "
+                         "spherical obstacles, 20 closed-loop steps, numeric mode "
+                         + ("mixed (fp16 noise)" if w.numeric_mode else "fp32")),
+            "agents_per_gpu": 32, "samples": 65536, "horizon": 100, "closed_loop_steps": 20,
+            "step": "one simulate_batch closed loop (20 control steps for every agent)",
+            "l2": "flushed between timed iterations (256 MiB device write)",
+            "parallelism": "agent-sharded replicas, no data-path collective",
+        }
     if name == "uneven":
         return {
             "workload": ("bicycle_uneven: 64 kinematic-bicycle instances per GPU, K log-uniform "
@@ -297,7 +318,7 @@ def run_b200(args):
     from mppi_metal_b200._lib import plugin_path
     from mppi_metal_b200.backend import Backend
 
-    w = workload_for_rank(rank, args.workload)
+    w = workload_for_rank(rank, args.workload, args.numeric)
     N, T = w.num_agents, w.num_steps
     ks, hs = agent_shapes(w)
     rs_per_step = rollout_steps_per_control_step(w) * T  # per bench step (this rank)
@@ -319,7 +340,7 @@ def run_b200(args):
     b = Backend(w.plugin, w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam, w.sigma,
                 w.u_min, w.u_max, sigma_inv=w.sigma_inv, cov_full=w.cov_full,
                 control_cost=w.control_cost, model_params_size=len(w.model_params),
-                cost_params_size=w.cost_stride, seed=w.seed)
+                cost_params_size=w.cost_stride, seed=w.seed, numeric_mode=w.numeric_mode)
     b.bind_params(w.model_params, w.cost_params[0])
     b.prepare(N, T, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
               sigma=w.agent_sigma, sample_counts=ks, horizons=hs)
@@ -348,7 +369,8 @@ def run_b200(args):
     form = D.CovarianceForm.kFull if w.cov_full else D.CovarianceForm.kDiagonal
     cfg = D.DriverConfig(w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam,
                          D.ControlNoiseConfig(form, w.sigma, w.sigma_inv, w.control_dim),
-                         D.ControlBounds(w.u_min, w.u_max, w.control_dim))
+                         D.ControlBounds(w.u_min, w.u_max, w.control_dim),
+                         D.NumericMode(w.numeric_mode))
     drv = D.MPPIDriver(cfg, D.DriverOptions(control_cost=w.control_cost))
     err = D.ErrorRef()
     spec = D.ModelPluginSpec(plugin_path(w.plugin),
@@ -434,7 +456,8 @@ def run_b200(args):
     line = {
         "metric": METRIC, "value": value, "unit": "rollout-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32" if w.numeric_mode == 0 else "fp32 (fp16 noise)",
         "data": "synthetic (seeded PCG64 workload generator, mppi_metal_b200/models.py)",
         "config": config_block(args.workload, w),
         "control_steps_per_s": value * N / rollout_steps_per_control_step(w),

@@ -48,7 +48,11 @@ typedef struct mppi_backend_config {
   const float* sigma_inv;   /* same shape; read only when control_cost != 0 */
   const float* u_min;       /* control_dim */
   const float* u_max;       /* control_dim */
-  uint32_t numeric_mode;    /* DriverConfig::NumericMode (0 = FP32) */
+  uint32_t numeric_mode;    /* DriverConfig::NumericMode: 0 = FP32; 1 (kFp16) and 2
+                               (kMixed) draw the noise with approximate
+                               transcendentals and round it to FP16 (staged in
+                               FP16); dynamics, costs, weights and the update
+                               stay FP32 */
   uint32_t control_cost;    /* DriverOptions::control_cost */
 } mppi_backend_config;
 

@@ -59,6 +59,11 @@ struct DriverConfig {
 		kMixed
 	};
 
+	// kFp32: every value in FP32 (bit-exact Philox, accurate Box-Muller).
+	// kFp16 / kMixed: the noise is drawn with approximate transcendentals and
+	// rounded once to FP16, and that value is used by rollout and update
+	// alike; the plugin's dynamics and costs, the weights and the update stay
+	// FP32.  (The reference accepts the field and ignores it.)
 	NumericMode numeric_mode = NumericMode::kFp32;
 };
 

@@ -51,7 +51,7 @@ class Backend:
                  cov_full: bool = False, control_cost: bool = False,
                  stage_cost: str = "mppi_stage_cost", terminal_cost: str = "mppi_terminal_cost",
                  dynamics: str = "mppi_dynamics", model_params_size: int = 0,
-                 cost_params_size: int = 0, seed: int = 0):
+                 cost_params_size: int = 0, seed: int = 0, numeric_mode: int = 0):
         self.lib = _lib.load()
         h = ctypes.c_void_p()
         if self.lib.mppi_backend_create(ctypes.byref(h)) != _lib.MPPI_OK:
@@ -64,8 +64,8 @@ class Backend:
         sinv = _f32(sigma_inv if sigma_inv is not None else np.zeros_like(sig))
         lo, hi = _f32(u_min), _f32(u_max)
         cfg = _lib.BackendConfig(state_dim, control_dim, horizon, sample_count, lam,
-                                 1 if cov_full else 0, _p(sig), _p(sinv), _p(lo), _p(hi), 0,
-                                 1 if control_cost else 0)
+                                 1 if cov_full else 0, _p(sig), _p(sinv), _p(lo), _p(hi),
+                                 numeric_mode, 1 if control_cost else 0)
         path = plugin if plugin.endswith(".cu") or "/" in plugin else _lib.plugin_path(plugin)
         plug = _lib.BackendPlugin(path.encode(), dynamics.encode(), stage_cost.encode(),
                                   terminal_cost.encode(), model_params_size, cost_params_size,

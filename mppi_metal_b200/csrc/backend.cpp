@@ -139,6 +139,8 @@ struct mppi_backend {
   float lambda = 1.0f;
   bool cov_full = false;
   bool control_cost = false;
+  bool noise_half = false;   // NumericMode kFp16 / kMixed
+  size_t stage_elem = 4;     // bytes per staged noise value
   uint32_t seed = 0;
   uint64_t mp_size = 0, cp_size = 0;
   std::vector<float> sigma_dev;  // std-devs (diag) or Cholesky factor (full)
@@ -249,23 +251,30 @@ LaunchGeom choose_geometry(const mppi_backend* b) {
   const size_t budget = std::min<size_t>(b->max_smem_optin ? b->max_smem_optin : 232448, 232448);
   // Prefer 128 threads; fall back to 64 for very long horizons.
   const int order[2] = {1, 0};
+  const size_t el = b->stage_elem;
+  // Four 128-thread CTAs per SM (16 warps) hide this kernel's dependency
+  // latencies; staging the whole horizon is used only while it keeps that
+  // residency, otherwise the noise is staged (and regenerated) in chunks that
+  // fill the same per-CTA share of shared memory.
+  const size_t per_cta = budget / 4 - 1024;
   for (int vi : order) {
     const uint32_t block = mppi_b200::kRolloutBlocks[vi];
     const size_t fixed = pad4(HM) * 4 + (size_t)block * 4;
-    const size_t full = fixed + HM * block * 4;
+    const size_t full = fixed + HM * block * el;
     g.variant = vi;
     g.block = block;
-    if (full <= budget / 2 - 4096) {
+    if (full <= per_cta) {
       g.stage_rows = (uint32_t)HM;
       g.smem = full;
       break;
     }
-    // chunked regeneration: ~32 KB of staging, whole time steps per chunk
-    uint32_t rows = (uint32_t)(32768 / ((size_t)block * 4));
+    const size_t room = per_cta > fixed + (size_t)block * el * b->m ? per_cta - fixed
+                                                                     : (size_t)block * el * b->m;
+    uint32_t rows = (uint32_t)(room / ((size_t)block * el));
     rows = std::max<uint32_t>(b->m, rows / b->m * b->m);
     rows = std::min<uint32_t>(rows, (uint32_t)HM);
     g.stage_rows = rows;
-    g.smem = fixed + (size_t)rows * block * 4;
+    g.smem = fixed + (size_t)rows * block * el;
     if (vi == 1) break;
   }
   g.nblk = (b->K + g.block - 1) / g.block;
@@ -287,10 +296,10 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
       const size_t HM = b->HM();
       g.variant = 1;
       g.block = 128;
-      uint32_t rows = 32768 / (128 * 4);
+      uint32_t rows = (uint32_t)(32768 / (128 * b->stage_elem));
       rows = std::min<uint32_t>(std::max<uint32_t>(b->m, rows / b->m * b->m), (uint32_t)HM);
       g.stage_rows = rows;
-      g.smem = pad4(HM) * 4 + (size_t)128 * 4 + (size_t)rows * 128 * 4;
+      g.smem = pad4(HM) * 4 + (size_t)128 * 4 + (size_t)rows * 128 * b->stage_elem;
       g.pstride = (uint32_t)pad4(MPPI_PARTIAL_HEAD + HM);
     }
     uint32_t maxblk = 0;
@@ -421,9 +430,10 @@ int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
   const size_t HM = b->HM();
   const size_t budget = std::min<size_t>(b->max_smem_optin ? b->max_smem_optin : 232448, 232448);
   std::vector<uint32_t> stage_options;
-  const size_t full = pad4(HM) * 4 + 128 * 4 + HM * 128 * 4;
+  const size_t el = b->stage_elem;
+  const size_t full = pad4(HM) * 4 + 128 * 4 + HM * 128 * el;
   if (full <= budget - 2048) stage_options.push_back((uint32_t)HM);
-  uint32_t chunk = std::max<uint32_t>(b->m, (32768 / 512) / b->m * b->m);
+  uint32_t chunk = std::max<uint32_t>(b->m, (uint32_t)(32768 / (128 * el)) / b->m * b->m);
   stage_options.push_back(std::min<uint32_t>(chunk, (uint32_t)HM));
   std::vector<uint32_t> grids = {0};
   for (uint32_t c = 1; c <= 4; ++c) grids.push_back(c * (uint32_t)b->num_sms);
@@ -435,7 +445,7 @@ int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
   if (const char* r = getenv("MPPI_B200_UNEVEN_STAGE_ROWS"); r && *r) {
     const uint32_t rows = (uint32_t)strtoul(r, nullptr, 10);
     if (rows >= b->m && rows % b->m == 0) {
-      const size_t sm = pad4(HM) * 4 + 128 * 4 + (size_t)std::min<size_t>(rows, HM) * 128 * 4;
+      const size_t sm = pad4(HM) * 4 + 128 * 4 + (size_t)std::min<size_t>(rows, HM) * 128 * el;
       if (sm <= budget) stage_options.assign(1, (uint32_t)std::min<size_t>(rows, HM));
     }
   }
@@ -446,7 +456,7 @@ int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
   for (uint32_t rows : stage_options) {
     LaunchGeom g = base;
     g.stage_rows = rows;
-    g.smem = pad4(HM) * 4 + 128 * 4 + (size_t)rows * 128 * 4;
+    g.smem = pad4(HM) * 4 + 128 * 4 + (size_t)rows * 128 * el;
     b->geom = g;
     CK(cudaFuncSetAttribute((const void*)b->mod->rollout_work,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
@@ -717,6 +727,8 @@ int mppi_backend_initialize(mppi_backend* b, const mppi_backend_plugin* plugin,
   b->lambda = cfg->lambda;
   b->cov_full = cfg->covariance_form == 1;
   b->control_cost = cfg->control_cost != 0;
+  b->noise_half = cfg->numeric_mode != 0;  // kFp16 and kMixed: FP16 noise
+  b->stage_elem = b->noise_half ? 2 : 4;
   b->seed = (uint32_t)plugin->seed;  // metal_backend.mm:565
   b->mp_size = plugin->model_params_size;
   b->cp_size = plugin->cost_params_size;
@@ -747,6 +759,7 @@ int mppi_backend_initialize(mppi_backend* b, const mppi_backend_plugin* plugin,
   spec.control_dim = m;
   spec.cov_full = b->cov_full;
   spec.control_cost = b->control_cost;
+  spec.noise_half = b->noise_half;
   spec.model_params_bytes = b->mp_size;
   spec.cost_params_bytes = b->cp_size;
   std::string merr;
@@ -1199,6 +1212,7 @@ int mppi_compile_check(const mppi_backend_plugin* plugin, const mppi_backend_con
   spec.control_dim = cfg->control_dim;
   spec.cov_full = cfg->covariance_form == 1;
   spec.control_cost = cfg->control_cost != 0;
+  spec.noise_half = cfg->numeric_mode != 0;
   spec.model_params_bytes = plugin->model_params_size;
   spec.cost_params_bytes = plugin->cost_params_size;
   if (!valid_identifier(spec.dynamics.c_str())) {

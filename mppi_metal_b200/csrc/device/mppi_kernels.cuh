@@ -8,6 +8,9 @@
 //   MPPI_COV_FULL                           0: sigma = per-dim std-dev
 //                                           1: sigma = Cholesky factor L
 //   MPPI_CONTROL_COST                       1: add lambda * u_nom^T Sigma^-1 eps
+//   MPPI_NOISE_HALF                         1: noise drawn with approximate
+//                                           transcendentals, rounded to FP16,
+//                                           staged in FP16 (kFp16 / kMixed)
 //   MPPI_DYNAMICS_FN / _STAGE_COST_FN / _TERMINAL_COST_FN   callable names
 //   MPPI_MP_BYTES / MPPI_CP_BYTES           ParamLayout blob sizes
 //
@@ -47,6 +50,9 @@
 #ifndef MPPI_CONTROL_COST
 #define MPPI_CONTROL_COST 0
 #endif
+#ifndef MPPI_NOISE_HALF
+#define MPPI_NOISE_HALF 0
+#endif
 #ifndef MPPI_MP_BYTES
 #define MPPI_MP_BYTES 0
 #endif
@@ -83,6 +89,17 @@ typedef typename mppi_first_arg<decltype(&MPPI_STAGE_COST_FN)>::type StageStateT
 typedef typename mppi_first_arg<decltype(&MPPI_TERMINAL_COST_FN)>::type TermStateT;
 
 __device__ __forceinline__ float pos_inf() { return __int_as_float(0x7f800000); }
+
+// Element type of the shared-memory noise staging buffer.
+#if MPPI_NOISE_HALF
+typedef uint16_t stage_t;
+__device__ __forceinline__ stage_t to_stage(float x) { return mppi_f32_to_f16(x); }
+__device__ __forceinline__ float from_stage(stage_t h) { return mppi_f16_to_f32(h); }
+#else
+typedef float stage_t;
+__device__ __forceinline__ stage_t to_stage(float x) { return x; }
+__device__ __forceinline__ float from_stage(stage_t x) { return x; }
+#endif
 
 __device__ __forceinline__ float warp_min(float v) {
 #pragma unroll
@@ -146,7 +163,11 @@ __device__ __forceinline__ void sample_noise(uint32_t step, uint32_t key, uint32
 #pragma unroll
   for (int p = 0; p < kP; ++p) {
     const uint2 w = mppi_philox2x32_10(make_uint2(step, mppi_noise_ctr(k, H, kP, t, p)), key);
+#if MPPI_NOISE_HALF
+    const float2 g = mppi_box_muller_fast(w);
+#else
     const float2 g = mppi_box_muller(w);
+#endif
     n[2 * p] = g.x;
     n[2 * p + 1] = g.y;
   }
@@ -161,6 +182,10 @@ __device__ __forceinline__ void sample_noise(uint32_t step, uint32_t key, uint32
 #else
 #pragma unroll
   for (int d = 0; d < kM; ++d) eps[d] = n[d] * sig[d];
+#endif
+#if MPPI_NOISE_HALF
+#pragma unroll
+  for (int d = 0; d < kM; ++d) eps[d] = from_stage(to_stage(eps[d]));
 #endif
 }
 
@@ -206,8 +231,8 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   const bool staged = a.stage_rows >= HM;
 
   float* un_s = dsm;
-  float* stage_s = dsm + ((a.H * kM + 3) & ~3u);
-  float* e_s = stage_s + (size_t)a.stage_rows * BLOCK;
+  stage_t* stage_s = reinterpret_cast<stage_t*>(dsm + ((a.H * kM + 3) & ~3u));
+  float* e_s = reinterpret_cast<float*>(stage_s + (size_t)a.stage_rows * BLOCK);
 
   for (uint32_t i = tid; i < HM; i += BLOCK) un_s[i] = un_g[i];
   const uint8_t* mp_g = a.model_params + a.model_stride * agent;
@@ -267,14 +292,15 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
         for (int d = 0; d < kM; ++d) eps[d] = 0.0f;
       }
 #pragma unroll
-      for (int d = 0; d < kM; ++d) stage_s[(size_t)((t - row0) * kM + d) * BLOCK + tid] = eps[d];
+      for (int d = 0; d < kM; ++d)
+        stage_s[(size_t)((t - row0) * kM + d) * BLOCK + tid] = to_stage(eps[d]);
     }
     if (active) {
       for (uint32_t t = t0; t < t1; ++t) {
         float eps[kM], u[kM];
 #pragma unroll
         for (int d = 0; d < kM; ++d) {
-          eps[d] = stage_s[(size_t)((t - row0) * kM + d) * BLOCK + tid];
+          eps[d] = from_stage(stage_s[(size_t)((t - row0) * kM + d) * BLOCK + tid]);
           u[d] = clampf(un_s[t * kM + d] + eps[d], lo[d], hi[d]);
         }
 #if MPPI_CONTROL_COST
@@ -328,7 +354,7 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   const uint32_t R = staged ? HM : a.stage_rows;  // rows per chunk (multiple of m)
   for (uint32_t r0 = 0; r0 < HM; r0 += R) {
     const uint32_t rows = min(R, HM - r0);
-    const float* base = stage_s;
+    const stage_t* base = stage_s;
     if (!staged) {
       // regenerate this chunk's noise (same counters, same values)
       __syncthreads();
@@ -343,17 +369,17 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
         }
 #pragma unroll
         for (int d = 0; d < kM; ++d)
-          stage_s[(size_t)((t - t0) * kM + d) * BLOCK + tid] = eps[d];
+          stage_s[(size_t)((t - t0) * kM + d) * BLOCK + tid] = to_stage(eps[d]);
       }
       __syncthreads();
     } else {
       base = stage_s + (size_t)r0 * BLOCK;
     }
     for (uint32_t r = warp; r < rows; r += NW) {
-      const float* row = base + (size_t)r * BLOCK;
+      const stage_t* row = base + (size_t)r * BLOCK;
       float s = 0.0f;
 #pragma unroll
-      for (int i = 0; i < PER_LANE; ++i) s = fmaf(e_r[i], row[lane + 32 * i], s);
+      for (int i = 0; i < PER_LANE; ++i) s = fmaf(e_r[i], from_stage(row[lane + 32 * i]), s);
       s = warp_sum(s);
       if (lane == 0) part[MPPI_PARTIAL_HEAD + r0 + r] = s;
     }

@@ -119,6 +119,20 @@ __device__ __forceinline__ float2 mppi_box_muller(uint2 w) {
   return make_float2(r * c, r * s);
 }
 
+// Half-precision noise mode (DriverConfig::NumericMode kFp16 / kMixed): the
+// shaped noise is rounded once to IEEE binary16 (round to nearest even) and
+// that rounded value is used everywhere -- rollout and weighted update alike.
+__device__ __forceinline__ uint16_t mppi_f32_to_f16(float x) {
+  uint16_t h;
+  asm("cvt.rn.f16.f32 %0, %1;" : "=h"(h) : "f"(x));
+  return h;
+}
+__device__ __forceinline__ float mppi_f16_to_f32(uint16_t h) {
+  float f;
+  asm("cvt.f32.f16 %0, %1;" : "=f"(f) : "h"(h));
+  return f;
+}
+
 // Square root by the SM's approximate square-root instruction (PTX
 // sqrt.approx.f32, relative error of order 2^-23): one instruction, exact
 // zero at zero.  For plugin cost terms where a few ulps do not matter.
@@ -126,6 +140,21 @@ __device__ __forceinline__ float mppi_sqrt_approx(float x) {
   float r;
   asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
+}
+
+// Box-Muller with the SM's approximate log2 / sqrt / sin / cos (relative
+// errors of order 2^-21), for the half-precision noise mode whose output is
+// rounded to 11 significant bits anyway.  The angle is taken as
+// 2 pi (u2 - 1/2), inside (-pi, pi) where the approximate sine / cosine are
+// accurate, and sin / cos(t + pi) = -sin / cos(t) restores the reference's
+// angle 2 pi u2.
+__device__ __forceinline__ float2 mppi_box_muller_fast(uint2 w) {
+  const float u1 = mppi_uint_to_01(w.x);
+  const float u2 = mppi_uint_to_01(w.y);
+  const float r = mppi_sqrt_approx(-2.0f * __logf(u1));
+  float s, c;
+  __sincosf(6.28318530717958647692f * (u2 - 0.5f), &s, &c);
+  return make_float2(-r * c, -r * s);
 }
 
 // Reference-compatible spellings for plugins ported from MSL

@@ -143,6 +143,7 @@ int compile_module(const ModuleSpec& spec, bool use_cache, bool ptxas_verbose,
       "-DMPPI_CONTROL_DIM=" + std::to_string(spec.control_dim),
       "-DMPPI_COV_FULL=" + std::to_string(spec.cov_full ? 1 : 0),
       "-DMPPI_CONTROL_COST=" + std::to_string(spec.control_cost ? 1 : 0),
+      "-DMPPI_NOISE_HALF=" + std::to_string(spec.noise_half ? 1 : 0),
       "-DMPPI_MP_BYTES=" + std::to_string(spec.model_params_bytes),
       "-DMPPI_CP_BYTES=" + std::to_string(spec.cost_params_bytes),
       "-DMPPI_DYNAMICS_FN=" + spec.dynamics,

@@ -27,6 +27,7 @@ struct ModuleSpec {
   uint32_t control_dim = 0;
   bool cov_full = false;
   bool control_cost = false;
+  bool noise_half = false;  // NumericMode kFp16 / kMixed: FP16 noise
   uint64_t model_params_bytes = 0;
   uint64_t cost_params_bytes = 0;
 };

@@ -92,6 +92,7 @@ class Workload:
     cov_full: bool = False
     control_cost: bool = False
     seed: int = 0
+    numeric_mode: int = 0  # DriverConfig::NumericMode (0 FP32, 1 FP16, 2 mixed)
 
     @property
     def cost_params_packed(self) -> bytes:
@@ -290,4 +291,54 @@ def executed_cost(w: Workload, states, controls, terminal) -> np.ndarray:
         return unicycle_executed_cost(states, controls, terminal, blobs)
     if w.plugin == "bicycle_lane":
         return bicycle_executed_cost(states, terminal, w.cost_params[0])
+    if w.plugin == "quadrotor":
+        return np.array([quadrotor_executed_cost(states[:, a], terminal[a], w.cost_params[a])
+                         for a in range(states.shape[1])])
     return np.full(states.shape[1], np.nan)
+
+
+def quadrotor_executed_cost(states: np.ndarray, terminal: np.ndarray, cost_blob: bytes) -> float:
+    """Closed-loop cost of one executed quadrotor trajectory (states [T][12],
+    terminal [12]): stage cost over x_1..x_T plus terminal cost of x_T."""
+    c = QuadrotorCostParams.from_buffer_copy(cost_blob)
+    nxt = np.concatenate([states[1:], terminal[None]], axis=0).astype(np.float64)
+    p = nxt[:, 0:3]
+    pos = c.w_pos * np.sum((p - np.array([c.wp_x, c.wp_y, c.wp_z])) ** 2, axis=1)
+    n = min(int(c.num_obs), QUAD_MAX_OBS)
+    ctr = np.stack([np.array(c.obs_cx[:n]), np.array(c.obs_cy[:n]), np.array(c.obs_cz[:n])], 1)
+    d = np.sqrt(np.sum((p[:, None, :] - ctr[None]) ** 2, axis=2))
+    pen = np.maximum(np.array(c.obs_r[:n])[None] - d, 0.0).sum(axis=1)
+    st = (pos + c.w_vel * np.sum(nxt[:, 3:6] ** 2, 1) + c.w_att * np.sum(nxt[:, 6:8] ** 2, 1)
+          + c.w_rate * np.sum(nxt[:, 9:12] ** 2, 1) + c.w_obs * pen)
+    return float(st.sum() + c.w_terminal * pos[-1])
+
+
+def quadrotor_batch(seed: int = 0, N: int = 32, K: int = 65536, H: int = 100, T: int = 100,
+                    n_obs: int = 32) -> Workload:
+    """Large rollout: N 12-state quadrotors (position, velocity, Euler
+    angles, body rates; four rotor thrusts in [0, 2 * hover]), dt 0.01,
+    H 100, K 65536, waypoint tracking and 32 spherical obstacles per agent."""
+    rng = np.random.default_rng(seed)
+    mp = QuadrotorModelParams(0.01, 1.0, 9.81, 0.25, 0.02, 0.01, 0.01, 0.02)
+    hover = 1.0 * 9.81 / 4.0
+    x0 = np.zeros((N, 12), np.float32)
+    x0[:, 0:2] = rng.uniform(-4.0, 4.0, size=(N, 2))
+    x0[:, 2] = 1.0
+    cps = []
+    for _ in range(N):
+        c = QuadrotorCostParams()
+        c.wp_x, c.wp_y = (float(v) for v in rng.uniform(-4.0, 4.0, size=2))
+        c.wp_z = float(rng.uniform(1.0, 3.0))
+        c.w_pos, c.w_vel, c.w_att, c.w_rate = 1.0, 0.1, 0.1, 0.01
+        c.w_obs, c.w_terminal = 1.0e3, 10.0
+        c.num_obs = n_obs
+        for i in range(n_obs):
+            c.obs_cx[i], c.obs_cy[i] = (float(v) for v in rng.uniform(-5.0, 5.0, size=2))
+            c.obs_cz[i] = float(rng.uniform(0.0, 4.0))
+            c.obs_r[i] = float(rng.uniform(0.2, 0.6))
+        cps.append(blob(c))
+    sigma = np.full(4, 1.0, np.float32)
+    return Workload("quadrotor_batch", "quadrotor", "quadrotor", 12, 4, H, K, 1.0, sigma,
+                    (1.0 / sigma ** 2).astype(np.float32), np.zeros(4, np.float32),
+                    np.full(4, 2.0 * hover, np.float32), N, T, x0, blob(mp), cps, None,
+                    seed=seed)

@@ -104,6 +104,7 @@ void oracle_sample_noise(const oracle_problem* p, uint32_t step, uint32_t key,
         } else {
           e = n[d] * sigma[d];
         }
+        if (p->noise_half) e = (double)(_Float16)(float)e; /* round to binary16 */
         eps[t * m + d] = e;
       }
     }
@@ -366,6 +367,39 @@ void oracle_rollout(const oracle_problem* p, uint32_t step, uint32_t key,
     costs[k] = J;
   }
   free(eps);
+}
+
+void oracle_rollout_eps(const oracle_problem* p, const double* x0, const double* u_nom,
+                        const void* model_params, const void* cost_params,
+                        const double* eps_all, double* costs) {
+  const uint32_t n = p->state_dim, m = p->control_dim, H = p->horizon, K = p->sample_count;
+  for (uint32_t k = 0; k < K; ++k) {
+    const double* eps = eps_all + (uint64_t)k * H * m;
+    double s[MAX_STATE];
+    for (uint32_t d = 0; d < n && d < MAX_STATE; ++d) s[d] = x0[d];
+    double J = 0.0;
+    for (uint32_t t = 0; t < H; ++t) {
+      double u[MAX_CTRL];
+      for (uint32_t d = 0; d < m; ++d)
+        u[d] = clampd(u_nom[t * m + d] + eps[t * m + d], p->u_min[d], p->u_max[d]);
+      if (p->control_cost) J += control_cost_term(p, u_nom + t * m, eps + t * m);
+      oracle_dynamics(p, s, u, model_params, 0, 0, 0);
+      J += oracle_stage_cost(p, s, u, model_params, cost_params);
+    }
+    J += oracle_terminal_cost(p, s, model_params, cost_params);
+    costs[k] = J;
+  }
+}
+
+void oracle_update_eps(const oracle_problem* p, const double* weights, const double* u_nom,
+                       const double* eps_all, double* u_out) {
+  const uint32_t m = p->control_dim, H = p->horizon, K = p->sample_count, L = H * m;
+  for (uint32_t j = 0; j < L; ++j) {
+    double acc = 0.0;
+    for (uint32_t k = 0; k < K; ++k) acc += weights[k] * eps_all[(uint64_t)k * L + j];
+    const uint32_t d = j % m;
+    u_out[j] = clampd(u_nom[j] + acc, p->u_min[d], p->u_max[d]);
+  }
 }
 
 /* ---- weights (shaders/mppi_reduce.metal:14-121) ------------------------- */

@@ -55,7 +55,7 @@ typedef struct {
   int32_t model;        /* ORACLE_MODEL_* */
   int32_t use_stage;    /* 0: library default stage cost (returns 0) */
   int32_t use_terminal; /* 0: library default terminal cost (returns 0) */
-  int32_t pad;
+  int32_t noise_half;   /* 1: shaped noise rounded to IEEE binary16 (kFp16 / kMixed) */
   const double* sigma;     /* m (diag) or m*m (full, row-major covariance) */
   const double* sigma_inv; /* m or m*m; read only when control_cost != 0 */
   const double* u_min;     /* m */
@@ -105,6 +105,14 @@ double oracle_stage_cost(const oracle_problem* p, const double* x,
                          const void* cost_params);
 double oracle_terminal_cost(const oracle_problem* p, const double* x,
                             const void* model_params, const void* cost_params);
+
+/* The rollout and the update on a given noise array eps[K][H][m] (for
+ * checking a device pass against the oracle on the device's own noise). */
+void oracle_rollout_eps(const oracle_problem* p, const double* x0, const double* u_nom,
+                        const void* model_params, const void* cost_params,
+                        const double* eps_all, double* costs);
+void oracle_update_eps(const oracle_problem* p, const double* weights, const double* u_nom,
+                       const double* eps_all, double* u_out);
 
 /* One control step for one agent: rollout -> weights -> update. */
 int oracle_step(const oracle_problem* p, uint32_t step, uint32_t key,

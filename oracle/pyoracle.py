@@ -75,7 +75,8 @@ class _OracleProblem(ctypes.Structure):
         ("state_dim", _u32), ("control_dim", _u32), ("horizon", _u32), ("sample_count", _u32),
         ("lambda_", ctypes.c_double),
         ("cov_full", ctypes.c_int32), ("control_cost", ctypes.c_int32), ("model", ctypes.c_int32),
-        ("use_stage", ctypes.c_int32), ("use_terminal", ctypes.c_int32), ("pad", ctypes.c_int32),
+        ("use_stage", ctypes.c_int32), ("use_terminal", ctypes.c_int32),
+        ("noise_half", ctypes.c_int32),
         ("sigma", _P), ("sigma_inv", _P), ("u_min", _P), ("u_max", _P),
         ("model_params", _P), ("cost_params", _P),
     ]
@@ -104,6 +105,7 @@ class Problem:
     control_cost: bool = False
     use_stage: bool = True
     use_terminal: bool = True
+    noise_half: bool = False
     model_params: bytes = b""
     cost_params: bytes = b""
     _keep: list = field(default_factory=list, repr=False)
@@ -138,7 +140,7 @@ class Oracle:
         sigma_inv = p.sigma_inv if p.sigma_inv is not None else np.zeros_like(np.asarray(p.sigma))
         s = _OracleProblem(p.state_dim, p.control_dim, p.horizon, p.sample_count, p.lam,
                            int(p.cov_full), int(p.control_cost), MODEL_IDS[p.model],
-                           int(p.use_stage), int(p.use_terminal), 0,
+                           int(p.use_stage), int(p.use_terminal), int(p.noise_half),
                            arr(p.sigma), arr(sigma_inv), arr(p.u_min), arr(p.u_max),
                            blob(p.model_params), blob(p.cost_params))
         s._keep = keep
@@ -184,6 +186,24 @@ class Oracle:
         self.lib.oracle_rollout(ctypes.byref(s), _u32(step), _u32(key), _ptr(x0), _ptr(u_nom),
                                 _ptr(sig), mp, cp, _ptr(costs))
         return costs
+
+    def rollout_eps(self, p: Problem, x0, u_nom, eps_all):
+        """Rollout costs on a given noise array [K][H][m]."""
+        s = self._prob(p)
+        x0, u_nom, eps = _f64(x0), _f64(u_nom), _f64(eps_all)
+        mp = ctypes.create_string_buffer(p.model_params or b"\0", max(1, len(p.model_params)))
+        cp = ctypes.create_string_buffer(p.cost_params or b"\0", max(1, len(p.cost_params)))
+        costs = np.zeros(p.sample_count)
+        self.lib.oracle_rollout_eps(ctypes.byref(s), _ptr(x0), _ptr(u_nom), mp, cp, _ptr(eps),
+                                    _ptr(costs))
+        return costs
+
+    def update_eps(self, p: Problem, weights, u_nom, eps_all):
+        s = self._prob(p)
+        w, u_nom, eps = _f64(weights), _f64(u_nom), _f64(eps_all)
+        out = np.zeros(p.horizon * p.control_dim)
+        self.lib.oracle_update_eps(ctypes.byref(s), _ptr(w), _ptr(u_nom), _ptr(eps), _ptr(out))
+        return out
 
     def weights(self, costs, lam: float):
         costs = _f64(costs)

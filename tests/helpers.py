@@ -16,7 +16,7 @@ def oracle_problem(w: models.Workload, use_stage=True, use_terminal=True,
         np.asarray(w.sigma, np.float64), np.asarray(w.u_min, np.float64),
         np.asarray(w.u_max, np.float64), sigma_inv=np.asarray(w.sigma_inv, np.float64),
         cov_full=w.cov_full, control_cost=w.control_cost, use_stage=use_stage,
-        use_terminal=use_terminal, model_params=w.model_params,
+        use_terminal=use_terminal, noise_half=w.numeric_mode != 0, model_params=w.model_params,
         cost_params=cost_params if cost_params is not None
         else (w.cost_params[0] if w.cost_params else b""))
 
@@ -30,7 +30,7 @@ def backend_for(w: models.Workload, use_stage=True, use_terminal=True, bind=True
                 terminal_cost="mppi_terminal_cost" if use_terminal else "",
                 model_params_size=len(w.model_params),
                 cost_params_size=len(w.cost_params[0]) if w.cost_params else 0,
-                seed=w.seed if seed is None else seed)
+                seed=w.seed if seed is None else seed, numeric_mode=w.numeric_mode)
     if bind and (w.model_params or w.cost_params):
         b.bind_params(w.model_params or None, w.cost_params[0] if w.cost_params else None)
     return b
