@@ -211,6 +211,44 @@ int mppi_backend_dispatch_rollout_noalloc(mppi_backend* b, uint64_t step_index, 
                                           const void* cost_params, float* u_out, float* diag3,
                                           char* err, size_t err_len);
 
+/* ---- learned proposal ---------------------------------------------------
+ * No counterpart in the reference (its rollouts all sample around the warm
+ * start, shaders/mppi_rollout.metal:96-112).  The network is the object of
+ * mppi_proposal.h; the plugin supplies its input through a feature callable
+ *   __device__ void f(const float* state, const uint8_t* model_params,
+ *                     const uint8_t* cost_params, float* features);
+ * that writes up to 32 features (the array arrives zeroed).
+ *
+ * set_features compiles the callable into the module (NULL / "" removes it;
+ * feature_dim = features used, 1..32).  features evaluates it on host state
+ * rows [rows][state_dim]: row r belongs to agent r % agents_mod, whose blobs
+ * come from the prepared batch (agents_mod == its num_agents) or the bound
+ * params (agents_mod == 1); out is [rows][feature_dim].
+ *
+ * set_proposal attaches a network (NULL detaches; the caller keeps ownership
+ * and keeps it alive while attached): every later step -- dispatch_rollout,
+ * the closed loops and batches -- first evaluates the features of the
+ * current states and the network, then draws samples k <
+ * proposal_samples of each agent as (mu - u_nom) + exp(clamp(s)) * n around
+ * the predicted sequence mu with the predicted log-scales s, and the other
+ * samples as before.  Weights, update and warm start are unchanged.  Needs
+ * the network's control_dim == control_dim, horizon >= horizon and
+ * input_dim <= feature_dim.  Takes effect at the next prepare.
+ *
+ * set_record_ustar (next prepare on) makes the batch closed loop keep the
+ * updated sequence u* of every step; batch_fetch_ustar copies it out as
+ * [num_steps][num_agents][horizon * control_dim] (the training targets of
+ * the network; the matching states are the batch's state history). */
+struct mppi_proposal; /* include/mppi_b200/mppi_proposal.h */
+int mppi_backend_set_features(mppi_backend* b, const char* callable, uint32_t feature_dim,
+                              char* err, size_t err_len);
+int mppi_backend_features(mppi_backend* b, const float* states, uint32_t rows,
+                          uint32_t agents_mod, float* out, char* err, size_t err_len);
+int mppi_backend_set_proposal(mppi_backend* b, struct mppi_proposal* proposal,
+                              uint32_t proposal_samples, char* err, size_t err_len);
+int mppi_backend_set_record_ustar(mppi_backend* b, uint32_t enable, char* err, size_t err_len);
+int mppi_backend_batch_fetch_ustar(mppi_backend* b, float* ustar_out, char* err, size_t err_len);
+
 /* Compiles a plugin with the library kernels for sm_100a without loading
  * the result (needs no GPU).  log receives the NVRTC log, including ptxas's
  * register / shared-memory / spill report for every kernel. */

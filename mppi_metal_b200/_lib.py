@@ -79,6 +79,15 @@ class DriverPluginC(ctypes.Structure):
     ]
 
 
+class ProposalConfig(ctypes.Structure):
+    """mppi_proposal_config (include/mppi_b200/mppi_proposal.h)."""
+    _fields_ = [
+        ("input_dim", c_u32), ("horizon", c_u32), ("control_dim", c_u32),
+        ("max_batch", c_u32), ("seed", c_u64), ("log_scale_min", c_f32),
+        ("log_scale_max", c_f32),
+    ]
+
+
 # name -> (restype, argtypes); every symbol the headers in include/mppi_b200 declare.
 _ERR = [ctypes.c_char_p, c_size]
 SIGNATURES = {
@@ -116,10 +125,28 @@ SIGNATURES = {
     "mppi_device_philox": (ctypes.c_int, [c_u64, c_ptr, c_ptr, c_ptr, c_ptr] + _ERR),
     "mppi_backend_dispatch_rollout_noalloc": (ctypes.c_int, [c_ptr, c_u64, c_ptr, c_ptr, c_ptr,
                                                              c_ptr, c_ptr, c_ptr] + _ERR),
+    "mppi_backend_set_features": (ctypes.c_int, [c_ptr, ctypes.c_char_p, c_u32] + _ERR),
+    "mppi_backend_features": (ctypes.c_int, [c_ptr, c_ptr, c_u32, c_u32, c_ptr] + _ERR),
+    "mppi_backend_set_proposal": (ctypes.c_int, [c_ptr, c_ptr, c_u32] + _ERR),
+    "mppi_backend_set_record_ustar": (ctypes.c_int, [c_ptr, c_u32] + _ERR),
+    "mppi_backend_batch_fetch_ustar": (ctypes.c_int, [c_ptr, c_ptr] + _ERR),
     "mppi_compile_check": (ctypes.c_int, [ctypes.POINTER(BackendPlugin),
                                           ctypes.POINTER(BackendConfig), ctypes.c_char_p,
                                           c_size] + _ERR),
     "mppi_b200_version": (ctypes.c_char_p, []),
+    # mppi_proposal.h
+    "mppi_proposal_create": (c_ptr, [ctypes.POINTER(ProposalConfig)] + _ERR),
+    "mppi_proposal_destroy": (None, [c_ptr]),
+    "mppi_proposal_param_count": (c_u64, [c_ptr]),
+    "mppi_proposal_output_stride": (c_u32, [c_ptr]),
+    "mppi_proposal_set_params": (ctypes.c_int, [c_ptr, c_ptr, c_u64] + _ERR),
+    "mppi_proposal_get_params": (ctypes.c_int, [c_ptr, c_ptr, c_u64] + _ERR),
+    "mppi_proposal_forward": (ctypes.c_int, [c_ptr, c_ptr, c_u32, c_u32, c_ptr] + _ERR),
+    "mppi_proposal_gradients": (ctypes.c_int, [c_ptr, c_ptr, c_u32, c_ptr, c_u32, c_ptr, c_u32,
+                                               ctypes.POINTER(c_f32), c_ptr] + _ERR),
+    "mppi_proposal_train_step": (ctypes.c_int, [c_ptr, c_ptr, c_u32, c_ptr, c_u32, c_ptr, c_u32,
+                                                c_f32, ctypes.POINTER(c_f32)] + _ERR),
+    "mppi_proposal_last_train_ms": (c_f32, [c_ptr]),
     # mppi_driver_c.h
     "mppi_driver_create": (c_ptr, [ctypes.POINTER(DriverConfigC)]),
     "mppi_driver_destroy": (None, [c_ptr]),

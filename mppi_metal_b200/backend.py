@@ -198,6 +198,41 @@ class Backend:
         self.N, self.T = N, T
         return dict(states=st, controls=ct, costs=co, terminal=te)
 
+    # -- learned proposal -------------------------------------------------------
+    def set_features(self, callable_name: Optional[str], feature_dim: int = 0) -> None:
+        """Compile the plugin's proposal-feature callable into the module."""
+        eb = _lib.err_buf()
+        name = callable_name.encode() if callable_name else None
+        _check(self.lib.mppi_backend_set_features(self.h, name, feature_dim, eb, len(eb)), eb)
+        self.feature_dim = feature_dim if callable_name else 0
+
+    def features(self, states, agents_mod: int = 1) -> np.ndarray:
+        """Features of host state rows [rows][n] (row r: agent r % agents_mod)."""
+        x = _f32(states).reshape(-1, self.n)
+        out = np.zeros((x.shape[0], self.feature_dim), np.float32)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_features(self.h, _p(x), x.shape[0], agents_mod, _p(out), eb,
+                                              len(eb)), eb)
+        return out
+
+    def set_proposal(self, net, proposal_samples: int = 0) -> None:
+        """Attach a ProposalNet (None detaches); takes effect at the next prepare."""
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_set_proposal(self.h, None if net is None else net.h,
+                                                  proposal_samples, eb, len(eb)), eb)
+        self._proposal = net  # keep the network alive while attached
+
+    def set_record_ustar(self, enable: bool) -> None:
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_set_record_ustar(self.h, int(enable), eb, len(eb)), eb)
+
+    def fetch_ustar(self) -> np.ndarray:
+        """u* of every step of the last recorded batch: [T][N][H][m]."""
+        out = np.zeros((self.T, self.N, self.H, self.m), np.float32)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_batch_fetch_ustar(self.h, _p(out), eb, len(eb)), eb)
+        return out
+
     # -- inspection ------------------------------------------------------------
     def last_costs(self, a0: int = 0, n: Optional[int] = None) -> np.ndarray:
         n = self.N - a0 if n is None else n

@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "device/mppi_launch.h"
+#include "proposal.hpp"
 #include "nvrtc_module.hpp"
 
 namespace {
@@ -45,6 +46,8 @@ void set_err(char* err, size_t len, const std::string& msg) {
 
 size_t pad4(size_t n) { return (n + 3) & ~size_t(3); }
 size_t pad16(size_t n) { return (n + 15) & ~size_t(15); }
+
+constexpr uint32_t kFeatureStride = 32;  // floats per feature row (network input)
 
 struct DevBuf {
   void* p = nullptr;
@@ -147,6 +150,7 @@ struct mppi_backend {
   std::vector<float> sigma_inv;
   std::vector<float> u_min, u_max;
   std::shared_ptr<const KernelModule> mod;
+  mppi_b200::ModuleSpec spec;  // what `mod` was compiled from
   int num_sms = 148;
   size_t max_smem_optin = 0;
 
@@ -187,6 +191,15 @@ struct mppi_backend {
   LaunchGeom tuned_geom;     // the autotuner's choice for tuned_key
   uint32_t tuned_grid = 0;
 
+  // ---- learned proposal ----
+  uint32_t feature_dim = 0;            // features per row (plugin callable)
+  mppi_proposal* proposal = nullptr;   // attached network (not owned)
+  uint32_t prop_samples = 0;           // samples per agent drawn from it
+  DevBuf d_feat;                       // [N][32] features of the current states
+  DevBuf d_prop;                       // [N][out_stride] network outputs
+  bool record_ustar = false;
+  DevBuf d_hu;                         // [T][N][H*m] u* of every closed-loop step
+
   // ---- closed-loop graph cache ----
   cudaGraphExec_t graph = nullptr;
   std::string graph_key;
@@ -217,6 +230,12 @@ struct mppi_backend {
 };
 
 namespace {
+
+// Shared memory of a rollout CTA in front of the noise staging: the nominal
+// sequence, plus the proposal's mean shift in modules compiled for one.
+size_t nominal_bytes(const mppi_backend* b) {
+  return pad4(b->HM()) * 4 * (b->spec.proposal ? 2 : 1);
+}
 
 #define CK(call)                                                                      \
   do {                                                                                \
@@ -259,7 +278,7 @@ LaunchGeom choose_geometry(const mppi_backend* b) {
   const size_t per_cta = budget / 4 - 1024;
   for (int vi : order) {
     const uint32_t block = mppi_b200::kRolloutBlocks[vi];
-    const size_t fixed = pad4(HM) * 4 + (size_t)block * 4;
+    const size_t fixed = nominal_bytes(b) + (size_t)block * 4;
     const size_t full = fixed + HM * block * el;
     g.variant = vi;
     g.block = block;
@@ -299,7 +318,7 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
       uint32_t rows = (uint32_t)(32768 / (128 * b->stage_elem));
       rows = std::min<uint32_t>(std::max<uint32_t>(b->m, rows / b->m * b->m), (uint32_t)HM);
       g.stage_rows = rows;
-      g.smem = pad4(HM) * 4 + (size_t)128 * 4 + (size_t)rows * 128 * b->stage_elem;
+      g.smem = nominal_bytes(b) + (size_t)128 * 4 + (size_t)rows * 128 * b->stage_elem;
       g.pstride = (uint32_t)pad4(MPPI_PARTIAL_HEAD + HM);
     }
     uint32_t maxblk = 0;
@@ -319,6 +338,12 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
   if (wc) CK(b->d_hc.ensure((size_t)T * N * b->m * 4, &grew));
   if (wk) CK(b->d_hk.ensure((size_t)T * N * 4, &grew));
   if (wt) CK(b->d_term.ensure((size_t)N * b->n * 4, &grew));
+  if (b->record_ustar && T) CK(b->d_hu.ensure((size_t)T * N * b->HM() * 4, &grew));
+  if (b->proposal) {
+    const mppi_b200::ProposalShape ps = mppi_b200::proposal_shape(b->proposal);
+    CK(b->d_feat.ensure((size_t)N * kFeatureStride * 4, &grew));
+    CK(b->d_prop.ensure((size_t)N * ps.out_stride * 4, &grew));
+  }
   CK(b->h_up.ensure((b->off_uout() + 64) * 4 + 2 * pad16(b->mp_size + b->cp_size) + 64));
   CK(b->h_down.ensure((b->io_floats() + 64) * 4));
   if (grew) ++b->generation;
@@ -364,6 +389,15 @@ MppiRolloutArgs rollout_args(const mppi_backend* b, uint32_t step_local) {
     a.work_counter = b->grid ? b->d_queue.as<uint32_t>() : nullptr;
     a.num_work = b->num_work;
   }
+  if (b->proposal && b->spec.proposal) {
+    const mppi_b200::ProposalShape ps = mppi_b200::proposal_shape(b->proposal);
+    a.prop_out = b->d_prop.as<float>();
+    a.prop_stride = ps.out_stride;
+    a.prop_count = std::min(b->prop_samples, b->K);
+    a.prop_ls_offset = ps.horizon * ps.control_dim;
+    a.prop_ls_min = ps.log_scale_min;
+    a.prop_ls_max = ps.log_scale_max;
+  }
   return a;
 }
 
@@ -392,6 +426,7 @@ MppiCombineArgs combine_args(const mppi_backend* b, uint32_t step_local, bool pr
   c.hist_controls = b->want_c ? b->d_hc.as<float>() : nullptr;
   c.hist_costs = b->want_k ? b->d_hk.as<float>() : nullptr;
   c.terminal = b->want_t ? b->d_term.as<float>() : nullptr;
+  c.hist_ustar = (b->record_ustar && b->T > 0 && propagate) ? b->d_hu.as<float>() : nullptr;
   if (b->ragged) {
     const uint32_t* info = b->d_agent_info.as<uint32_t>();
     c.agent_K = info;
@@ -406,7 +441,33 @@ size_t combine_smem(const mppi_backend* b) {
   return (pad4(b->geom.nblk) + pad4(b->HM())) * 4;
 }
 
+// Proposal features of the current states, then the network's forward pass
+// (both on the backend stream, so they are captured into the closed loop).
+cudaError_t launch_proposal(mppi_backend* b) {
+  MppiFeaturesArgs f{};
+  f.rows = b->N;
+  f.agents_mod = b->N;
+  f.x_stride = b->n;
+  f.out_stride = kFeatureStride;
+  f.x = b->io() + b->off_x();
+  f.model_params = b->run_mp;
+  f.cost_params = b->run_cp;
+  f.model_stride = b->run_mp_stride;
+  f.cost_stride = b->run_cp_stride;
+  f.out = b->d_feat.as<float>();
+  void* fa[] = {&f};
+  cudaError_t e = cudaLaunchKernel((const void*)b->mod->features, dim3((b->N + 127) / 128),
+                                   dim3(128), fa, 0, b->stream);
+  if (e != cudaSuccess) return e;
+  return mppi_b200::proposal_enqueue_forward(b->proposal, b->stream, b->d_feat.as<float>(),
+                                             kFeatureStride, b->N, b->d_prop.as<float>());
+}
+
 cudaError_t launch_rollout(mppi_backend* b, uint32_t step_local) {
+  if (b->proposal && b->spec.proposal) {
+    cudaError_t e = launch_proposal(b);
+    if (e != cudaSuccess) return e;
+  }
   MppiRolloutArgs a = rollout_args(b, step_local);
   void* args[] = {&a};
   if (b->ragged) {
@@ -431,7 +492,7 @@ int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
   const size_t budget = std::min<size_t>(b->max_smem_optin ? b->max_smem_optin : 232448, 232448);
   std::vector<uint32_t> stage_options;
   const size_t el = b->stage_elem;
-  const size_t full = pad4(HM) * 4 + 128 * 4 + HM * 128 * el;
+  const size_t full = nominal_bytes(b) + 128 * 4 + HM * 128 * el;
   if (full <= budget - 2048) stage_options.push_back((uint32_t)HM);
   uint32_t chunk = std::max<uint32_t>(b->m, (uint32_t)(32768 / (128 * el)) / b->m * b->m);
   stage_options.push_back(std::min<uint32_t>(chunk, (uint32_t)HM));
@@ -445,7 +506,7 @@ int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
   if (const char* r = getenv("MPPI_B200_UNEVEN_STAGE_ROWS"); r && *r) {
     const uint32_t rows = (uint32_t)strtoul(r, nullptr, 10);
     if (rows >= b->m && rows % b->m == 0) {
-      const size_t sm = pad4(HM) * 4 + 128 * 4 + (size_t)std::min<size_t>(rows, HM) * 128 * el;
+      const size_t sm = nominal_bytes(b) + 128 * 4 + (size_t)std::min<size_t>(rows, HM) * 128 * el;
       if (sm <= budget) stage_options.assign(1, (uint32_t)std::min<size_t>(rows, HM));
     }
   }
@@ -456,7 +517,7 @@ int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
   for (uint32_t rows : stage_options) {
     LaunchGeom g = base;
     g.stage_rows = rows;
-    g.smem = pad4(HM) * 4 + 128 * 4 + (size_t)rows * 128 * el;
+    g.smem = nominal_bytes(b) + 128 * 4 + (size_t)rows * 128 * el;
     b->geom = g;
     CK(cudaFuncSetAttribute((const void*)b->mod->rollout_work,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
@@ -587,12 +648,13 @@ int check_override_sizes(mppi_backend* b, size_t mp_bytes, const void* mp, size_
 // Enqueues T closed-loop steps (rollout + combine/propagate each), through a
 // CUDA graph captured once per (shape, buffers) and replayed afterwards.
 int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
-  char keybuf[256];
-  snprintf(keybuf, sizeof(keybuf), "%u/%u/%llu/%d/%d%d%d%d/%p/%p/%llu/%llu/%p/%u",
+  char keybuf[320];
+  snprintf(keybuf, sizeof(keybuf), "%u/%u/%llu/%d/%d%d%d%d%d/%p/%p/%llu/%llu/%p/%u/%p/%u/%p",
            b->N, b->T, (unsigned long long)b->generation, b->geom.variant, b->want_s, b->want_c,
-           b->want_k, b->want_t, (const void*)b->run_mp, (const void*)b->run_cp,
+           b->want_k, b->want_t, b->record_ustar, (const void*)b->run_mp, (const void*)b->run_cp,
            (unsigned long long)b->run_mp_stride, (unsigned long long)b->run_cp_stride,
-           (const void*)b->run_sigma, b->run_sigma_stride);
+           (const void*)b->run_sigma, b->run_sigma_stride, (const void*)b->proposal,
+           b->prop_samples, (const void*)b->mod.get());
   if (b->ragged) {
     const std::string rk = ragged_key(b);
     if (b->tuned_key != rk) {
@@ -768,6 +830,9 @@ int mppi_backend_initialize(mppi_backend* b, const mppi_backend_plugin* plugin,
     set_err(err, err_len, merr);
     return rc;
   }
+  b->spec = spec;
+  b->proposal = nullptr;
+  b->feature_dim = 0;
 
   if (!b->stream) CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   if (!b->ev0) CK(cudaEventCreate(&b->ev0));
@@ -1250,6 +1315,177 @@ int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
 }
 
 }  // extern "C"
+
+// ---- learned proposal (include/mppi_b200/mppi_backend.h, "proposal") ------
+
+namespace {
+
+// Recompiles the kernel module after a change of b->spec; drops the graph
+// and the tuned geometry, which depend on the module.
+int reload_module(mppi_backend* b, char* err, size_t err_len) {
+  CK(cudaStreamSynchronize(b->stream));
+  std::string merr;
+  std::shared_ptr<const KernelModule> mod;
+  const int rc = mppi_b200::load_module(b->spec, &mod, &merr);
+  if (rc != MPPI_OK) {
+    set_err(err, err_len, merr);
+    return rc;
+  }
+  b->mod = mod;
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+  }
+  b->graph_key.clear();
+  b->tuned_key.clear();
+  ++b->generation;
+  return MPPI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mppi_backend_set_features(mppi_backend* b, const char* callable, uint32_t feature_dim,
+                              char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  const bool none = callable == nullptr || *callable == '\0';
+  if (!none && !valid_identifier(callable)) {
+    set_err(err, err_len, std::string("Callable '") + callable + "' is not a valid identifier.");
+    return MPPI_ERR_CALLABLE;
+  }
+  if (!none && (feature_dim == 0 || feature_dim > kFeatureStride)) {
+    set_err(err, err_len, "feature_dim must be in [1, 32].");
+    return MPPI_ERR_INVALID;
+  }
+  if (none && b->proposal) {
+    set_err(err, err_len, "detach the proposal before removing its feature callable.");
+    return MPPI_ERR_INVALID;
+  }
+  const std::string old = b->spec.features;
+  b->spec.features = none ? "" : callable;
+  if (int rc = reload_module(b, err, err_len)) {
+    b->spec.features = old;
+    return rc;
+  }
+  b->feature_dim = none ? 0 : feature_dim;
+  return MPPI_OK;
+}
+
+int mppi_backend_features(mppi_backend* b, const float* states, uint32_t rows,
+                          uint32_t agents_mod, float* out, char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (!b->mod->features || b->feature_dim == 0) {
+    set_err(err, err_len, "no feature callable set (mppi_backend_set_features).");
+    return MPPI_ERR_INVALID;
+  }
+  if (rows == 0) return MPPI_OK;
+  if (!states || !out || agents_mod == 0) {
+    set_err(err, err_len, "states and out must not be null and agents_mod must be > 0.");
+    return MPPI_ERR_INVALID;
+  }
+  const uint8_t* mp;
+  const uint8_t* cp;
+  uint64_t mps = 0, cps = 0;
+  if (b->N > 0 && agents_mod == b->N) {  // the prepared batch's per-agent blobs
+    mp = b->run_mp;
+    cp = b->run_cp;
+    mps = b->run_mp_stride;
+    cps = b->run_cp_stride;
+  } else if (agents_mod == 1) {  // the bound blobs
+    mp = pick_params(b, true, nullptr, 0);
+    cp = pick_params(b, false, nullptr, 0);
+  } else {
+    set_err(err, err_len, "agents_mod must be 1 or the prepared batch's num_agents.");
+    return MPPI_ERR_INVALID;
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  DevBuf dx, dout;
+  CK(dx.ensure((size_t)rows * b->n * 4));
+  CK(dout.ensure((size_t)rows * b->feature_dim * 4));
+  CK(cudaMemcpyAsync(dx.p, states, (size_t)rows * b->n * 4, cudaMemcpyHostToDevice, b->stream));
+  MppiFeaturesArgs f{};
+  f.rows = rows;
+  f.agents_mod = agents_mod;
+  f.x_stride = b->n;
+  f.out_stride = b->feature_dim;
+  f.x = dx.as<float>();
+  f.model_params = mp;
+  f.cost_params = cp;
+  f.model_stride = mps;
+  f.cost_stride = cps;
+  f.out = dout.as<float>();
+  void* fa[] = {&f};
+  CK(cudaLaunchKernel((const void*)b->mod->features, dim3((rows + 127) / 128), dim3(128), fa, 0,
+                      b->stream));
+  CK(cudaMemcpyAsync(out, dout.p, (size_t)rows * b->feature_dim * 4, cudaMemcpyDeviceToHost,
+                     b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return MPPI_OK;
+}
+
+int mppi_backend_set_proposal(mppi_backend* b, mppi_proposal* p, uint32_t proposal_samples,
+                              char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (p) {
+    const mppi_b200::ProposalShape ps = mppi_b200::proposal_shape(p);
+    if (b->feature_dim == 0) {
+      set_err(err, err_len, "set a feature callable first (mppi_backend_set_features).");
+      return MPPI_ERR_INVALID;
+    }
+    if (ps.control_dim != b->m || ps.horizon < b->H || ps.input_dim > b->feature_dim) {
+      set_err(err, err_len,
+              "proposal network shape does not fit: need control_dim == DriverConfig::control_dim, "
+              "horizon >= DriverConfig::horizon and input_dim <= the feature dimension.");
+      return MPPI_ERR_INVALID;
+    }
+    if (ps.device != b->device) {
+      set_err(err, err_len, "proposal network lives on another device.");
+      return MPPI_ERR_INVALID;
+    }
+    if (proposal_samples == 0 || proposal_samples > b->K) {
+      set_err(err, err_len, "proposal_samples must be in [1, DriverConfig::sample_count].");
+      return MPPI_ERR_INVALID;
+    }
+  }
+  const bool want = p != nullptr;
+  if (want != b->spec.proposal) {
+    b->spec.proposal = want;
+    if (int rc = reload_module(b, err, err_len)) {
+      b->spec.proposal = !want;
+      return rc;
+    }
+  }
+  CK(cudaStreamSynchronize(b->stream));
+  b->proposal = p;
+  b->prop_samples = p ? proposal_samples : 0;
+  b->N = 0;  // buffers and launch geometry are re-derived by the next prepare
+  return MPPI_OK;
+}
+
+int mppi_backend_set_record_ustar(mppi_backend* b, uint32_t enable, char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  CK(cudaStreamSynchronize(b->stream));
+  b->record_ustar = enable != 0;
+  b->N = 0;  // takes effect at the next prepare
+  return MPPI_OK;
+}
+
+int mppi_backend_batch_fetch_ustar(mppi_backend* b, float* out, char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (!out || !b->record_ustar || b->N == 0 || b->T == 0) {
+    set_err(err, err_len, "no recorded batch: enable mppi_backend_set_record_ustar before prepare.");
+    return MPPI_ERR_INVALID;
+  }
+  CK(cudaMemcpyAsync(out, b->d_hu.p, (size_t)b->T * b->N * b->HM() * 4, cudaMemcpyDeviceToHost,
+                     b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return MPPI_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 
 // ---------------------------------------------------------------------------
 // Single-agent step on caller memory + a caller scratch area (used by the

@@ -13,6 +13,11 @@
 //                                           staged in FP16 (kFp16 / kMixed)
 //   MPPI_DYNAMICS_FN / _STAGE_COST_FN / _TERMINAL_COST_FN   callable names
 //   MPPI_MP_BYTES / MPPI_CP_BYTES           ParamLayout blob sizes
+//   MPPI_PROPOSAL                           1: a share of the samples draws
+//                                           around a learned proposal
+//                                           (MppiRolloutArgs::prop_out)
+//   MPPI_FEATURES_FN                        the plugin's proposal-feature
+//                                           callable (mppi_features kernel)
 //
 // Kernels (extern "C" names are looked up by the backend):
 //   mppi_rollout_b{64,128,256}  fused rollout + per-CTA softmax partials +
@@ -21,6 +26,8 @@
 //                               optional propagate & shift (closed loop)
 //   mppi_weights                normalised weights (inspection only)
 //   mppi_noise                  shaped noise of a sample range (inspection)
+//   mppi_features               proposal features of state rows (only with
+//                               MPPI_FEATURES_FN)
 //
 // Reference semantics followed (MarshallVielmetti/mppi_metal):
 //   rollout          shaders/mppi_rollout.metal:36-96 and :103-170
@@ -53,9 +60,14 @@
 #ifndef MPPI_NOISE_HALF
 #define MPPI_NOISE_HALF 0
 #endif
+#ifndef MPPI_PROPOSAL
+#define MPPI_PROPOSAL 0
+#endif
 #ifndef MPPI_MP_BYTES
 #define MPPI_MP_BYTES 0
 #endif
+// Features per row of the proposal network's input.
+#define MPPI_MAX_FEATURES 32
 #ifndef MPPI_CP_BYTES
 #define MPPI_CP_BYTES 0
 #endif
@@ -200,6 +212,23 @@ __device__ __forceinline__ void copy_words(uint32_t* dst, const uint8_t* src, in
   for (int i = threadIdx.x; i < (bytes + 3) / 4; i += blockDim.x) dst[i] = s[i];
 }
 
+// Proposal samples replace the plain draw eps = sigma n by
+// (mu - u_nom) + exp(s) n on the same standard normals n (rounded like the
+// plain draw in the FP16 modes).
+#if MPPI_PROPOSAL
+#define MPPI_PROPOSAL_EPS()                                                       \
+  do {                                                                            \
+    if (k < pcount) {                                                             \
+      _Pragma("unroll") for (int d_ = 0; d_ < kM; ++d_) eps[d_] =                 \
+          from_stage(to_stage(fmaf(ps[d_], n[d_], sh_s[t * kM + d_])));            \
+    }                                                                             \
+  } while (0)
+#else
+#define MPPI_PROPOSAL_EPS() \
+  do {                      \
+  } while (0)
+#endif
+
 // --------------------------------------------------------------------------
 // Fused rollout of one work item: CTA `blk` of agent `agent` (K samples,
 // horizon H, nominal at un_g, partial record at part).  One thread per
@@ -230,11 +259,32 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   const uint32_t key = a.seed + agent;
   const bool staged = a.stage_rows >= HM;
 
+  const uint32_t HMp = (a.H * kM + 3) & ~3u;
   float* un_s = dsm;
-  stage_t* stage_s = reinterpret_cast<stage_t*>(dsm + ((a.H * kM + 3) & ~3u));
+#if MPPI_PROPOSAL
+  float* sh_s = dsm + HMp;  // proposal mean shift mu - u_nom
+  stage_t* stage_s = reinterpret_cast<stage_t*>(dsm + 2 * HMp);
+#else
+  stage_t* stage_s = reinterpret_cast<stage_t*>(dsm + HMp);
+#endif
   float* e_s = reinterpret_cast<float*>(stage_s + (size_t)a.stage_rows * BLOCK);
 
   for (uint32_t i = tid; i < HM; i += BLOCK) un_s[i] = un_g[i];
+#if MPPI_PROPOSAL
+  // samples k < pcount draw around the network's predicted sequence
+  const uint32_t pcount = a.prop_out ? a.prop_count : 0u;
+  float ps[kM];
+  if (pcount) {
+    const float* po = a.prop_out + (size_t)agent * a.prop_stride;
+    for (uint32_t i = tid; i < HM; i += BLOCK) sh_s[i] = po[i] - un_g[i];
+#pragma unroll
+    for (int d = 0; d < kM; ++d)
+      ps[d] = expf(clampf(po[a.prop_ls_offset + d], a.prop_ls_min, a.prop_ls_max));
+  } else {
+#pragma unroll
+    for (int d = 0; d < kM; ++d) ps[d] = 1.0f;
+  }
+#endif
   const uint8_t* mp_g = a.model_params + a.model_stride * agent;
   const uint8_t* cp_g = a.cost_params + a.cost_stride * agent;
 #if MPPI_MP_SMEM
@@ -287,6 +337,7 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
       float n[2 * kP], eps[kM];
       if (active) {
         sample_noise(step, key, k, H, t, sig, n, eps);
+        MPPI_PROPOSAL_EPS();
       } else {
 #pragma unroll
         for (int d = 0; d < kM; ++d) eps[d] = 0.0f;
@@ -363,6 +414,7 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
         float n[2 * kP], eps[kM];
         if (active) {
           sample_noise(step, key, k, H, t, sig, n, eps);
+          MPPI_PROPOSAL_EPS();
         } else {
 #pragma unroll
           for (int d = 0; d < kM; ++d) eps[d] = 0.0f;
@@ -461,6 +513,10 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
     const float u = clampf(un[j] + v * invS, a.u_min[d], a.u_max[d]);
     u_s[j] = u;
     uo[j] = u;
+  }
+  if (a.hist_ustar) {
+    float* hu = a.hist_ustar + ((size_t)a.step_local * a.num_agents + agent) * a.H * kM;
+    for (uint32_t j = tid; j < HM; j += kCombineBlock) hu[j] = u_s[j];
   }
   if (tid == 0) {
     a.diag[agent * 3 + 0] = M;
@@ -561,3 +617,27 @@ extern "C" __global__ void __launch_bounds__(128) mppi_noise(const MppiNoiseArgs
     }
   }
 }
+
+#ifdef MPPI_FEATURES_FN
+// Proposal features: one thread per state row.
+extern "C" __global__ void __launch_bounds__(128) mppi_features(const MppiFeaturesArgs a) {
+  const uint32_t r = blockIdx.x * 128 + threadIdx.x;
+  if (r >= a.rows) return;
+  const uint32_t agent = r % a.agents_mod;
+  __align__(16) float st[mppi::kNPad];
+  const float* xr = a.x + (size_t)r * a.x_stride;
+#pragma unroll
+  for (int d = 0; d < mppi::kN; ++d) st[d] = xr[d];
+#pragma unroll
+  for (int d = mppi::kN; d < mppi::kNPad; ++d) st[d] = 0.0f;
+  float f[MPPI_MAX_FEATURES];
+#pragma unroll
+  for (int i = 0; i < MPPI_MAX_FEATURES; ++i) f[i] = 0.0f;
+  MPPI_FEATURES_FN(st, a.model_params + a.model_stride * agent,
+                   a.cost_params + a.cost_stride * agent, f);
+  float* o = a.out + (size_t)r * a.out_stride;
+#pragma unroll
+  for (int i = 0; i < MPPI_MAX_FEATURES; ++i)
+    if ((uint32_t)i < a.out_stride) o[i] = f[i];
+}
+#endif

@@ -55,6 +55,19 @@ struct MppiRolloutArgs {
   uint32_t* work_counter;
   uint32_t num_work;
   uint32_t pad1;
+  // Learned proposal (read by modules compiled with MPPI_PROPOSAL; prop_out
+  // null = plain MPPI).  Samples k < prop_count of agent a draw
+  //   eps_t = (mu_t - u_nom_t) + exp(clamp(s, prop_ls_min, prop_ls_max)) * n_t
+  // with mu_t[d] = prop_out[a * prop_stride + t * m + d] (the network's
+  // predicted u*) and s[d] = prop_out[a * prop_stride + prop_ls_offset + d];
+  // the other samples draw the plain eps_t = sigma * n_t.
+  const float* prop_out;
+  uint32_t prop_stride;
+  uint32_t prop_count;
+  uint32_t prop_ls_offset;
+  float prop_ls_min;
+  float prop_ls_max;
+  uint32_t pad2;
 };
 
 // One launch of the combine (+ optional propagate & shift) kernel.
@@ -90,6 +103,23 @@ struct MppiCombineArgs {
   const uint32_t* agent_blk0;
   uint32_t block;
   uint32_t pad0;
+  float* hist_ustar;   // [T][N][H*m] the updated sequence u* of every step (may be null)
+};
+
+// Proposal features of state rows: row r is a state of agent r % agents_mod
+// (its parameter blobs), out[r][0..out_stride) = the plugin's feature
+// callable (entries it does not set are zero).
+struct MppiFeaturesArgs {
+  uint32_t rows;
+  uint32_t agents_mod;
+  uint32_t x_stride;    // floats between state rows
+  uint32_t out_stride;  // floats between feature rows, <= MPPI_MAX_FEATURES
+  const float* x;
+  const uint8_t* model_params;
+  const uint8_t* cost_params;
+  uint64_t model_stride;
+  uint64_t cost_stride;
+  float* out;
 };
 
 // Normalised weights from the per-sample costs and the combine statistics

@@ -149,7 +149,9 @@ int compile_module(const ModuleSpec& spec, bool use_cache, bool ptxas_verbose,
       "-DMPPI_DYNAMICS_FN=" + spec.dynamics,
       "-DMPPI_STAGE_COST_FN=" + stage,
       "-DMPPI_TERMINAL_COST_FN=" + term,
+      "-DMPPI_PROPOSAL=" + std::to_string(spec.proposal ? 1 : 0),
   };
+  if (!spec.features.empty()) opts.push_back("-DMPPI_FEATURES_FN=" + spec.features);
   if (ptxas_verbose) opts.push_back("--ptxas-options=-v");
 
   const std::string main_src = "#include \"mppi_prelude.cuh\"\n#line 1 \"" + spec.plugin_path +
@@ -205,7 +207,7 @@ int compile_module(const ModuleSpec& spec, bool use_cache, bool ptxas_verbose,
                spec.plugin_path + "'.";
       return MPPI_ERR_CALLABLE;
     }
-    for (const std::string* nm : {&spec.stage_cost, &spec.terminal_cost}) {
+    for (const std::string* nm : {&spec.stage_cost, &spec.terminal_cost, &spec.features}) {
       if (log_names_undefined(log, *nm)) {
         *error = "Callable '" + *nm + "' not found in user plugin source '" + spec.plugin_path +
                  "'.";
@@ -273,6 +275,8 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->combine, mod->library, "mppi_combine");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->weights, mod->library, "mppi_weights");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->noise, mod->library, "mppi_noise");
+  if (ce == cudaSuccess && !spec.features.empty())
+    ce = cudaLibraryGetKernel(&mod->features, mod->library, "mppi_features");
   if (ce != cudaSuccess) {
     *error = std::string("Required library kernel missing from the module: ") +
              cudaGetErrorString(ce);

@@ -28,6 +28,8 @@ struct ModuleSpec {
   bool cov_full = false;
   bool control_cost = false;
   bool noise_half = false;  // NumericMode kFp16 / kMixed: FP16 noise
+  bool proposal = false;    // rollout reads a learned proposal (MPPI_PROPOSAL)
+  std::string features;     // proposal-feature callable ("" = none)
   uint64_t model_params_bytes = 0;
   uint64_t cost_params_bytes = 0;
 };
@@ -42,6 +44,7 @@ struct KernelModule {
   cudaKernel_t combine = nullptr;
   cudaKernel_t weights = nullptr;
   cudaKernel_t noise = nullptr;
+  cudaKernel_t features = nullptr;  // only when ModuleSpec::features is set
   std::string build_log;  // NVRTC log of the compile (warnings, ptxas info)
 };
 

@@ -7,6 +7,8 @@
 // compile-time bound chosen by one uniform branch on num_obs, so the
 // obstacles form independent instruction streams the compiler can
 // interleave; the terms are summed as a tree.
+//
+// mppi_proposal_features gives the learned proposal its 31 inputs.
 #include "mppi_core.h"
 #include "model_params.h"
 
@@ -72,4 +74,53 @@ __device__ float mppi_terminal_cost(const float* s, const uint8_t* model_params_
                                     const uint8_t* cost_params_raw) {
   const UnicycleCostParams* c = reinterpret_cast<const UnicycleCostParams*>(cost_params_raw);
   return c->w_terminal * unicycle_goal(s, c);
+}
+
+// Proposal features (31 of them):
+//   [0..5)   x / 10, y / 10, cos(theta), sin(theta), t / 15
+//   [5..7)   goal offset in the body frame (forward, left) / 10
+//   [7..31)  the 8 obstacles of least clearance |p - c_i(t)| - r_i (ties:
+//            lower index first), each as its centre's body-frame offset / 10
+//            and its radius; missing obstacles give zeros
+__device__ void mppi_proposal_features(const float* s, const uint8_t* model_params_raw,
+                                       const uint8_t* cost_params_raw, float* f) {
+  const UnicycleCostParams* c = reinterpret_cast<const UnicycleCostParams*>(cost_params_raw);
+  const float x = s[0], y = s[1], t = s[3];
+  float sn, cs;
+  sincosf(s[2], &sn, &cs);
+  f[0] = x * 0.1f;
+  f[1] = y * 0.1f;
+  f[2] = cs;
+  f[3] = sn;
+  f[4] = t * (1.0f / 15.0f);
+  const float gx = c->goal_x - x, gy = c->goal_y - y;
+  f[5] = (cs * gx + sn * gy) * 0.1f;
+  f[6] = (cs * gy - sn * gx) * 0.1f;
+  const unsigned n = c->num_obs < MPPI_UNICYCLE_MAX_OBS ? c->num_obs : MPPI_UNICYCLE_MAX_OBS;
+  float clr[MPPI_UNICYCLE_MAX_OBS];
+  for (unsigned i = 0; i < MPPI_UNICYCLE_MAX_OBS; ++i) {
+    if (i < n) {
+      const float ex = fmaf(c->obs_vx[i], t, c->obs_cx[i]) - x;
+      const float ey = fmaf(c->obs_vy[i], t, c->obs_cy[i]) - y;
+      clr[i] = sqrtf(ex * ex + ey * ey) - c->obs_r[i];
+    } else {
+      clr[i] = __int_as_float(0x7f800000);
+    }
+  }
+  for (unsigned j = 0; j < 8; ++j) {
+    int best = -1;
+    float bv = __int_as_float(0x7f800000);
+    for (unsigned i = 0; i < n; ++i)
+      if (clr[i] < bv) {
+        bv = clr[i];
+        best = (int)i;
+      }
+    if (best < 0) break;
+    clr[best] = __int_as_float(0x7f800000);
+    const float ex = fmaf(c->obs_vx[best], t, c->obs_cx[best]) - x;
+    const float ey = fmaf(c->obs_vy[best], t, c->obs_cy[best]) - y;
+    f[7 + 3 * j] = (cs * ex + sn * ey) * 0.1f;
+    f[8 + 3 * j] = (cs * ey - sn * ex) * 0.1f;
+    f[9 + 3 * j] = c->obs_r[best];
+  }
 }

@@ -54,8 +54,8 @@ def build_oracle() -> None:
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={ref_root}"], check=True)
         product = HERE.parent / "mppi_metal_b200" / "lib" / "libmppi_b200.so"
         if product.exists():
-            subprocess.run(["make", "-s", "-C", str(HERE), "ref_suite", f"REF_ROOT={ref_root}"],
-                           check=True)
+            subprocess.run(["make", "-s", "-C", str(HERE), "ref_suite", "ref_examples",
+                            f"REF_ROOT={ref_root}"], check=True)
 
 
 def _ptr(a: np.ndarray | None):

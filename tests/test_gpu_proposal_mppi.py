@@ -1,0 +1,145 @@
+"""GPU parity of proposal-MPPI: the plugin's feature callable, the recorded
+u* history, and a control step whose samples partly draw around the
+network's prediction, all against the CPU oracle.
+
+Tolerances as in the plain parity tests: features 1e-5 absolute (FP32
+against float64; obstacle ranking may differ only on near-ties), per-sample
+costs 1e-5 relative, u_next 1e-4 absolute (the update checked on the
+device's own costs).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import mlp_oracle as mo
+from helpers import backend_for, oracle_problem, rel_err
+from mppi_metal_b200 import models
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+FEATURES = "mppi_proposal_features"
+
+
+def _batch_backend(w):
+    b = backend_for(w, bind=False)
+    b.prepare(w.num_agents, w.num_steps, w.x0, cost_params=w.cost_params_packed,
+              cost_stride=w.cost_stride, model_params=w.model_params, model_stride=0,
+              sigma=w.agent_sigma)
+    return b
+
+
+def test_features_match_oracle():
+    w = models.unicycle_batch(seed=3, N=64, K=256, H=16, T=2)
+    b = _batch_backend(w)
+    b.set_features(FEATURES, 31)
+    rng = np.random.default_rng(0)
+    R = 64 * 4
+    st = np.zeros((R, 4), np.float32)
+    st[:, :2] = rng.uniform(-10, 10, (R, 2))
+    st[:, 2] = rng.uniform(-np.pi, np.pi, R)
+    st[:, 3] = rng.uniform(0, 15, R)
+    f = b.features(st, agents_mod=64)
+    ref = np.stack([mo.unicycle_features(st[r], w.cost_params[r % 64]) for r in range(R)])
+    d = np.abs(f - ref).max(axis=1)
+    assert f.shape == (R, 31)
+    assert np.mean(d <= 1e-5) >= 0.99, np.sort(d)[-5:]
+    # the state and goal features never depend on the ranking
+    assert np.abs(f[:, :7] - ref[:, :7]).max() <= 1e-5
+
+
+def test_missing_feature_callable_is_named():
+    from mppi_metal_b200.backend import BackendError
+    w = models.unicycle_batch(seed=3, N=4, K=128, H=8, T=1)
+    b = backend_for(w)
+    with pytest.raises(BackendError) as e:
+        b.set_features("no_such_features", 31)
+    assert "no_such_features" in e.value.msg and e.value.code == 3
+
+
+def test_recorded_ustar_matches_the_applied_controls():
+    w = models.unicycle_batch(seed=4, N=16, K=512, H=20, T=6)
+    b = backend_for(w, bind=False)
+    b.set_record_ustar(True)
+    b.prepare(16, 6, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+              model_params=w.model_params, sigma=w.agent_sigma)
+    b.run(0)
+    r = b.fetch()
+    us = b.fetch_ustar()
+    assert us.shape == (6, 16, 20, 2)
+    assert np.array_equal(us[:, :, 0, :], r["controls"])
+    last = us[-1]
+    shifted = np.concatenate([last[:, 1:], last[:, -1:]], axis=1).reshape(16, -1)
+    assert np.array_equal(shifted, r["u_nom"])
+
+
+def _proposal_case(samples: int):
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.unicycle_batch(seed=5, N=1, K=1024, H=64, T=1)
+    b = backend_for(w)
+    b.set_features(FEATURES, 31)
+    shape = mo.Shape(31, 64, 2)
+    net = ProposalNet(31, 64, 2, max_batch=256, seed=1)
+    net.set_params(mo.init_params(shape, 4))
+    b.set_proposal(net, samples)
+    return w, b, net, shape
+
+
+@pytest.mark.parametrize("samples", [512, 1024])
+def test_proposal_step_matches_oracle(oracle, samples):
+    w, b, net, shape = _proposal_case(samples)
+    x0 = w.x0[0].copy()
+    rng = np.random.default_rng(6)
+    u_nom = (rng.normal(size=64 * 2) * 0.3).astype(np.float32)
+    step = 7
+    u_out, diag = b.dispatch_rollout(step, x0, u_nom)
+    costs = b.last_costs()[0]
+    # the network's output on the same features (same kernels, same bits)
+    feats = b.features(x0[None, :], agents_mod=1)
+    out = net.forward(torch.from_numpy(np.ascontiguousarray(feats)).cuda()).cpu().numpy()[0]
+    mu = out[:128].astype(np.float64)
+    ps = np.exp(np.clip(out[128:130].astype(np.float32), -3.0, 1.0)).astype(np.float64)
+    p = oracle_problem(w)
+    eps = np.zeros((1024, 64, 2))
+    sh = (mu - u_nom.astype(np.float64)).reshape(64, 2)
+    for k in range(1024):
+        n, e = oracle.noise(p, step, w.seed, k)
+        eps[k] = sh + ps * n if k < samples else e
+    ref = oracle.rollout_eps(p, x0, u_nom, eps)
+    assert rel_err(costs, ref) <= 1e-5
+    wts, _ = oracle.weights(costs.astype(np.float64), w.lam)
+    u_ref = oracle.update_eps(p, wts, u_nom, eps)
+    assert np.abs(u_out - u_ref).max() <= 1e-4
+    assert diag[0] == pytest.approx(costs.min(), rel=1e-6)
+
+
+def test_detaching_restores_the_plain_path():
+    w, b, net, shape = _proposal_case(512)
+    x0 = w.x0[0].copy()
+    u_nom = np.zeros(128, np.float32)
+    b.set_proposal(None)
+    u1, _ = b.dispatch_rollout(3, x0, u_nom)
+    plain = backend_for(w)
+    u2, _ = plain.dispatch_rollout(3, x0, u_nom)
+    assert np.array_equal(u1, u2)
+
+
+def test_proposal_batch_closed_loop_runs():
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.unicycle_batch(seed=7, N=130, K=256, H=64, T=5)
+    b = backend_for(w, bind=False)
+    b.set_features(FEATURES, 31)
+    net = ProposalNet(31, 64, 2, max_batch=256, seed=2)
+    b.set_proposal(net, 128)
+    b.prepare(130, 5, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+              model_params=w.model_params, sigma=w.agent_sigma)
+    b.run(0)
+    r1 = b.fetch()
+    assert np.all(np.isfinite(r1["states"])) and np.all(np.isfinite(r1["controls"]))
+    # replay of the captured graph gives the same bits
+    b.prepare(130, 5, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+              model_params=w.model_params, sigma=w.agent_sigma)
+    b.run(0)
+    r2 = b.fetch()
+    assert np.array_equal(r1["states"], r2["states"])

@@ -1,0 +1,135 @@
+"""GPU parity of the proposal network's tcgen05 kernels against the CPU
+restatement (oracle/mlp_oracle.py, bfloat16 rounding mirrored).
+
+Tolerances: the kernels and the oracle round the same values to bfloat16;
+what differs is FP32 (device) against float64 (oracle) accumulation, which
+occasionally moves a value across a bfloat16 rounding boundary.
+  outputs        max |d| <= 2e-3 * max|out| + 1e-4
+  loss           1e-4 relative
+  gradients      per layer, ||d||_F <= 1e-2 ||g||_F
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _net(shape: mo.Shape, seed: int, max_batch: int = 1024):
+    from mppi_metal_b200.proposal import ProposalNet
+    net = ProposalNet(shape.input_dim, shape.horizon, shape.control_dim, max_batch=max_batch,
+                      seed=seed, log_scale_min=shape.log_scale_min,
+                      log_scale_max=shape.log_scale_max)
+    return net
+
+
+def _layer_slices(shape):
+    out, o = [], 0
+    for r, c in shape.layer_dims():
+        out.append(slice(o, o + r * c))
+        o += r * c
+        out.append(slice(o, o + r))
+        o += r
+    return out
+
+
+@pytest.mark.parametrize("rows", [1, 128, 300])
+def test_forward_matches_oracle(rows):
+    s = mo.Shape(31, 64, 2)
+    net = _net(s, 0)
+    p = mo.init_params(s, 11)
+    net.set_params(p)
+    assert np.array_equal(net.get_params(), p)
+    rng = np.random.default_rng(rows)
+    x = rng.normal(size=(rows, 31)).astype(np.float32)
+    out = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    ref = mo.forward(s, p.astype(np.float64), x)
+    assert out.shape == (rows, s.out_pad)
+    tol = 2e-3 * np.abs(ref).max() + 1e-4
+    assert np.abs(out[:, :s.out_dim] - ref[:, :s.out_dim]).max() <= tol
+
+
+def test_forward_odd_shapes():
+    # input narrower than 32, output width not a multiple of 16 (H 50, m 2 -> 102 -> 112)
+    s = mo.Shape(9, 50, 2)
+    net = _net(s, 1)
+    p = mo.init_params(s, 12)
+    net.set_params(p)
+    x = np.random.default_rng(3).normal(size=(200, 9)).astype(np.float32)
+    out = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    ref = mo.forward(s, p.astype(np.float64), x)
+    assert np.abs(out[:, :s.out_dim] - ref[:, :s.out_dim]).max() <= 2e-3 * np.abs(ref).max() + 1e-4
+
+
+@pytest.mark.parametrize("rows", [128, 333, 1024])
+def test_gradients_match_oracle(rows):
+    s = mo.Shape(31, 64, 2, log_scale_min=-3.0, log_scale_max=1.0)
+    net = _net(s, 0)
+    p = mo.init_params(s, 21)
+    net.set_params(p)
+    rng = np.random.default_rng(100 + rows)
+    x = rng.normal(size=(rows, 31)).astype(np.float32)
+    y = (rng.normal(size=(rows, s.hm)) * 0.7).astype(np.float32)
+    loss, g = net.gradients(torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda())
+    lref, gref = mo.loss_and_grad(s, p.astype(np.float64), x, y)
+    assert abs(loss - lref) <= 1e-4 * abs(lref)
+    for sl in _layer_slices(s):
+        d = np.linalg.norm(g[sl] - gref[sl])
+        assert d <= 1e-2 * np.linalg.norm(gref[sl]) + 1e-7, (sl, d, np.linalg.norm(gref[sl]))
+
+
+def test_gradients_with_row_gather():
+    s = mo.Shape(31, 64, 2)
+    net = _net(s, 0)
+    p = mo.init_params(s, 22)
+    net.set_params(p)
+    rng = np.random.default_rng(7)
+    x = rng.normal(size=(500, 31)).astype(np.float32)
+    y = rng.normal(size=(500, s.hm)).astype(np.float32)
+    idx = rng.permutation(500)[:200].astype(np.int32)
+    loss, g = net.gradients(torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda(),
+                            torch.from_numpy(idx).cuda())
+    lref, gref = mo.loss_and_grad(s, p.astype(np.float64), x[idx], y[idx])
+    assert abs(loss - lref) <= 1e-4 * abs(lref)
+    assert np.linalg.norm(g - gref) <= 1e-2 * np.linalg.norm(gref)
+
+
+def test_adam_step_matches_oracle():
+    s = mo.Shape(31, 64, 2)
+    net = _net(s, 0)
+    p = mo.init_params(s, 23)
+    net.set_params(p)
+    rng = np.random.default_rng(8)
+    x = rng.normal(size=(256, 31)).astype(np.float32)
+    y = rng.normal(size=(256, s.hm)).astype(np.float32)
+    xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    _, g = net.gradients(xd, yd)
+    net.train_step(xd, yd, lr=1e-3)
+    p1 = net.get_params().astype(np.float64)
+    ref, _, _ = mo.adam(p.astype(np.float64), g.astype(np.float64), 0.0, 0.0, 1, 1e-3)
+    # entries with a clear gradient move by lr * sign(g) on the first step
+    live = np.abs(g) > 1e-3 * np.abs(g).max()
+    assert np.abs(p1[live] - ref[live]).max() <= 1e-6
+    assert np.all(p1[s.param_count - s.out_pad + s.out_dim:] == 0)  # padding bias rows stay zero
+
+
+def test_training_reduces_the_loss():
+    s = mo.Shape(31, 64, 2)
+    net = _net(s, 5, max_batch=2048)
+    rng = np.random.default_rng(9)
+    x = rng.normal(size=(8192, 31)).astype(np.float32)
+    A = rng.normal(size=(31, s.hm)) / np.sqrt(31)
+    y = np.tanh(x @ A).astype(np.float32)              # a smooth target
+    xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    l0, _ = net.gradients(xd, yd, torch.arange(2048, dtype=torch.int32, device="cuda"))
+    hist = net.fit(xd, yd, epochs=30, batch=2048, lr=2e-3, seed=0)
+    l1, _ = net.gradients(xd, yd, torch.arange(2048, dtype=torch.int32, device="cuda"))
+    assert l1 < l0 - 1.0, (l0, l1, hist)
+    out = net.forward(xd[:512]).cpu().numpy()
+    mse = float(np.mean((out[:, :s.hm] - y[:512]) ** 2))
+    assert mse < 0.25 * float(np.mean(y[:512] ** 2)), mse
