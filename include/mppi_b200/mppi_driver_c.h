@@ -35,6 +35,9 @@ typedef struct mppi_driver_config {
   uint32_t bounds_control_dim; /* ControlBounds::control_dim */
   uint32_t numeric_mode;       /* DriverConfig::NumericMode */
   uint32_t control_cost;       /* DriverOptions::control_cost */
+  struct mppi_proposal* proposal;  /* DriverOptions::proposal (may be NULL) */
+  uint32_t proposal_samples;       /* DriverOptions::proposal_samples */
+  const char* proposal_features;   /* DriverOptions::proposal_features (NULL: default) */
 } mppi_driver_config;
 
 /* ModelPluginSpec, flattened (reference mppi_types.hpp:79-101). */

@@ -14,6 +14,8 @@
 #include <string>
 #include <string_view>
 
+struct mppi_proposal;  // include/mppi_b200/mppi_proposal.h
+
 namespace mppi_metal {
 
 // ---- control noise (reference mppi_types.hpp:15-29) ------------------------
@@ -175,6 +177,15 @@ struct DriverOptions {
 	// Add lambda * u_nom_t^T Sigma^-1 eps_t to every stage cost (the MPPI
 	// control-cost term of Williams et al.); Sigma^-1 is noise.sigma_inv.
 	bool control_cost = false;
+
+	// Learned sampling proposal (include/mppi_b200/mppi_proposal.h).  When
+	// `proposal` is set, initialize() compiles the plugin's feature callable
+	// `proposal_features` and every step draws `proposal_samples` of its
+	// samples around the network's predicted sequence (the rest as plain
+	// MPPI).  The caller owns the network and keeps it alive.
+	struct mppi_proposal* proposal = nullptr;
+	uint32_t proposal_samples = 0;
+	std::string_view proposal_features = "mppi_proposal_features";
 };
 
 // Per-agent inputs for simulate_batch: every agent may carry its own model /

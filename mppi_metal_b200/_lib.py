@@ -65,7 +65,8 @@ class DriverConfigC(ctypes.Structure):
         ("sample_count", c_u32), ("lambda_", c_f32), ("covariance_form", c_u32),
         ("sigma", c_ptr), ("sigma_inv", c_ptr), ("noise_control_dim", c_u32),
         ("u_min", c_ptr), ("u_max", c_ptr), ("bounds_control_dim", c_u32),
-        ("numeric_mode", c_u32), ("control_cost", c_u32),
+        ("numeric_mode", c_u32), ("control_cost", c_u32), ("proposal", c_ptr),
+        ("proposal_samples", c_u32), ("proposal_features", c_char_p),
     ]
 
 

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "../../include/mppi_b200/mppi_backend.h"
+#include "proposal.hpp"
 
 namespace mppi_metal {
 
@@ -173,6 +174,20 @@ bool MPPIDriver::initialize(const ModelPluginSpec& model, std::string* error) {
 		mppi_backend_destroy(impl_->backend);
 		impl_->backend = nullptr;
 		return fail(err.data());
+	}
+
+	if (impl_->options.proposal != nullptr) {
+		const mppi_b200::ProposalShape ps = mppi_b200::proposal_shape(impl_->options.proposal);
+		const std::string feat(impl_->options.proposal_features);
+		if (mppi_backend_set_features(impl_->backend, feat.c_str(), ps.input_dim, err.data(),
+		                              err.size()) != MPPI_OK ||
+		    mppi_backend_set_proposal(impl_->backend, impl_->options.proposal,
+		                              impl_->options.proposal_samples, err.data(),
+		                              err.size()) != MPPI_OK) {
+			mppi_backend_destroy(impl_->backend);
+			impl_->backend = nullptr;
+			return fail(err.data());
+		}
 	}
 
 	impl_->param_layout = model.param_layout;

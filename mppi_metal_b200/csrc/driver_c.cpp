@@ -58,6 +58,9 @@ mppi_driver* mppi_driver_create(const mppi_driver_config* c) {
                                             : DriverConfig::NumericMode::kFp32;
   DriverOptions opts;
   opts.control_cost = c->control_cost != 0;
+  opts.proposal = c->proposal;
+  opts.proposal_samples = c->proposal_samples;
+  if (c->proposal_features && *c->proposal_features) opts.proposal_features = c->proposal_features;
   return new (std::nothrow) mppi_driver(cfg, opts);
 }
 

@@ -85,8 +85,13 @@ class DriverConfig:
 
 @dataclass
 class DriverOptions:
-    """Project extension: lambda * u^T Sigma^-1 eps control cost."""
+    """Project extensions: the lambda * u^T Sigma^-1 eps control cost, and a
+    learned sampling proposal (a mppi_metal_b200.proposal.ProposalNet) that
+    draws `proposal_samples` of every step's samples around its prediction."""
     control_cost: bool = False
+    proposal: object = None
+    proposal_samples: int = 0
+    proposal_features: str = "mppi_proposal_features"
 
 
 @dataclass
@@ -228,7 +233,10 @@ class MPPIDriver:
             config.lambda_, int(config.noise.covariance_form), _ptr(self._keep[0]),
             _ptr(self._keep[1]), config.noise.control_dim, _ptr(self._keep[2]),
             _ptr(self._keep[3]), config.bounds.control_dim, int(config.numeric_mode),
-            int(options.control_cost))
+            int(options.control_cost),
+            None if options.proposal is None else options.proposal.h,
+            int(options.proposal_samples), options.proposal_features.encode())
+        self._proposal = options.proposal  # keep the network alive
         self._h = self._lib.mppi_driver_create(ctypes.byref(c))
         if not self._h:
             raise MemoryError("mppi_driver_create failed")

@@ -143,3 +143,41 @@ def test_proposal_batch_closed_loop_runs():
     b.run(0)
     r2 = b.fetch()
     assert np.array_equal(r1["states"], r2["states"])
+
+
+def test_driver_api_runs_the_proposal():
+    """DriverOptions.proposal through the public MPPIDriver API gives the same
+    closed loop, bit for bit, as the backend path."""
+    from mppi_metal_b200 import driver as D
+    from mppi_metal_b200._lib import plugin_path
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.unicycle_batch(seed=8, N=32, K=256, H=64, T=4)
+    net = ProposalNet(31, 64, 2, max_batch=256, seed=3)
+    cfg = D.DriverConfig(4, 2, 64, 256, w.lam,
+                         D.ControlNoiseConfig(D.CovarianceForm.kDiagonal, w.sigma, w.sigma_inv, 2),
+                         D.ControlBounds(w.u_min, w.u_max, 2))
+    drv = D.MPPIDriver(cfg, D.DriverOptions(proposal=net, proposal_samples=128))
+    err = D.ErrorRef()
+    spec = D.ModelPluginSpec(plugin_path(w.plugin),
+                             D.CallableNames("mppi_dynamics", "mppi_stage_cost",
+                                             "mppi_terminal_cost"),
+                             D.ParamLayout(len(w.model_params), 4, w.cost_stride, 4),
+                             D.RngConfig(w.seed))
+    assert drv.initialize(spec, err), err.value
+    assert drv.set_problem_params(D.ProblemParams(D.ByteView.of(w.model_params),
+                                                  D.ByteView.of(w.cost_params[0])), err), err.value
+    outs = D.BatchSimulationResults(np.zeros((4, 32, 4), np.float32),
+                                    np.zeros((4, 32, 2), np.float32), np.zeros((4, 32), np.float32),
+                                    np.zeros((32, 4), np.float32), 32, 4)
+    ap = D.BatchAgentParams(cost_params=w.cost_params_packed, cost_params_stride=w.cost_stride,
+                            sigma=w.agent_sigma)
+    assert drv.simulate_batch(32, 4, w.x0, outs, ap, err), err.value
+    b = backend_for(w, bind=True)
+    b.set_features(FEATURES, 31)
+    b.set_proposal(net, 128)
+    b.prepare(32, 4, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+              sigma=w.agent_sigma)
+    b.run(0)
+    r = b.fetch()
+    assert np.array_equal(outs.states_out, r["states"])
+    assert np.array_equal(outs.controls_out, r["controls"])
