@@ -64,6 +64,10 @@ class QuadrotorCostParams(ctypes.Structure):
                 ("obs_cz", _f * QUAD_MAX_OBS), ("obs_r", _f * QUAD_MAX_OBS)]
 
 
+class GustModelParams(ctypes.Structure):
+    _fields_ = [("dt", _f), ("noise_std", _f), ("p_event", _f), ("gust_accel", _f)]
+
+
 def blob(s: ctypes.Structure) -> bytes:
     return ctypes.string_at(ctypes.addressof(s), ctypes.sizeof(s))
 
@@ -159,6 +163,22 @@ def unicycle_batch(seed: int = 0, N: int = 256, K: int = 4096, H: int = 50, T: i
                     1.0, sigma, (1.0 / sigma ** 2).astype(np.float32),
                     np.array([-1.0, -1.5], np.float32), np.array([2.0, 1.5], np.float32),
                     N, T, x0, blob(mp), cps, agent_sigma, control_cost=False, seed=seed)
+
+
+def gust_batch(seed: int = 0, N: int = 16, K: int = 1024, H: int = 30, T: int = 20,
+               lam: float = 10.0) -> Workload:
+    """Stochastic dynamics (plugins/gust_integrator.cu): a double integrator
+    with process noise and a random sticky gust, both drawn inside the
+    dynamics from the callable's Philox counter and key; N agents start at
+    rest from positions U[-3, 3]^2, sigma [1, 1], |a| <= 2, dt 0.1."""
+    rng = np.random.default_rng(seed)
+    mp = GustModelParams(0.1, 0.5, 0.02, 1.5)
+    x0 = np.zeros((N, 5), np.float32)
+    x0[:, :2] = rng.uniform(-3.0, 3.0, size=(N, 2))
+    sigma = np.ones(2, np.float32)
+    return Workload("gust_batch", "gust_integrator", "gust_integrator", 5, 2, H, K, lam,
+                    sigma, sigma.copy(), np.full(2, -2.0, np.float32),
+                    np.full(2, 2.0, np.float32), N, T, x0, blob(mp), [], None, seed=seed)
 
 
 def double_integrator_test(K: int = 64, H: int = 10) -> Workload:

@@ -157,4 +157,22 @@ typedef struct {
   float obs_r[MPPI_QUAD_MAX_OBS];
 } QuadrotorCostParams;
 
+/* ------------------------------------------------------------------------ */
+/* gust_integrator: stochastic dynamics (draws its own Philox randoms from  */
+/* the callable's rng_counter / rng_seed, as the reference's WEZ example    */
+/* does, examples/wez_environment_batch/wez_environment.metal:166-173).     */
+/* State [px, py, vx, vy, gust], control [ax, ay].                          */
+/*   n = box_muller(philox(rng_counter, rng_seed))                           */
+/*   e = uint_to_01(philox((ctr.x, ctr.y + 0x1000), rng_seed).x)             */
+/*   gust = 1 once e < p_event (sticky)                                      */
+/*   v += (u + noise_std * n + gust * (gust_accel, 0)) dt;  p += v dt        */
+/*   stage = px^2 + py^2 + 0.1 |v|^2;  terminal = 10 (px^2 + py^2)           */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  float dt;
+  float noise_std;
+  float p_event;
+  float gust_accel;
+} GustModelParams;
+
 #endif /* MPPI_B200_MODEL_PARAMS_H */

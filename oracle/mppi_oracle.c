@@ -198,13 +198,31 @@ static void dyn_quadrotor(double* s, const double* u, const QuadrotorModelParams
   s[11] += dr * dt;
 }
 
+/* gust_integrator (plugins/gust_integrator.cu): stochastic dynamics drawing
+ * from the callable's counter and key; the event test compares the
+ * bit-exact float uniform, so both sides take the same branch. */
+static void dyn_gust(double* s, const double* u, const GustModelParams* mp, uint32_t ctr0,
+                     uint32_t ctr1, uint32_t key) {
+  uint32_t w[2], e[2];
+  double n[2];
+  oracle_philox2x32_10(ctr0, ctr1, key, w);
+  oracle_box_muller(w[0], w[1], n);
+  oracle_philox2x32_10(ctr0, ctr1 + 0x1000u, key, e);
+  if (oracle_uint_to_01(e[0]) < mp->p_event) s[4] = 1.0;
+  const double dt = mp->dt;
+  s[2] += (u[0] + (double)mp->noise_std * n[0] + s[4] * (double)mp->gust_accel) * dt;
+  s[3] += (u[1] + (double)mp->noise_std * n[1]) * dt;
+  s[0] += s[2] * dt;
+  s[1] += s[3] * dt;
+}
+
 void oracle_dynamics(const oracle_problem* p, double* x, const double* u,
                      const void* model_params, uint32_t ctr0, uint32_t ctr1,
                      uint32_t key) {
-  (void)ctr0;
-  (void)ctr1;
-  (void)key; /* all shipped models are deterministic */
   switch (p->model) {
+    case ORACLE_MODEL_GUST:
+      dyn_gust(x, u, (const GustModelParams*)model_params, ctr0, ctr1, key);
+      break;
     case ORACLE_MODEL_DOUBLE_INTEGRATOR: dyn_double_integrator(x, u); break;
     case ORACLE_MODEL_NONHOLONOMIC:
       dyn_nonholonomic(x, u, (const NonholonomicModelParams*)model_params);
@@ -295,6 +313,8 @@ double oracle_stage_cost(const oracle_problem* p, const double* x, const double*
       return bicycle_state_cost(x, (const BicycleCostParams*)cost_params);
     case ORACLE_MODEL_QUADROTOR:
       return quad_state_cost(x, (const QuadrotorCostParams*)cost_params, 0);
+    case ORACLE_MODEL_GUST: /* plugins/gust_integrator.cu */
+      return x[0] * x[0] + x[1] * x[1] + (double)0.1f * (x[2] * x[2] + x[3] * x[3]);
     default: return 0.0;
   }
 }
@@ -319,6 +339,8 @@ double oracle_terminal_cost(const oracle_problem* p, const double* x,
     }
     case ORACLE_MODEL_QUADROTOR:
       return quad_state_cost(x, (const QuadrotorCostParams*)cost_params, 1);
+    case ORACLE_MODEL_GUST:
+      return 10.0 * (x[0] * x[0] + x[1] * x[1]);
     default: return 0.0;
   }
 }

@@ -42,6 +42,7 @@ enum {
   ORACLE_MODEL_UNICYCLE_OBSTACLES = 2,
   ORACLE_MODEL_BICYCLE_LANE = 3,
   ORACLE_MODEL_QUADROTOR = 4,
+  ORACLE_MODEL_GUST = 5,
 };
 
 typedef struct {

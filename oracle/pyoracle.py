@@ -31,6 +31,7 @@ MODEL_IDS = {
     "unicycle_obstacles": 2,
     "bicycle_lane": 3,
     "quadrotor": 4,
+    "gust_integrator": 5,
 }
 
 # Which oracle/_ref library runs the reference kernels for each model.

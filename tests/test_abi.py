@@ -58,6 +58,9 @@ PLUGINS = [
     ("double_integrator", 4, 2, 0, 0),
     ("nonholonomic_vehicle", 4, 2, 8, 24),
     ("unicycle_obstacles", 4, 2, 16, 352),
+    ("gust_integrator", 5, 2, 16, 0),
+    ("bicycle_lane", 5, 2, 16, 544),
+    ("quadrotor", 12, 4, 32, 560),
 ]
 
 
