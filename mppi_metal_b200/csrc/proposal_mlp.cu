@@ -4,7 +4,7 @@
 // accumulators in TMEM), trained with its own backward and Adam kernels.
 //
 // Kernels
-//   mlp_fused   one CTA per 128 batch rows.  Forward: 4 GEMMs, each an
+//   mlp_fused   one CTA (512 threads) per 128 batch rows.  Forward: 4 GEMMs, each an
 //               A (activations, 128 x K) x B (weights, N x K) product issued
 //               as K/16 tcgen05.mma instructions by one thread into a
 //               128 x N FP32 TMEM accumulator; the weights arrive by bulk
@@ -54,6 +54,11 @@ namespace prop {
 using bf16 = __nv_bfloat16;
 
 constexpr uint32_t kTile = 128;  // batch rows per CTA = TMEM lanes
+// mlp_fused runs kGroups warps per TMEM lane quarter: warp w reads lanes
+// 32 (w % 4) .. +31 (its rows) and handles the 16-column chunks
+// j = w / 4 (mod kGroups) of every epilogue.
+constexpr uint32_t kGroups = 4;
+constexpr uint32_t kFusedThreads = kTile * kGroups;
 constexpr uint32_t kHid = 256;   // hidden width
 constexpr uint32_t kIn = 32;     // padded input width
 constexpr uint32_t kMaxM = 16;   // control dims handled by the loss epilogue
@@ -167,7 +172,7 @@ __device__ __forceinline__ const bf16* gemm_b(const FusedArgs& a, uint32_t g) {
   return g < 4 ? a.W[g] : a.WT[7 - g];
 }
 
-__global__ void __launch_bounds__(128, 1) mlp_fused_kernel(const FusedArgs a) {
+__global__ void __launch_bounds__(kFusedThreads, 1) mlp_fused_kernel(const FusedArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   bf16* as = reinterpret_cast<bf16*>(smem);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kSmemA + kSmemW);
@@ -178,7 +183,9 @@ __global__ void __launch_bounds__(128, 1) mlp_fused_kernel(const FusedArgs a) {
   float* gls_s = iv_s + kMaxM * kTile;
 
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t row = blockIdx.x * kTile + tid;
+  const uint32_t quarter = warp & 3u, grp = warp >> 2;
+  const uint32_t r = quarter * 32 + lane;  // this thread's row of the tile
+  const uint32_t row = blockIdx.x * kTile + r;
   const bool valid = row < a.rows;
   const uint32_t bar_w = tc::smem_addr(&bars[0]), bar_m = tc::smem_addr(&bars[1]);
   const uint32_t a_s = tc::smem_addr(as), w_s = a_s + kSmemA;
@@ -197,7 +204,7 @@ __global__ void __launch_bounds__(128, 1) mlp_fused_kernel(const FusedArgs a) {
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tmem = *tslot;
-  const uint32_t t_row = tmem + ((warp * 32u) << 16);
+  const uint32_t t_row = tmem + ((quarter * 32u) << 16);
 
   bool w_pending = false;
   uint32_t ph_w = 0, ph_m = 0;
@@ -209,14 +216,14 @@ __global__ void __launch_bounds__(128, 1) mlp_fused_kernel(const FusedArgs a) {
   // ---- input row -> A (contraction 32); training keeps x^T for dW0 ----
   const uint32_t src = valid ? (a.index ? a.index[row] : row) : 0u;
 #pragma unroll
-  for (uint32_t j = 0; j < kIn / 16; ++j) {
+  for (uint32_t j = grp; j < kIn / 16; j += kGroups) {
     float v[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const uint32_t c = 16 * j + i;
       v[i] = (valid && c < a.in_dim) ? a.x[(size_t)src * a.x_stride + c] : 0.0f;
     }
-    a_store16(as, tid, j, kIn, v);
+    a_store16(as, r, j, kIn, v);
     if (a.train) t_store16(a.hT[0], kIn, row, 16 * j, v);
   }
 
@@ -263,7 +270,7 @@ __global__ void __launch_bounds__(128, 1) mlp_fused_kernel(const FusedArgs a) {
     if (g < 3) {
       // hidden layer g: z = acc + b; h = GELU(z) -> A of layer g + 1
       const float* bias = a.b[g];
-      for (uint32_t j = 0; j < kHid / 16; ++j) {
+      for (uint32_t j = grp; j < kHid / 16; j += kGroups) {
         float v[16];
         tc::tmem_ld16(t_row + 16 * j, v);
 #pragma unroll
@@ -276,13 +283,13 @@ __global__ void __launch_bounds__(128, 1) mlp_fused_kernel(const FusedArgs a) {
         }
 #pragma unroll
         for (int i = 0; i < 16; ++i) v[i] = gelu(v[i]);
-        a_store16(as, tid, j, kHid, v);
+        a_store16(as, r, j, kHid, v);
         if (a.train) t_store16(a.hT[g + 1], kHid, row, 16 * j, v);
       }
     } else if (g == 3 && !a.train) {
       // output layer (inference): out = acc + b
       const float* bias = a.b[3];
-      for (uint32_t j = 0; j < a.out_pad / 16; ++j) {
+      for (uint32_t j = grp; j < a.out_pad / 16; j += kGroups) {
         float v[16];
         tc::tmem_ld16(t_row + 16 * j, v);
         if (valid) {
@@ -293,15 +300,17 @@ __global__ void __launch_bounds__(128, 1) mlp_fused_kernel(const FusedArgs a) {
       }
     } else if (g == 3) {
       // output layer (training): loss and dL/d(out) -> A of GEMM 4 and dZ3^T
+      // (one warp per lane quarter: the log-scale gradient sums a whole row)
+      if (grp == 0) {
       const float* bias = a.b[3];
       const uint32_t m = a.m, hm = a.hm;
       uint32_t inside = 0;
       for (uint32_t d = 0; d < m; ++d) {
         const float raw = tc::tmem_ld1(t_row + hm + d) + bias[hm + d];
         const float c = fminf(fmaxf(raw, a.ls_min), a.ls_max);
-        lsc_s[d * kTile + tid] = c;
-        iv_s[d * kTile + tid] = expf(-2.0f * c);
-        gls_s[d * kTile + tid] = 0.0f;
+        lsc_s[d * kTile + r] = c;
+        iv_s[d * kTile + r] = expf(-2.0f * c);
+        gls_s[d * kTile + r] = 0.0f;
         if (raw > a.ls_min && raw < a.ls_max) inside |= 1u << d;
       }
       const float* tg = a.target + (size_t)src * a.target_stride;
@@ -317,28 +326,29 @@ __global__ void __launch_bounds__(128, 1) mlp_fused_kernel(const FusedArgs a) {
           if (valid && c < a.out_dim) {
             if (c < hm) {
               const float diff = tg[c] - (v[i] + bias[c]);
-              const float iv = iv_s[d * kTile + tid];
-              lrow += 0.5f * diff * diff * iv + lsc_s[d * kTile + tid];
+              const float iv = iv_s[d * kTile + r];
+              lrow += 0.5f * diff * diff * iv + lsc_s[d * kTile + r];
               gv = -diff * iv * a.inv_norm;
-              gls_s[d * kTile + tid] += (1.0f - diff * diff * iv) * a.inv_norm;
+              gls_s[d * kTile + r] += (1.0f - diff * diff * iv) * a.inv_norm;
             } else {
               const uint32_t e = c - hm;
-              gv = ((inside >> e) & 1u) ? gls_s[e * kTile + tid] : 0.0f;
+              gv = ((inside >> e) & 1u) ? gls_s[e * kTile + r] : 0.0f;
             }
           }
           if (c < hm) d = (d + 1 == m) ? 0u : d + 1;
           v[i] = gv;
         }
-        a_store16(as, tid, j, a.out_pad, v);
+        a_store16(as, r, j, a.out_pad, v);
         t_store16(a.dzT[3], kHid, row, 16 * j, v);
       }
       const float s = warp_sum(lrow * a.inv_norm);
       if (lane == 0) atomicAdd(a.loss, s);
+      }
     } else {
       // activation gradient through layer 7 - g: dZ = dH * GELU'(z)
       const uint32_t l = 6 - g;
       const float* zr = a.z[l] + (size_t)row * kHid;
-      for (uint32_t j = 0; j < kHid / 16; ++j) {
+      for (uint32_t j = grp; j < kHid / 16; j += kGroups) {
         float v[16];
         tc::tmem_ld16(t_row + 16 * j, v);
         const float4* zp = reinterpret_cast<const float4*>(zr + 16 * j);
@@ -350,7 +360,7 @@ __global__ void __launch_bounds__(128, 1) mlp_fused_kernel(const FusedArgs a) {
           v[4 * q + 2] *= gelu_grad(zz.z);
           v[4 * q + 3] *= gelu_grad(zz.w);
         }
-        if (g < 6) a_store16(as, tid, j, kHid, v);
+        if (g < 6) a_store16(as, r, j, kHid, v);
         t_store16(a.dzT[l], kHid, row, 16 * j, v);
       }
     }
@@ -731,7 +741,7 @@ int run_train(mppi_proposal* p, const float* x, uint32_t x_stride, const float* 
   f.ls_min = p->cfg.log_scale_min;
   f.ls_max = p->cfg.log_scale_max;
   f.inv_norm = 1.0f / ((float)rows * (float)p->hm);
-  mlp_fused_kernel<<<tiles, 128, kFusedSmem, p->stream>>>(f);
+  mlp_fused_kernel<<<tiles, kFusedThreads, kFusedSmem, p->stream>>>(f);
   PROP_CUDA(cudaGetLastError(), "mlp_fused launch");
 
   WgradArgs w{};
@@ -815,7 +825,7 @@ cudaError_t proposal_enqueue_forward(mppi_proposal* p, cudaStream_t stream, cons
   f.hm = p->hm;
   f.m = p->cfg.control_dim;
   f.train = 0;
-  mlp_fused_kernel<<<f.mp / kTile, 128, kFusedSmem, stream>>>(f);
+  mlp_fused_kernel<<<f.mp / kTile, kFusedThreads, kFusedSmem, stream>>>(f);
   return cudaGetLastError();
 }
 

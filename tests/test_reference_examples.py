@@ -52,7 +52,9 @@ def test_batch_example(tmp_path):
 
 @pytest.mark.parametrize("name", ["nonholonomic_vehicle", "nonholonomic_vehicle_concurrent"])
 def test_single_and_concurrent_examples(tmp_path, name):
+    # both programs run 1000 simulations (their loop bound), one driver per
+    # host thread, and log every one of them
     out = _run(name, tmp_path)
     data = _csv(tmp_path / "trajectory.csv")
-    assert len(np.unique(data[:, 0])) == 100
-    assert len(re.findall(r"Finished simulation \d+", out)) == 100
+    assert len(np.unique(data[:, 0])) == 1000
+    assert len(re.findall(r"Finished simulation \d+", out)) == 1000
