@@ -67,9 +67,12 @@ def parse():
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--workload", choices=WORKLOADS, default="batch",
                     help="batch (default, the headline configuration), uneven, single, "
-                         "quadrotor")
+                         "quadrotor, proposal")
     ap.add_argument("--numeric", choices=["fp32", "mixed"], default="fp32",
                     help="numeric mode of the quadrotor workload")
+    ap.add_argument("--proposal-weights", default="",
+                    help="proposal workload: load the network from this .npz instead of "
+                         "training it on the GPU first (python -m mppi_metal_b200.proposal)")
     return ap.parse_args()
 
 
@@ -78,7 +81,7 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
-WORKLOADS = ("batch", "uneven", "single", "quadrotor")
+WORKLOADS = ("batch", "uneven", "single", "quadrotor", "proposal")
 
 
 def workload_for_rank(rank: int, name: str = "batch", numeric: str = "fp32"):
@@ -496,12 +499,203 @@ def run_kernels_only(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# learned proposal vs plain MPPI
+# ---------------------------------------------------------------------------
+PROPOSAL_AGENTS = 128
+PROPOSAL_K = 256
+PROPOSAL_SAMPLES = 128
+PROPOSAL_PLAIN_K = 4096
+PROPOSAL_H = 64
+
+
+def run_proposal(args):
+    """Proposal-MPPI at K = 256 (128 samples around the network's prediction)
+    against plain MPPI at K = 4096, both on 128 unicycle agents x 300
+    closed-loop steps, H = 64.  value = control steps/s of the proposal arm;
+    the plain arm's rate and both closed-loop costs ride along.  Setup (not
+    timed): the network is trained on this GPU by the library's kernels on
+    ~1.2e6 (features, u*) pairs from plain MPPI at K = 16384."""
+    import torch
+    rank, world, local_rank = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    else:
+        torch.cuda.set_device(0)
+    from mppi_metal_b200 import driver as D
+    from mppi_metal_b200 import models
+    from mppi_metal_b200 import proposal as P
+    from mppi_metal_b200._lib import plugin_path
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    t_setup = time.time()
+    if args.proposal_weights and Path(args.proposal_weights).exists():
+        net = P.ProposalNet.load(args.proposal_weights)
+        training = {"loaded": args.proposal_weights}
+    else:
+        net, hist, pairs = P.train_unicycle_proposal()
+        training = {"pairs": pairs, "epochs": len(hist), "final_loss": hist[-1],
+                    "train_ms_per_step": net.last_train_ms(), "batch": 8192,
+                    "data": "plain MPPI K=16384, H=64, 4 seeds x 1024 agents x 300 steps"}
+    training["setup_s"] = round(time.time() - t_setup, 1)
+
+    w = models.unicycle_batch(seed=4000 + rank, N=PROPOSAL_AGENTS, K=PROPOSAL_PLAIN_K,
+                              H=PROPOSAL_H, T=CLOSED_LOOP_STEPS)
+    N, T = w.num_agents, w.num_steps
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def timed_arm(b):
+        P._prepare(b, w)
+        for _ in range(args.warmup):
+            b.run(0)
+            b.last_run_ms()
+        times = []
+        barrier()
+        with ClockSampler(physical_gpu_index(local_rank)) as clocks:
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                P._prepare(b, w)  # every timed loop starts from x0 and a zero nominal
+                b.run(0)
+                times.append(b.last_run_ms())
+        barrier()
+        r = b.fetch()
+        cost = models.executed_cost(w, r["states"], r["controls"], r["terminal"])
+        return max_over_ranks(sum(times)), cost, clocks.summary()
+
+    plain = P.make_backend(w)
+    plain_ms, plain_cost, _ = timed_arm(plain)
+    plain.close()
+    prop = P.make_backend(w, PROPOSAL_K)
+    prop.set_features(P.FEATURES_CALLABLE, P.UNICYCLE_FEATURES)
+    prop.set_proposal(net, PROPOSAL_SAMPLES)
+    prop_ms, prop_cost, clk = timed_arm(prop)
+    rollout_ms, combine_ms = prop.time_passes(20)
+    feat_ms, net_ms = prop.time_proposal(20)
+    prop.set_proposal(None)
+    prop.close()
+    value = world * N * T * args.steps / (prop_ms / 1e3)
+    plain_value = world * N * T * args.steps / (plain_ms / 1e3)
+
+    # ---- e2e: public API (DriverOptions.proposal), host buffers --------------
+    cfg = D.DriverConfig(w.state_dim, w.control_dim, w.horizon, PROPOSAL_K, w.lam,
+                         D.ControlNoiseConfig(D.CovarianceForm.kDiagonal, w.sigma, w.sigma_inv,
+                                              w.control_dim),
+                         D.ControlBounds(w.u_min, w.u_max, w.control_dim))
+    drv = D.MPPIDriver(cfg, D.DriverOptions(proposal=net, proposal_samples=PROPOSAL_SAMPLES))
+    err = D.ErrorRef()
+    spec = D.ModelPluginSpec(plugin_path(w.plugin),
+                             D.CallableNames("mppi_dynamics", "mppi_stage_cost",
+                                             "mppi_terminal_cost"),
+                             D.ParamLayout(len(w.model_params), 4, w.cost_stride, 4),
+                             D.RngConfig(w.seed))
+    assert drv.initialize(spec, err), err.value
+    assert drv.set_problem_params(D.ProblemParams(D.ByteView.of(w.model_params),
+                                                  D.ByteView.of(w.cost_params[0])), err), err.value
+    ap = D.BatchAgentParams(cost_params=w.cost_params_packed, cost_params_stride=w.cost_stride,
+                            sigma=w.agent_sigma)
+    outs = D.BatchSimulationResults(np.zeros((T, N, 4), np.float32),
+                                    np.zeros((T, N, 2), np.float32), np.zeros((T, N), np.float32),
+                                    np.zeros((N, 4), np.float32), N, T)
+    for _ in range(args.warmup):
+        assert drv.reset(None, err)
+        assert drv.simulate_batch(N, T, w.x0, outs, ap, err), err.value
+    e2e_times = []
+    barrier()
+    for _ in range(args.steps):
+        assert drv.reset(None, err)
+        t0 = time.perf_counter()
+        assert drv.simulate_batch(N, T, w.x0, outs, ap, err), err.value
+        e2e_times.append(time.perf_counter() - t0)
+    barrier()
+    e2e_total = max_over_ranks(sum(e2e_times))
+    e2e_cost = models.executed_cost(w, outs.states_out, outs.controls_out,
+                                    outs.terminal_states_out)
+    h2d = (N * 4 + N * PROPOSAL_H * 2 + 4) * 4 + N * ((w.cost_stride + 15) // 16 * 16) + N * 2 * 4
+    d2h = (T * N * (4 + 2 + 1) + N * 4) * 4
+
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return 0
+    # proposal network forward: 2 * rows * (32*256 + 2*256*256 + 256*P) FLOPs
+    out_pad = (PROPOSAL_H * 2 + 2 + 15) // 16 * 16
+    mlp_flops = 2 * N * (32 * 256 + 2 * 256 * 256 + 256 * out_pad)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    bf16_peak = peaks.get("bf16_tflops") or 1590.0
+    line = {
+        "metric": METRIC, "value": value, "unit": "control-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": prop_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 rollout, bf16 network (fp32 accumulate)",
+        "data": "synthetic (seeded PCG64 workload generator, mppi_metal_b200/models.py)",
+        "config": {
+            "workload": (f"proposal: {N} unicycle agents per GPU (16 moving obstacles, sigma "
+                         f"U[0.2,0.8]), H={PROPOSAL_H}, {T} closed-loop steps; proposal-MPPI "
+                         f"K={PROPOSAL_K} ({PROPOSAL_SAMPLES} samples around the network's "
+                         f"prediction) against plain MPPI K={PROPOSAL_PLAIN_K}"),
+            "agents_per_gpu": N, "samples": PROPOSAL_K, "proposal_samples": PROPOSAL_SAMPLES,
+            "plain_samples": PROPOSAL_PLAIN_K, "horizon": PROPOSAL_H, "closed_loop_steps": T,
+            "network": "MLP 31->256->256->256->130, GELU, bf16 weights, fp32 accumulate",
+            "step": "one simulate_batch closed loop (300 control steps for every agent)",
+            "l2": "flushed between timed iterations (256 MiB device write)",
+            "parallelism": "agent-sharded replicas, no data-path collective",
+        },
+        "rollout_steps_per_s": value * PROPOSAL_K * PROPOSAL_H,
+        "plain": {"control_steps_per_s": plain_value, "samples": PROPOSAL_PLAIN_K,
+                  "ms_per_step": plain_ms / args.steps,
+                  "closed_loop_cost_mean": float(plain_cost.mean())},
+        "closed_loop_cost": {"mean": float(prop_cost.mean()), "agents": N,
+                             "vs_plain": float(prop_cost.mean() / plain_cost.mean())},
+        "speedup_vs_plain": value / plain_value,
+        "training": training,
+        "e2e": {"value": world * N * T * args.steps / e2e_total, "unit": "control-steps/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": 1e3 * e2e_total / args.steps,
+                "closed_loop_cost_mean": float(e2e_cost.mean())},
+        "gpu_launches": 4 * T * args.steps,
+        "kernel_ms_per_pass": {"rollout": rollout_ms, "combine": combine_ms,
+                               "features": feat_ms, "network": net_ms},
+        "roofline": {"kernel": "mlp_fused_kernel (proposal network forward)", "bound": "tensor",
+                     "achieved": mlp_flops / (net_ms / 1e3) / 1e12, "peak": bf16_peak,
+                     "unit": "TFLOP/s", "frac": mlp_flops / (net_ms / 1e3) / 1e12 / bf16_peak,
+                     "traffic": None,
+                     "note": "M = 128 rows: one CTA, latency-bound; peak = measured bf16 "
+                             "burst" + ("" if peaks.get("bf16_tflops") else " (fallback)")},
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.mode == "kernels":
         return run_kernels_only(args)
+    if args.workload == "proposal":
+        return run_proposal(args)
     return run_b200(args)
 
 

@@ -248,6 +248,10 @@ int mppi_backend_set_proposal(mppi_backend* b, struct mppi_proposal* proposal,
                               uint32_t proposal_samples, char* err, size_t err_len);
 int mppi_backend_set_record_ustar(mppi_backend* b, uint32_t enable, char* err, size_t err_len);
 int mppi_backend_batch_fetch_ustar(mppi_backend* b, float* ustar_out, char* err, size_t err_len);
+/* Device time (CUDA events) of the proposal stage of one pass on the
+ * prepared batch: the feature kernel and the network's forward pass. */
+int mppi_backend_time_proposal(mppi_backend* b, uint32_t iters, float* features_ms,
+                               float* network_ms, char* err, size_t err_len);
 
 /* Compiles a plugin with the library kernels for sm_100a without loading
  * the result (needs no GPU).  log receives the NVRTC log, including ptxas's

@@ -131,6 +131,8 @@ SIGNATURES = {
     "mppi_backend_set_proposal": (ctypes.c_int, [c_ptr, c_ptr, c_u32] + _ERR),
     "mppi_backend_set_record_ustar": (ctypes.c_int, [c_ptr, c_u32] + _ERR),
     "mppi_backend_batch_fetch_ustar": (ctypes.c_int, [c_ptr, c_ptr] + _ERR),
+    "mppi_backend_time_proposal": (ctypes.c_int, [c_ptr, c_u32, ctypes.POINTER(c_f32),
+                                                  ctypes.POINTER(c_f32)] + _ERR),
     "mppi_compile_check": (ctypes.c_int, [ctypes.POINTER(BackendPlugin),
                                           ctypes.POINTER(BackendConfig), ctypes.c_char_p,
                                           c_size] + _ERR),

@@ -265,6 +265,14 @@ class Backend:
                                                  eb, len(eb)), eb)
         return r.value, c.value
 
+    def time_proposal(self, iters: int = 20):
+        """(features ms, network ms) of one proposal stage on the prepared batch."""
+        f, n = ctypes.c_float(), ctypes.c_float()
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_time_proposal(self.h, iters, ctypes.byref(f),
+                                                   ctypes.byref(n), eb, len(eb)), eb)
+        return f.value, n.value
+
     def tuning_info(self) -> dict:
         """Autotuner choice for the prepared uneven batch (after a run)."""
         g, n, r = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()

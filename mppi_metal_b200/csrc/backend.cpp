@@ -463,11 +463,8 @@ cudaError_t launch_proposal(mppi_backend* b) {
                                              kFeatureStride, b->N, b->d_prop.as<float>());
 }
 
-cudaError_t launch_rollout(mppi_backend* b, uint32_t step_local) {
-  if (b->proposal && b->spec.proposal) {
-    cudaError_t e = launch_proposal(b);
-    if (e != cudaSuccess) return e;
-  }
+// The rollout kernel alone (the proposal's outputs already in place).
+cudaError_t launch_rollout_kernel(mppi_backend* b, uint32_t step_local) {
   MppiRolloutArgs a = rollout_args(b, step_local);
   void* args[] = {&a};
   if (b->ragged) {
@@ -482,6 +479,16 @@ cudaError_t launch_rollout(mppi_backend* b, uint32_t step_local) {
   return cudaLaunchKernel((const void*)b->mod->rollout[b->geom.variant],
                           dim3(b->geom.nblk, b->N), dim3(b->geom.block), args, b->geom.smem,
                           b->stream);
+}
+
+// One rollout pass: the proposal's features and network first when one is
+// attached, then the rollout kernel.
+cudaError_t launch_rollout(mppi_backend* b, uint32_t step_local) {
+  if (b->proposal && b->spec.proposal) {
+    cudaError_t e = launch_proposal(b);
+    if (e != cudaSuccess) return e;
+  }
+  return launch_rollout_kernel(b, step_local);
 }
 
 // Uneven batches: times candidate (grid size, noise staging) pairs on the
@@ -1248,7 +1255,7 @@ int mppi_backend_time_passes(mppi_backend* b, uint32_t iters, float* rollout_ms,
   }
   float ms = 0.0f;
   CK(cudaEventRecord(b->ev0, b->stream));
-  for (uint32_t i = 0; i < iters; ++i) CK(launch_rollout(b, 0));
+  for (uint32_t i = 0; i < iters; ++i) CK(launch_rollout_kernel(b, 0));
   CK(cudaEventRecord(b->ev1, b->stream));
   CK(cudaEventSynchronize(b->ev1));
   CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
@@ -1259,6 +1266,32 @@ int mppi_backend_time_passes(mppi_backend* b, uint32_t iters, float* rollout_ms,
   CK(cudaEventSynchronize(b->ev1));
   CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
   if (combine_ms) *combine_ms = ms / iters;
+  return MPPI_OK;
+}
+
+int mppi_backend_time_proposal(mppi_backend* b, uint32_t iters, float* features_ms,
+                               float* network_ms, char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (b->N == 0 || iters == 0 || !b->proposal || !b->spec.proposal) {
+    set_err(err, err_len, "no proposal attached / no batch prepared / iters == 0.");
+    return MPPI_ERR_INVALID;
+  }
+  float ms = 0.0f;
+  CK(cudaEventRecord(b->ev0, b->stream));
+  for (uint32_t i = 0; i < iters; ++i) CK(launch_proposal(b));
+  CK(cudaEventRecord(b->ev1, b->stream));
+  CK(cudaEventSynchronize(b->ev1));
+  CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  const float both = ms / iters;
+  CK(cudaEventRecord(b->ev0, b->stream));
+  for (uint32_t i = 0; i < iters; ++i)
+    CK(mppi_b200::proposal_enqueue_forward(b->proposal, b->stream, b->d_feat.as<float>(),
+                                           kFeatureStride, b->N, b->d_prop.as<float>()));
+  CK(cudaEventRecord(b->ev1, b->stream));
+  CK(cudaEventSynchronize(b->ev1));
+  CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+  if (network_ms) *network_ms = ms / iters;
+  if (features_ms) *features_ms = both - ms / iters;
   return MPPI_OK;
 }
 

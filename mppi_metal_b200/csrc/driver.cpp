@@ -38,6 +38,7 @@ public:
 	std::vector<float> u_min_storage;
 	std::vector<float> u_max_storage;
 	std::vector<float> u_nominal;  // horizon * control_dim warm start
+	std::string proposal_features;  // owned copy of options.proposal_features
 
 	ParamLayout param_layout{};
 	bool params_bound = false;
@@ -50,7 +51,8 @@ public:
 // Deep copies (reference mppi_driver.cpp:40-76): sigma / sigma_inv hold m
 // floats for kDiagonal, m*m for kFull; bounds hold m floats.
 MPPIDriver::Impl::Impl(const DriverConfig& cfg, const DriverOptions& opts)
-	: config(cfg), options(opts) {
+	: config(cfg), options(opts), proposal_features(opts.proposal_features) {
+	options.proposal_features = proposal_features;  // the caller's view need not outlive us
 	const uint32_t m = cfg.control_dim;
 	const size_t nsig = cfg.noise.covariance_form == ControlNoiseConfig::CovarianceForm::kDiagonal
 		? m
@@ -178,7 +180,7 @@ bool MPPIDriver::initialize(const ModelPluginSpec& model, std::string* error) {
 
 	if (impl_->options.proposal != nullptr) {
 		const mppi_b200::ProposalShape ps = mppi_b200::proposal_shape(impl_->options.proposal);
-		const std::string feat(impl_->options.proposal_features);
+		const std::string& feat = impl_->proposal_features;
 		if (mppi_backend_set_features(impl_->backend, feat.c_str(), ps.input_dim, err.data(),
 		                              err.size()) != MPPI_OK ||
 		    mppi_backend_set_proposal(impl_->backend, impl_->options.proposal,

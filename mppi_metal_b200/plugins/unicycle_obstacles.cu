@@ -82,6 +82,8 @@ __device__ float mppi_terminal_cost(const float* s, const uint8_t* model_params_
 //   [7..31)  the 8 obstacles of least clearance |p - c_i(t)| - r_i (ties:
 //            lower index first), each as its centre's body-frame offset / 10
 //            and its radius; missing obstacles give zeros
+// Everything stays in registers: the clearances of the 16 slots are ranked
+// by 8 unrolled arg-min passes, each taking its winner out of the running.
 __device__ void mppi_proposal_features(const float* s, const uint8_t* model_params_raw,
                                        const uint8_t* cost_params_raw, float* f) {
   const UnicycleCostParams* c = reinterpret_cast<const UnicycleCostParams*>(cost_params_raw);
@@ -97,30 +99,33 @@ __device__ void mppi_proposal_features(const float* s, const uint8_t* model_para
   f[5] = (cs * gx + sn * gy) * 0.1f;
   f[6] = (cs * gy - sn * gx) * 0.1f;
   const unsigned n = c->num_obs < MPPI_UNICYCLE_MAX_OBS ? c->num_obs : MPPI_UNICYCLE_MAX_OBS;
-  float clr[MPPI_UNICYCLE_MAX_OBS];
+  const float inf = __int_as_float(0x7f800000);
+  float ex[MPPI_UNICYCLE_MAX_OBS], ey[MPPI_UNICYCLE_MAX_OBS], clr[MPPI_UNICYCLE_MAX_OBS];
+#pragma unroll
   for (unsigned i = 0; i < MPPI_UNICYCLE_MAX_OBS; ++i) {
-    if (i < n) {
-      const float ex = fmaf(c->obs_vx[i], t, c->obs_cx[i]) - x;
-      const float ey = fmaf(c->obs_vy[i], t, c->obs_cy[i]) - y;
-      clr[i] = sqrtf(ex * ex + ey * ey) - c->obs_r[i];
-    } else {
-      clr[i] = __int_as_float(0x7f800000);
-    }
+    ex[i] = fmaf(c->obs_vx[i], t, c->obs_cx[i]) - x;
+    ey[i] = fmaf(c->obs_vy[i], t, c->obs_cy[i]) - y;
+    clr[i] = i < n ? sqrtf(ex[i] * ex[i] + ey[i] * ey[i]) - c->obs_r[i] : inf;
   }
+#pragma unroll
   for (unsigned j = 0; j < 8; ++j) {
-    int best = -1;
-    float bv = __int_as_float(0x7f800000);
-    for (unsigned i = 0; i < n; ++i)
-      if (clr[i] < bv) {
-        bv = clr[i];
-        best = (int)i;
-      }
-    if (best < 0) break;
-    clr[best] = __int_as_float(0x7f800000);
-    const float ex = fmaf(c->obs_vx[best], t, c->obs_cx[best]) - x;
-    const float ey = fmaf(c->obs_vy[best], t, c->obs_cy[best]) - y;
-    f[7 + 3 * j] = (cs * ex + sn * ey) * 0.1f;
-    f[8 + 3 * j] = (cs * ey - sn * ex) * 0.1f;
-    f[9 + 3 * j] = c->obs_r[best];
+    float bv = inf, bx = 0.0f, by = 0.0f, br = 0.0f;
+    unsigned best = MPPI_UNICYCLE_MAX_OBS;
+#pragma unroll
+    for (unsigned i = 0; i < MPPI_UNICYCLE_MAX_OBS; ++i) {
+      const bool take = clr[i] < bv;  // strict: the lower index wins ties
+      bv = take ? clr[i] : bv;
+      bx = take ? ex[i] : bx;
+      by = take ? ey[i] : by;
+      br = take ? c->obs_r[i] : br;
+      best = take ? i : best;
+    }
+#pragma unroll
+    for (unsigned i = 0; i < MPPI_UNICYCLE_MAX_OBS; ++i) clr[i] = i == best ? inf : clr[i];
+    if (best < MPPI_UNICYCLE_MAX_OBS) {
+      f[7 + 3 * j] = (cs * bx + sn * by) * 0.1f;
+      f[8 + 3 * j] = (cs * by - sn * bx) * 0.1f;
+      f[9 + 3 * j] = br;
+    }
   }
 }
