@@ -77,8 +77,9 @@ def parse():
 
 
 def dist_env():
-    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
-            int(os.environ.get("LOCAL_RANK", 0)))
+    from mppi_metal_b200 import dist
+    r = dist.env()
+    return r.rank, r.world, r.local_rank
 
 
 WORKLOADS = ("batch", "uneven", "single", "quadrotor", "proposal")
@@ -308,36 +309,27 @@ def config_block(name: str = "batch", w=None):
 # ---------------------------------------------------------------------------
 def run_b200(args):
     import torch
-    rank, world, local_rank = dist_env()
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(0)
+    from mppi_metal_b200 import dist
+    R = dist.env()
+    rank, world, local_rank = R.rank, R.world, R.local_rank
+    torch.cuda.set_device(local_rank if world > 1 else 0)
+    dist.init(R, "nccl", timeout_s=300)
     from mppi_metal_b200 import driver as D
     from mppi_metal_b200 import models
     from mppi_metal_b200._lib import plugin_path
     from mppi_metal_b200.backend import Backend
 
-    w = workload_for_rank(rank, args.workload, args.numeric)
+    w = workload_for_rank(rank, args.workload, args.numeric)  # per-rank seed: disjoint agents
     N, T = w.num_agents, w.num_steps
     ks, hs = agent_shapes(w)
     rs_per_step = rollout_steps_per_control_step(w) * T  # per bench step (this rank)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
+        dist.barrier(R, "cuda")
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return dist.max_over_ranks(R, x, "cuda")
 
     # ---- value: device-resident closed loop ---------------------------------
     b = Backend(w.plugin, w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam, w.sigma,
@@ -436,8 +428,7 @@ def run_b200(args):
                    "gpu_closed_loop_cost_same_sample": float(gpu_c.mean())}
 
     if rank != 0:
-        if world > 1:
-            torch.distributed.destroy_process_group()
+        dist.finish(R)
         return 0
 
     rollout_units = rollout_steps_per_control_step(w)  # rollout-steps per rollout launch
@@ -476,8 +467,7 @@ def run_b200(args):
         "clocks": clk,
     }
     print(json.dumps(line))
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    dist.finish(R)
     return 0
 
 
@@ -517,30 +507,21 @@ def run_proposal(args):
     timed): the network is trained on this GPU by the library's kernels on
     ~1.2e6 (features, u*) pairs from plain MPPI at K = 16384."""
     import torch
-    rank, world, local_rank = dist_env()
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
-    else:
-        torch.cuda.set_device(0)
+    from mppi_metal_b200 import dist
+    R = dist.env()
+    rank, world, local_rank = R.rank, R.world, R.local_rank
+    torch.cuda.set_device(local_rank if world > 1 else 0)
+    dist.init(R, "nccl", timeout_s=900)
     from mppi_metal_b200 import driver as D
     from mppi_metal_b200 import models
     from mppi_metal_b200 import proposal as P
     from mppi_metal_b200._lib import plugin_path
 
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
+        dist.barrier(R, "cuda")
 
     def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
+        return dist.max_over_ranks(R, x, "cuda")
 
     t_setup = time.time()
     if args.proposal_weights and Path(args.proposal_weights).exists():
@@ -629,8 +610,7 @@ def run_proposal(args):
     d2h = (T * N * (4 + 2 + 1) + N * 4) * 4
 
     if rank != 0:
-        if world > 1:
-            torch.distributed.destroy_process_group()
+        dist.finish(R)
         return 0
     # proposal network forward: 2 * rows * (32*256 + 2*256*256 + 256*P) FLOPs
     out_pad = (PROPOSAL_H * 2 + 2 + 15) // 16 * 16
@@ -683,8 +663,7 @@ def run_proposal(args):
         "clocks": clk,
     }
     print(json.dumps(line))
-    if world > 1:
-        torch.distributed.destroy_process_group()
+    dist.finish(R)
     return 0
 
 
