@@ -427,6 +427,13 @@ MppiCombineArgs combine_args(const mppi_backend* b, uint32_t step_local, bool pr
   c.hist_costs = b->want_k ? b->d_hk.as<float>() : nullptr;
   c.terminal = b->want_t ? b->d_term.as<float>() : nullptr;
   c.hist_ustar = (b->record_ustar && b->T > 0 && propagate) ? b->d_hu.as<float>() : nullptr;
+  if (propagate && b->proposal && b->spec.proposal) {
+    // features of the propagated state feed the next step's network
+    c.cost_params = b->run_cp;
+    c.cost_stride = b->run_cp_stride;
+    c.features = b->d_feat.as<float>();
+    c.feature_stride = kFeatureStride;
+  }
   if (b->ragged) {
     const uint32_t* info = b->d_agent_info.as<uint32_t>();
     c.agent_K = info;
@@ -441,9 +448,9 @@ size_t combine_smem(const mppi_backend* b) {
   return (pad4(b->geom.nblk) + pad4(b->HM())) * 4;
 }
 
-// Proposal features of the current states, then the network's forward pass
-// (both on the backend stream, so they are captured into the closed loop).
-cudaError_t launch_proposal(mppi_backend* b) {
+// Proposal features of the current states (the closed loop computes them
+// inside the previous step's combine instead, once it has the new state).
+cudaError_t launch_features(mppi_backend* b) {
   MppiFeaturesArgs f{};
   f.rows = b->N;
   f.agents_mod = b->N;
@@ -456,11 +463,20 @@ cudaError_t launch_proposal(mppi_backend* b) {
   f.cost_stride = b->run_cp_stride;
   f.out = b->d_feat.as<float>();
   void* fa[] = {&f};
-  cudaError_t e = cudaLaunchKernel((const void*)b->mod->features, dim3((b->N + 127) / 128),
-                                   dim3(128), fa, 0, b->stream);
-  if (e != cudaSuccess) return e;
+  return cudaLaunchKernel((const void*)b->mod->features, dim3((b->N + 127) / 128), dim3(128), fa,
+                          0, b->stream);
+}
+
+// The network's forward pass on the current features.
+cudaError_t launch_network(mppi_backend* b) {
   return mppi_b200::proposal_enqueue_forward(b->proposal, b->stream, b->d_feat.as<float>(),
                                              kFeatureStride, b->N, b->d_prop.as<float>());
+}
+
+// Features, then the network (both on the backend stream).
+cudaError_t launch_proposal(mppi_backend* b) {
+  cudaError_t e = launch_features(b);
+  return e == cudaSuccess ? launch_network(b) : e;
 }
 
 // The rollout kernel alone (the proposal's outputs already in place).
@@ -687,8 +703,13 @@ int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t le = cudaSuccess;
+    const bool prop = b->proposal && b->spec.proposal;
+    // with a proposal: features of x0 once, then per step network -> rollout
+    // -> combine (which leaves the next step's features behind)
+    if (prop) le = launch_features(b);
     for (uint32_t s = 0; s < b->T && le == cudaSuccess; ++s) {
-      le = launch_rollout(b, s);
+      if (prop) le = launch_network(b);
+      if (le == cudaSuccess) le = launch_rollout_kernel(b, s);
       if (le == cudaSuccess) le = launch_combine(b, s, true);
     }
     cudaError_t ce = cudaStreamEndCapture(b->stream, &g);

@@ -558,6 +558,20 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
     for (int d = 0; d < kN; ++d) xg[d] = st[d];
     if (a.terminal)
       for (int d = 0; d < kN; ++d) a.terminal[(size_t)agent * kN + d] = st[d];
+#ifdef MPPI_FEATURES_FN
+    // the next step's proposal features, from the state just propagated
+    if (a.features) {
+      float f[MPPI_MAX_FEATURES];
+#pragma unroll
+      for (int i = 0; i < MPPI_MAX_FEATURES; ++i) f[i] = 0.0f;
+      MPPI_FEATURES_FN(st, a.model_params + a.model_stride * agent,
+                       a.cost_params + a.cost_stride * agent, f);
+      float* o = a.features + (size_t)agent * a.feature_stride;
+#pragma unroll
+      for (int i = 0; i < MPPI_MAX_FEATURES; ++i)
+        if ((uint32_t)i < a.feature_stride) o[i] = f[i];
+    }
+#endif
   }
   for (uint32_t j = tid; j < HM; j += kCombineBlock) {
     const uint32_t t = j / kM, d = j % kM;

@@ -104,6 +104,13 @@ struct MppiCombineArgs {
   uint32_t block;
   uint32_t pad0;
   float* hist_ustar;   // [T][N][H*m] the updated sequence u* of every step (may be null)
+  // Proposal features of the propagated state, for the next step's network
+  // (modules compiled with MPPI_FEATURES_FN; null = none).
+  const uint8_t* cost_params;
+  uint64_t cost_stride;
+  float* features;          // [N][feature_stride]
+  uint32_t feature_stride;  // <= MPPI_MAX_FEATURES
+  uint32_t pad1;
 };
 
 // Proposal features of state rows: row r is a state of agent r % agents_mod

@@ -14,6 +14,11 @@
 //               with the loss (Gaussian NLL of u*) and three more GEMMs for
 //               the activation gradients dH = dZ W, saving for the weight
 //               gradients dZ^T and H^T (batch-contiguous images).
+//   mlp_forward_cluster   inference: a cluster of 4 CTAs per 128 rows, each
+//               computing a quarter of every layer's output columns and
+//               broadcasting its slice of the activations into the other
+//               CTAs' shared memory (DSMEM), so the epilogues and weight
+//               loads of one tile are spread over 4 SMs.
 //   mlp_wgrad   dW_l = dZ_l^T H_{l-1} summed over the batch: split over
 //               batch chunks, a 4-stage bulk-copy ring feeding the MMAs,
 //               FP32 atomics into the gradient.
@@ -372,6 +377,213 @@ __global__ void __launch_bounds__(kFusedThreads, 1) mlp_fused_kernel(const Fused
   if (warp == 0) {
     tc::fence_after_sync();
     tc::tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// mlp_forward_cluster: inference, 4 CTAs (one cluster) per 128-row tile
+// ---------------------------------------------------------------------------
+constexpr uint32_t kCluster = 4;
+constexpr uint32_t kCThreads = kTile * kGroups;        // 512
+constexpr uint32_t kCSmemW = 64 * kHid * 2;            // this CTA's weight rows (<= 64)
+constexpr uint32_t kBiasFloats = 3 * kHid + kHid;       // b0..b2 and b3 (<= 256)
+constexpr uint32_t kClusterSmem = 2 * kSmemA + kCSmemW + kSmemBar + kBiasFloats * 4;
+constexpr uint32_t kCTmemCols = 64;
+static_assert(kClusterSmem <= 232448, "cluster kernel exceeds the shared-memory limit");
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t map_to_rank(uint32_t saddr, uint32_t rank) {
+  uint32_t out;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(saddr), "r"(rank));
+  return out;
+}
+__device__ __forceinline__ void st_cluster_v4(uint32_t addr, uint4 v) {
+  asm volatile("st.shared::cluster.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x),
+               "r"(v.y), "r"(v.z), "r"(v.w)
+               : "memory");
+}
+// Every thread of every CTA of the cluster arrives; all pass together.
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_cluster() {
+  asm volatile("fence.proxy.async.shared::cluster;" ::: "memory");
+}
+
+// 16-column chunks of an N-wide layer dealt to the cluster's CTAs.
+__device__ __forceinline__ void cluster_slice(uint32_t N, uint32_t c, uint32_t& col0,
+                                              uint32_t& ncols) {
+  const uint32_t chunks = N / 16, q = chunks / kCluster, rem = chunks % kCluster;
+  col0 = 16 * (c * q + min(c, rem));
+  ncols = 16 * (q + (c < rem ? 1u : 0u));
+}
+
+// Activations ping-pong between two A tiles: layer g reads A[g % 2] and its
+// epilogue writes A[(g + 1) % 2] in all four CTAs.  A CTA last read that
+// tile in layer g - 1, which it finished before the cluster barrier that
+// ends layer g - 1, so no write can reach a tile still being read.
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
+    mlp_forward_cluster_kernel(const FusedArgs a) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  bf16* as0 = reinterpret_cast<bf16*>(smem);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * kSmemA + kCSmemW);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+  volatile uint32_t* abort_s = tslot + 1;
+  float* bias_s = reinterpret_cast<float*>(smem + 2 * kSmemA + kCSmemW + kSmemBar);  // [4][256]
+
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t quarter = warp & 3u, grp = warp >> 2;
+  const uint32_t r = quarter * 32 + lane;
+  const uint32_t crank = cluster_rank();
+  for (uint32_t i = tid; i < kBiasFloats; i += kCThreads) {
+    const uint32_t l = i / kHid, n = i % kHid;
+    bias_s[i] = (l < 3 || n < a.out_pad) ? a.b[l][n] : 0.0f;
+  }
+  const uint32_t row = (blockIdx.x / kCluster) * kTile + r;
+  const bool valid = row < a.rows;
+  const uint32_t bar_w = tc::smem_addr(&bars[0]), bar_m = tc::smem_addr(&bars[1]);
+  const uint32_t a_s0 = tc::smem_addr(as0), w_s = a_s0 + 2 * kSmemA;
+
+  if (tid == 0) {
+    tc::mbar_init(bar_w, 1);
+    tc::mbar_init(bar_m, 1);
+    *abort_s = 0;
+    tc::mbar_init_fence();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tc::smem_addr(tslot), kCTmemCols);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = *tslot;
+  const uint32_t t_row = tmem + ((quarter * 32u) << 16);
+  cluster_sync_all();  // every CTA of the cluster is running before any DSMEM write
+
+  bool w_pending = false;
+  uint32_t ph_w = 0, ph_m = 0;
+  {
+    uint32_t c0, nc;
+    cluster_slice(kHid, crank, c0, nc);
+    if (tid == 0 && nc) {
+      load_operand(w_s, a.W[0] + (size_t)c0 * kIn, nc * kIn * 2, bar_w);
+      w_pending = true;
+    }
+  }
+  // input rows -> A[0] (every CTA stages the whole tile)
+#pragma unroll
+  for (uint32_t j = grp; j < kIn / 16; j += kGroups) {
+    float v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const uint32_t c = 16 * j + i;
+      v[i] = (valid && c < a.in_dim) ? a.x[(size_t)row * a.x_stride + c] : 0.0f;
+    }
+    a_store16(as0, r, j, kIn, v);
+  }
+
+  for (uint32_t g = 0; g < 4; ++g) {
+    const uint32_t K = g == 0 ? kIn : kHid, N = g == 3 ? a.out_pad : kHid;
+    uint32_t col0, nc;
+    cluster_slice(N, crank, col0, nc);
+    const uint32_t a_in = a_s0 + (g & 1u) * kSmemA;
+    if (tid == 0 && w_pending) {
+      if (tc::mbar_wait(bar_w, ph_w)) {
+        w_pending = false;
+        ph_w ^= 1u;
+      } else {
+        atomicOr(a.err, 1);
+        *abort_s = 1;
+      }
+    }
+    tc::fence_async_shared();
+    tc::fence_before_sync();
+    __syncthreads();
+    const bool run = !*abort_s && nc > 0;
+    if (run && tid == 0) {
+      tc::fence_async_shared();
+      tc::fence_after_sync();
+      const uint32_t idesc = tc::idesc_bf16(kTile, nc);
+      const uint32_t sbo = K * 16;
+      for (uint32_t s = 0; s < K / 16; ++s)
+        tc::mma_bf16(tmem, tc::sdesc(a_in + s * 256, 128, sbo), tc::sdesc(w_s + s * 256, 128, sbo),
+                     idesc, s > 0 ? 1u : 0u);
+      tc::mma_commit(bar_m);
+    }
+    bool done = true;
+    if (run) {
+      done = tc::mbar_wait(bar_m, ph_m);
+      ph_m ^= 1u;
+    }
+    if (__syncthreads_or(!done)) {
+      if (tid == 0) {
+        atomicOr(a.err, 2);
+        *abort_s = 1;
+      }
+      __syncthreads();
+    }
+    tc::fence_after_sync();
+    const bool ok = run && !*abort_s;
+    // the next layer's weight rows stream in during this epilogue
+    if (tid == 0 && g < 3 && !*abort_s) {
+      uint32_t c1, n1;
+      cluster_slice(g == 2 ? a.out_pad : kHid, crank, c1, n1);
+      if (n1) {
+        load_operand(w_s, a.W[g + 1] + (size_t)c1 * kHid, n1 * kHid * 2, bar_w);
+        w_pending = true;
+      }
+    }
+    if (ok && g < 3) {
+      // h = GELU(acc + b) for this CTA's columns, into A[(g + 1) % 2] of all CTAs
+      const float* bias = bias_s + g * kHid + col0;
+      const uint32_t a_out = a_s0 + ((g + 1) & 1u) * kSmemA;
+      for (uint32_t j = grp; j < nc / 16; j += kGroups) {
+        float v[16];
+        tc::tmem_ld16(t_row + 16 * j, v);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = gelu(v[i] + bias[16 * j + i]);
+        const uint4 lo = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]),
+                                    pack2(v[6], v[7]));
+        const uint4 hi = make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]),
+                                    pack2(v[14], v[15]));
+        const uint32_t off = a_out + 2 * canon(r, col0 + 16 * j, kHid);
+#pragma unroll
+        for (uint32_t q = 0; q < kCluster; ++q) {
+          const uint32_t dst = map_to_rank(off, q);
+          st_cluster_v4(dst, lo);
+          st_cluster_v4(dst + 128, hi);
+        }
+      }
+    } else if (ok) {
+      // output layer: this CTA's columns straight to global memory
+      const float* bias = bias_s + 3 * kHid + col0;
+      for (uint32_t j = grp; j < nc / 16; j += kGroups) {
+        float v[16];
+        tc::tmem_ld16(t_row + 16 * j, v);
+        if (valid) {
+          float* o = a.out + (size_t)row * a.out_stride + col0 + 16 * j;
+#pragma unroll
+          for (int i = 0; i < 16; ++i) o[i] = v[i] + bias[16 * j + i];
+        }
+      }
+    }
+    fence_async_cluster();
+    tc::fence_before_sync();
+    cluster_sync_all();
+  }
+
+  if (tid == 0 && w_pending && !tc::mbar_wait(bar_w, ph_w)) atomicOr(a.err, 4);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_dealloc(tmem, kCTmemCols);
   }
 }
 
@@ -825,7 +1037,7 @@ cudaError_t proposal_enqueue_forward(mppi_proposal* p, cudaStream_t stream, cons
   f.hm = p->hm;
   f.m = p->cfg.control_dim;
   f.train = 0;
-  mlp_fused_kernel<<<f.mp / kTile, kFusedThreads, kFusedSmem, stream>>>(f);
+  mlp_forward_cluster_kernel<<<(f.mp / kTile) * kCluster, kCThreads, kClusterSmem, stream>>>(f);
   return cudaGetLastError();
 }
 
@@ -915,7 +1127,10 @@ mppi_proposal* mppi_proposal_create(const mppi_proposal_config* c, char* err, si
   if ((e = cudaFuncSetAttribute(mlp_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kFusedSmem)) != cudaSuccess ||
       (e = cudaFuncSetAttribute(mlp_wgrad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                kWgradSmem)) != cudaSuccess)
+                                kWgradSmem)) != cudaSuccess ||
+      (e = cudaFuncSetAttribute(mlp_forward_cluster_kernel,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kClusterSmem)) !=
+          cudaSuccess)
     return fail("cudaFuncSetAttribute", e);
 
   // initial weights: U(-1/sqrt(fan_in), 1/sqrt(fan_in)), output layer x 0.1

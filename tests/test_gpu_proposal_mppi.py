@@ -181,3 +181,35 @@ def test_driver_api_runs_the_proposal():
     r = b.fetch()
     assert np.array_equal(outs.states_out, r["states"])
     assert np.array_equal(outs.controls_out, r["controls"])
+
+
+def test_fused_next_step_features_match_the_feature_kernel():
+    """In the captured closed loop each combine also evaluates the next
+    step's features; chaining one-step loops (each starting with the
+    separate feature kernel) must give the same trajectory bit for bit."""
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.unicycle_batch(seed=9, N=16, K=256, H=64, T=4)
+    net = ProposalNet(31, 64, 2, max_batch=256, seed=4)
+
+    def backend():
+        b = backend_for(w, bind=True)
+        b.set_features(FEATURES, 31)
+        b.set_proposal(net, 128)
+        return b
+
+    b = backend()
+    b.prepare(16, 4, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+              sigma=w.agent_sigma)
+    b.run(0)
+    whole = b.fetch()
+    c = backend()
+    x, un, states = w.x0, None, []
+    for s in range(4):
+        c.prepare(16, 1, x, un, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+                  sigma=w.agent_sigma)
+        c.run(s)
+        r = c.fetch()
+        states.append(r["states"][0])
+        x, un = r["x"], r["u_nom"]
+    assert np.array_equal(whole["states"], np.stack(states))
+    assert np.array_equal(whole["terminal"], x)
