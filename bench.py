@@ -473,7 +473,24 @@ def run_b200(args):
 
 def run_kernels_only(args):
     """Prepares the workload and launches the rollout and combine kernels
-    `iters` times each (no closed loop, no host copies in between)."""
+    `iters` times each (no closed loop, no host copies in between).  For the
+    proposal workload: a 3-step proposal closed loop (features, network,
+    rollout, combine) with an untrained network, then one training step on
+    8192 random rows (the network kernels' small capture target)."""
+    if args.workload == "proposal":
+        import torch
+        from mppi_metal_b200 import models
+        from mppi_metal_b200 import proposal as P
+        torch.cuda.set_device(0)
+        net = P.ProposalNet(P.UNICYCLE_FEATURES, PROPOSAL_H, 2, max_batch=8192, seed=0)
+        w = models.unicycle_batch(seed=4000, N=PROPOSAL_AGENTS, K=PROPOSAL_K, H=PROPOSAL_H, T=3)
+        r = P.closed_loop(w, net, PROPOSAL_SAMPLES, repeats=args.iters)
+        x = torch.randn(8192, P.UNICYCLE_FEATURES, device="cuda")
+        y = torch.randn(8192, PROPOSAL_H * 2, device="cuda")
+        loss = net.train_step(x, y, lr=1e-3)
+        print(json.dumps({"mode": "kernels", "workload": "proposal", "closed_loop_ms": r["ms"],
+                          "train_loss": loss, "train_ms": net.last_train_ms()}))
+        return 0
     from mppi_metal_b200.backend import Backend
     w = workload_for_rank(0)
     b = Backend(w.plugin, w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam, w.sigma,

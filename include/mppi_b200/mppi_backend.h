@@ -232,8 +232,10 @@ int mppi_backend_dispatch_rollout_noalloc(mppi_backend* b, uint64_t step_index, 
  * proposal_samples of each agent as (mu - u_nom) + exp(clamp(s)) * n around
  * the predicted sequence mu with the predicted log-scales s, and the other
  * samples as before.  Weights, update and warm start are unchanged.  Needs
- * the network's control_dim == control_dim, horizon >= horizon and
- * input_dim <= feature_dim.  Takes effect at the next prepare.
+ * the network's control_dim == control_dim and input_dim <= feature_dim; a
+ * network predicting fewer steps than the horizon shifts only those steps
+ * (the rest keep the warm start as their mean).  Takes effect at the next
+ * prepare.
  *
  * set_record_ustar (next prepare on) makes the batch closed loop keep the
  * updated sequence u* of every step; batch_fetch_ustar copies it out as
@@ -258,6 +260,13 @@ int mppi_backend_time_proposal(mppi_backend* b, uint32_t iters, float* features_
  * register / shared-memory / spill report for every kernel. */
 int mppi_compile_check(const mppi_backend_plugin* plugin, const mppi_backend_config* config,
                        char* log, size_t log_len, char* err, size_t err_len);
+/* The same for the module a learned proposal uses: proposal != 0 compiles
+ * the proposal sampling into the rollout, features (may be NULL) names the
+ * plugin's feature callable. */
+int mppi_compile_check_proposal(const mppi_backend_plugin* plugin,
+                                const mppi_backend_config* config, uint32_t proposal,
+                                const char* features, char* log, size_t log_len, char* err,
+                                size_t err_len);
 
 /* Library version string. */
 const char* mppi_b200_version(void);

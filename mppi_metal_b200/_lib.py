@@ -136,6 +136,10 @@ SIGNATURES = {
     "mppi_compile_check": (ctypes.c_int, [ctypes.POINTER(BackendPlugin),
                                           ctypes.POINTER(BackendConfig), ctypes.c_char_p,
                                           c_size] + _ERR),
+    "mppi_compile_check_proposal": (ctypes.c_int, [ctypes.POINTER(BackendPlugin),
+                                                   ctypes.POINTER(BackendConfig), c_u32,
+                                                   ctypes.c_char_p, ctypes.c_char_p, c_size]
+                                    + _ERR),
     "mppi_b200_version": (ctypes.c_char_p, []),
     # mppi_proposal.h
     "mppi_proposal_create": (c_ptr, [ctypes.POINTER(ProposalConfig)] + _ERR),

@@ -306,7 +306,9 @@ def device_philox(c0, c1, key) -> np.ndarray:
 def compile_check(plugin: str, state_dim: int, control_dim: int, cov_full: bool = False,
                   control_cost: bool = False, stage_cost: str = "mppi_stage_cost",
                   terminal_cost: str = "mppi_terminal_cost", dynamics: str = "mppi_dynamics",
-                  model_params_size: int = 0, cost_params_size: int = 0):
+                  model_params_size: int = 0, cost_params_size: int = 0,
+                  proposal: bool = False, features: Optional[str] = None,
+                  numeric_mode: int = 0):
     """NVRTC-compile a plugin with the library kernels for sm_100a (no GPU).
     Returns (status, error, log)."""
     lib = _lib.load()
@@ -314,8 +316,10 @@ def compile_check(plugin: str, state_dim: int, control_dim: int, cov_full: bool 
     plug = _lib.BackendPlugin(path.encode(), dynamics.encode(), stage_cost.encode(),
                               terminal_cost.encode(), model_params_size, cost_params_size, 0)
     cfg = _lib.BackendConfig(state_dim, control_dim, 8, 64, 1.0, 1 if cov_full else 0, None, None,
-                             None, None, 0, 1 if control_cost else 0)
+                             None, None, numeric_mode, 1 if control_cost else 0)
     log = ctypes.create_string_buffer(1 << 18)
     eb = _lib.err_buf(1 << 16)
-    rc = lib.mppi_compile_check(ctypes.byref(plug), ctypes.byref(cfg), log, len(log), eb, len(eb))
+    rc = lib.mppi_compile_check_proposal(ctypes.byref(plug), ctypes.byref(cfg), int(proposal),
+                                         features.encode() if features else None, log, len(log),
+                                         eb, len(eb))
     return rc, eb.value.decode(errors="replace"), log.value.decode(errors="replace")

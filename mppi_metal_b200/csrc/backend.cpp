@@ -1318,6 +1318,12 @@ int mppi_backend_time_proposal(mppi_backend* b, uint32_t iters, float* features_
 
 int mppi_compile_check(const mppi_backend_plugin* plugin, const mppi_backend_config* cfg,
                        char* log, size_t log_len, char* err, size_t err_len) {
+  return mppi_compile_check_proposal(plugin, cfg, 0, nullptr, log, log_len, err, err_len);
+}
+
+int mppi_compile_check_proposal(const mppi_backend_plugin* plugin, const mppi_backend_config* cfg,
+                                uint32_t proposal, const char* features, char* log,
+                                size_t log_len, char* err, size_t err_len) {
   if (!plugin || !cfg) {
     set_err(err, err_len, "null argument.");
     return MPPI_ERR_INVALID;
@@ -1334,6 +1340,12 @@ int mppi_compile_check(const mppi_backend_plugin* plugin, const mppi_backend_con
   spec.noise_half = cfg->numeric_mode != 0;
   spec.model_params_bytes = plugin->model_params_size;
   spec.cost_params_bytes = plugin->cost_params_size;
+  spec.proposal = proposal != 0;
+  spec.features = features ? features : "";
+  if (!spec.features.empty() && !valid_identifier(features)) {
+    set_err(err, err_len, std::string("Callable '") + features + "' is not a valid identifier.");
+    return MPPI_ERR_CALLABLE;
+  }
   if (!valid_identifier(spec.dynamics.c_str())) {
     set_err(err, err_len, "Required callable '" + spec.dynamics + "' is not a valid identifier.");
     return MPPI_ERR_CALLABLE;
@@ -1487,10 +1499,10 @@ int mppi_backend_set_proposal(mppi_backend* b, mppi_proposal* p, uint32_t propos
       set_err(err, err_len, "set a feature callable first (mppi_backend_set_features).");
       return MPPI_ERR_INVALID;
     }
-    if (ps.control_dim != b->m || ps.horizon < b->H || ps.input_dim > b->feature_dim) {
+    if (ps.control_dim != b->m || ps.input_dim > b->feature_dim) {
       set_err(err, err_len,
-              "proposal network shape does not fit: need control_dim == DriverConfig::control_dim, "
-              "horizon >= DriverConfig::horizon and input_dim <= the feature dimension.");
+              "proposal network shape does not fit: need control_dim == DriverConfig::control_dim "
+              "and input_dim <= the feature dimension.");
       return MPPI_ERR_INVALID;
     }
     if (ps.device != b->device) {

@@ -276,7 +276,8 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   float ps[kM];
   if (pcount) {
     const float* po = a.prop_out + (size_t)agent * a.prop_stride;
-    for (uint32_t i = tid; i < HM; i += BLOCK) sh_s[i] = po[i] - un_g[i];
+    for (uint32_t i = tid; i < HM; i += BLOCK)
+      sh_s[i] = i < a.prop_ls_offset ? po[i] - un_g[i] : 0.0f;
 #pragma unroll
     for (int d = 0; d < kM; ++d)
       ps[d] = expf(clampf(po[a.prop_ls_offset + d], a.prop_ls_min, a.prop_ls_max));

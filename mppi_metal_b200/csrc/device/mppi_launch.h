@@ -61,6 +61,8 @@ struct MppiRolloutArgs {
   // with mu_t[d] = prop_out[a * prop_stride + t * m + d] (the network's
   // predicted u*) and s[d] = prop_out[a * prop_stride + prop_ls_offset + d];
   // the other samples draw the plain eps_t = sigma * n_t.
+  // The network may predict fewer steps than the horizon: entries j >=
+  // prop_ls_offset (= its H * m) of the sequence get no mean shift.
   const float* prop_out;
   uint32_t prop_stride;
   uint32_t prop_count;

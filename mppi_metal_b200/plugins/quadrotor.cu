@@ -2,6 +2,7 @@
 // (layout and formulas in model_params.h).  State [p(3), v(3), phi, theta,
 // psi, p, q, r], control [f1..f4].  Cost: waypoint tracking plus the
 // penetration of up to 32 spherical obstacles, evaluated branch-free.
+// mppi_proposal_features gives the learned proposal its 29 inputs.
 #include "mppi_core.h"
 #include "model_params.h"
 
@@ -78,4 +79,56 @@ __device__ float mppi_terminal_cost(const float* s, const uint8_t* model_params_
                                     const uint8_t* cost_params_raw) {
   const QuadrotorCostParams* c = reinterpret_cast<const QuadrotorCostParams*>(cost_params_raw);
   return c->w_terminal * quad_position_cost(s, c);
+}
+
+// Proposal features (29 of them):
+//   [0..3)   (p - waypoint) / 4        [3..6)   v / 2
+//   [6..9)   phi, theta, psi           [9..12)  body rates / 4
+//   [12]     z / 4
+//   [13..29) the 4 obstacles of least clearance |p - c_i| - r_i (ties: lower
+//            index first): (c_i - p) / 4 and r_i; missing ones give zeros
+// The ranking stays in registers (4 unrolled arg-min passes over 32 slots).
+__device__ void mppi_proposal_features(const float* s, const uint8_t* model_params_raw,
+                                       const uint8_t* cost_params_raw, float* f) {
+  const QuadrotorCostParams* c = reinterpret_cast<const QuadrotorCostParams*>(cost_params_raw);
+  f[0] = (s[0] - c->wp_x) * 0.25f;
+  f[1] = (s[1] - c->wp_y) * 0.25f;
+  f[2] = (s[2] - c->wp_z) * 0.25f;
+  f[3] = s[3] * 0.5f;
+  f[4] = s[4] * 0.5f;
+  f[5] = s[5] * 0.5f;
+  f[6] = s[6];
+  f[7] = s[7];
+  f[8] = s[8];
+  f[9] = s[9] * 0.25f;
+  f[10] = s[10] * 0.25f;
+  f[11] = s[11] * 0.25f;
+  f[12] = s[2] * 0.25f;
+  const unsigned n = c->num_obs < MPPI_QUAD_MAX_OBS ? c->num_obs : MPPI_QUAD_MAX_OBS;
+  const float inf = __int_as_float(0x7f800000);
+  float clr[MPPI_QUAD_MAX_OBS];
+#pragma unroll
+  for (unsigned i = 0; i < MPPI_QUAD_MAX_OBS; ++i) {
+    const float ex = c->obs_cx[i] - s[0], ey = c->obs_cy[i] - s[1], ez = c->obs_cz[i] - s[2];
+    clr[i] = i < n ? sqrtf(ex * ex + ey * ey + ez * ez) - c->obs_r[i] : inf;
+  }
+#pragma unroll
+  for (unsigned j = 0; j < 4; ++j) {
+    float bv = inf;
+    unsigned best = MPPI_QUAD_MAX_OBS;
+#pragma unroll
+    for (unsigned i = 0; i < MPPI_QUAD_MAX_OBS; ++i) {
+      const bool take = clr[i] < bv;  // strict: the lower index wins ties
+      bv = take ? clr[i] : bv;
+      best = take ? i : best;
+    }
+#pragma unroll
+    for (unsigned i = 0; i < MPPI_QUAD_MAX_OBS; ++i) clr[i] = i == best ? inf : clr[i];
+    if (best < MPPI_QUAD_MAX_OBS) {
+      f[13 + 4 * j] = (c->obs_cx[best] - s[0]) * 0.25f;
+      f[14 + 4 * j] = (c->obs_cy[best] - s[1]) * 0.25f;
+      f[15 + 4 * j] = (c->obs_cz[best] - s[2]) * 0.25f;
+      f[16 + 4 * j] = c->obs_r[best];
+    }
+  }
 }

@@ -15,10 +15,12 @@ import numpy as np
 from . import _lib, models
 from .backend import Backend, BackendError
 
-# The unicycle plugin's feature callable and its width (31 = state 5, goal 2,
-# 8 obstacles x 3); the network's input is padded to 32.
+# The plugins' feature callable and its widths: unicycle 31 (state 5, goal 2,
+# 8 obstacles x 3), quadrotor 29 (state 13, 4 obstacles x 4); the network's
+# input is padded to 32.
 FEATURES_CALLABLE = "mppi_proposal_features"
 UNICYCLE_FEATURES = 31
+QUADROTOR_FEATURES = 29
 
 
 def _check(rc: int, eb) -> None:
@@ -173,24 +175,36 @@ def _prepare(b: Backend, w: models.Workload) -> None:
               cost_stride=w.cost_stride, sigma=w.agent_sigma)
 
 
-def collect_pairs(seeds, agents: int = 1024, steps: int = 300, sample_count: int = 16384,
-                  horizon: int = 64):
-    """(features [R][31], u* [R][H*m]) from plain-MPPI closed loops of the
-    batched unicycle problem, one run of `agents` x `steps` per seed."""
+def collect_pairs_for(make_workload, seeds, feature_dim: int, target_steps: Optional[int] = None):
+    """(features [R][feature_dim], u* [R][target_steps*m]) from plain-MPPI
+    closed loops: one batched run of make_workload(seed) per seed, u* of
+    every step recorded on the device, the recorded states featurised by the
+    plugin's feature callable.  target_steps keeps the first steps of u*
+    (a network may predict fewer steps than the horizon)."""
     feats, targets = [], []
     for seed in seeds:
-        w = models.unicycle_batch(seed=seed, N=agents, K=sample_count, H=horizon, T=steps)
+        w = make_workload(seed)
+        N, T, m = w.num_agents, w.num_steps, w.control_dim
         b = make_backend(w)
-        b.set_features(FEATURES_CALLABLE, UNICYCLE_FEATURES)
+        b.set_features(FEATURES_CALLABLE, feature_dim)
         b.set_record_ustar(True)
         _prepare(b, w)
         b.run(0)
         r = b.fetch()
-        us = b.fetch_ustar()
-        feats.append(b.features(r["states"].reshape(-1, w.state_dim), agents_mod=agents))
-        targets.append(us.reshape(steps * agents, horizon * w.control_dim))
+        us = b.fetch_ustar()[:, :, :(target_steps or w.horizon)]
+        feats.append(b.features(r["states"].reshape(-1, w.state_dim), agents_mod=N))
+        targets.append(np.ascontiguousarray(us.reshape(T * N, -1)))
         b.close()
     return np.concatenate(feats), np.concatenate(targets)
+
+
+def collect_pairs(seeds, agents: int = 1024, steps: int = 300, sample_count: int = 16384,
+                  horizon: int = 64):
+    """(features [R][31], u* [R][H*m]) from plain-MPPI closed loops of the
+    batched unicycle problem, one run of `agents` x `steps` per seed."""
+    return collect_pairs_for(
+        lambda seed: models.unicycle_batch(seed=seed, N=agents, K=sample_count, H=horizon,
+                                           T=steps), seeds, UNICYCLE_FEATURES)
 
 
 def train(features: np.ndarray, targets: np.ndarray, horizon: int, control_dim: int,
@@ -212,7 +226,7 @@ def closed_loop(w: models.Workload, net: Optional[ProposalNet] = None,
     returns the executed cost per agent and the device time per run."""
     b = make_backend(w, sample_count)
     if net is not None:
-        b.set_features(FEATURES_CALLABLE, UNICYCLE_FEATURES)
+        b.set_features(FEATURES_CALLABLE, net.input_dim)
         b.set_proposal(net, proposal_samples)
     ms = []
     for _ in range(repeats):

@@ -200,3 +200,29 @@ def unicycle_features(state, blob: bytes) -> np.ndarray:
         f[8 + 3 * j] = (cs * ey[i] - sn * ex[i]) * 0.1
         f[9 + 3 * j] = r[i]
     return f
+
+
+# Proposal features of the quadrotor plugin (mppi_proposal_features in
+# mppi_metal_b200/plugins/quadrotor.cu; QuadrotorCostParams: 12 header words,
+# then cx, cy, cz, r x 32).
+QUAD_MAX_OBS = 32
+
+
+def quadrotor_features(state, blob: bytes) -> np.ndarray:
+    """The 29 features of one quadrotor state (float64)."""
+    w = np.frombuffer(blob, dtype=np.float32).astype(np.float64)
+    n = min(int(np.frombuffer(blob[36:40], dtype=np.uint32)[0]), QUAD_MAX_OBS)
+    wp = w[0:3]
+    cx, cy, cz, r = w[12:12 + 4 * QUAD_MAX_OBS].reshape(4, QUAD_MAX_OBS)
+    s = np.asarray(state, np.float64)
+    f = np.zeros(29)
+    f[0:3] = (s[0:3] - wp) * 0.25
+    f[3:6] = s[3:6] * 0.5
+    f[6:9] = s[6:9]
+    f[9:12] = s[9:12] * 0.25
+    f[12] = s[2] * 0.25
+    ex, ey, ez = cx[:n] - s[0], cy[:n] - s[1], cz[:n] - s[2]
+    clr = np.sqrt(ex * ex + ey * ey + ez * ez) - r[:n]
+    for j, i in enumerate(np.argsort(clr, kind="stable")[:4]):
+        f[13 + 4 * j:17 + 4 * j] = [ex[i] * 0.25, ey[i] * 0.25, ez[i] * 0.25, r[i]]
+    return f
