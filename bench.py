@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--workload", choices=WORKLOADS, default="batch",
                     help="batch (default, the headline configuration), uneven, single, "
-                         "quadrotor, proposal")
+                         "quadrotor, proposal, quadrotor_proposal")
     ap.add_argument("--numeric", choices=["fp32", "mixed"], default="fp32",
                     help="numeric mode of the quadrotor workload")
     ap.add_argument("--proposal-weights", default="",
@@ -82,7 +82,7 @@ def dist_env():
     return r.rank, r.world, r.local_rank
 
 
-WORKLOADS = ("batch", "uneven", "single", "quadrotor", "proposal")
+WORKLOADS = ("batch", "uneven", "single", "quadrotor", "proposal", "quadrotor_proposal")
 
 
 def workload_for_rank(rank: int, name: str = "batch", numeric: str = "fp32"):
@@ -516,13 +516,39 @@ PROPOSAL_PLAIN_K = 4096
 PROPOSAL_H = 64
 
 
+def proposal_spec(name: str) -> dict:
+    """proposal          : configs[3] -- 128 unicycle agents x 300 steps, H 64;
+                          proposal-MPPI K 256 (128 around the prediction) vs plain K 4096
+    quadrotor_proposal : configs[4]'s third arm -- 32 quadrotors x 100 steps, H 100;
+                          proposal-MPPI K 4096 (1024 around the prediction, the network
+                          predicts 60 steps) vs plain K 65536"""
+    from mppi_metal_b200 import models
+    from mppi_metal_b200 import proposal as P
+    if name == "quadrotor_proposal":
+        return dict(agents=32, K=4096, samples=1024, plain_K=65536, H=100, T=100, net_H=60,
+                    features=P.QUADROTOR_FEATURES, label="quadrotor",
+                    make=lambda rank: models.quadrotor_batch(seed=4100 + rank, N=32, K=65536,
+                                                             H=100, T=100),
+                    train=P.train_quadrotor_proposal,
+                    data="plain MPPI K=65536, H=100, 4 seeds x 256 agents x 100 steps",
+                    desc="32 quadrotors per GPU (n=12, m=4, dt=0.01, 32 spherical obstacles)")
+    return dict(agents=PROPOSAL_AGENTS, K=PROPOSAL_K, samples=PROPOSAL_SAMPLES,
+                plain_K=PROPOSAL_PLAIN_K, H=PROPOSAL_H, T=CLOSED_LOOP_STEPS, net_H=PROPOSAL_H,
+                features=P.UNICYCLE_FEATURES, label="unicycle",
+                make=lambda rank: models.unicycle_batch(seed=4000 + rank, N=PROPOSAL_AGENTS,
+                                                        K=PROPOSAL_PLAIN_K, H=PROPOSAL_H,
+                                                        T=CLOSED_LOOP_STEPS),
+                train=P.train_unicycle_proposal,
+                data="plain MPPI K=16384, H=64, 4 seeds x 1024 agents x 300 steps",
+                desc="128 unicycle agents per GPU (16 moving obstacles, sigma U[0.2,0.8])")
+
+
 def run_proposal(args):
-    """Proposal-MPPI at K = 256 (128 samples around the network's prediction)
-    against plain MPPI at K = 4096, both on 128 unicycle agents x 300
-    closed-loop steps, H = 64.  value = control steps/s of the proposal arm;
+    """Proposal-MPPI against plain MPPI with 16x the samples, on the same
+    agents (proposal_spec).  value = control steps/s of the proposal arm;
     the plain arm's rate and both closed-loop costs ride along.  Setup (not
     timed): the network is trained on this GPU by the library's kernels on
-    ~1.2e6 (features, u*) pairs from plain MPPI at K = 16384."""
+    (features, u*) pairs from plain MPPI."""
     import torch
     from mppi_metal_b200 import dist
     R = dist.env()
@@ -533,6 +559,7 @@ def run_proposal(args):
     from mppi_metal_b200 import models
     from mppi_metal_b200 import proposal as P
     from mppi_metal_b200._lib import plugin_path
+    spec = proposal_spec(args.workload)
 
     def barrier():
         dist.barrier(R, "cuda")
@@ -545,15 +572,15 @@ def run_proposal(args):
         net = P.ProposalNet.load(args.proposal_weights)
         training = {"loaded": args.proposal_weights}
     else:
-        net, hist, pairs = P.train_unicycle_proposal()
+        net, hist, pairs = spec["train"]()
         training = {"pairs": pairs, "epochs": len(hist), "final_loss": hist[-1],
                     "train_ms_per_step": net.last_train_ms(), "batch": 8192,
-                    "data": "plain MPPI K=16384, H=64, 4 seeds x 1024 agents x 300 steps"}
+                    "data": spec["data"]}
     training["setup_s"] = round(time.time() - t_setup, 1)
 
-    w = models.unicycle_batch(seed=4000 + rank, N=PROPOSAL_AGENTS, K=PROPOSAL_PLAIN_K,
-                              H=PROPOSAL_H, T=CLOSED_LOOP_STEPS)
-    N, T = w.num_agents, w.num_steps
+    w = spec["make"](rank)
+    N, T, K, KS = w.num_agents, w.num_steps, spec["K"], spec["samples"]
+    n, m, H = w.state_dim, w.control_dim, w.horizon
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def timed_arm(b):
@@ -575,12 +602,12 @@ def run_proposal(args):
         cost = models.executed_cost(w, r["states"], r["controls"], r["terminal"])
         return max_over_ranks(sum(times)), cost, clocks.summary()
 
-    plain = P.make_backend(w)
+    plain = P.make_backend(w, spec["plain_K"])
     plain_ms, plain_cost, _ = timed_arm(plain)
     plain.close()
-    prop = P.make_backend(w, PROPOSAL_K)
-    prop.set_features(P.FEATURES_CALLABLE, P.UNICYCLE_FEATURES)
-    prop.set_proposal(net, PROPOSAL_SAMPLES)
+    prop = P.make_backend(w, K)
+    prop.set_features(P.FEATURES_CALLABLE, spec["features"])
+    prop.set_proposal(net, KS)
     prop_ms, prop_cost, clk = timed_arm(prop)
     rollout_ms, combine_ms = prop.time_passes(20)
     feat_ms, net_ms = prop.time_proposal(20)
@@ -590,25 +617,24 @@ def run_proposal(args):
     plain_value = world * N * T * args.steps / (plain_ms / 1e3)
 
     # ---- e2e: public API (DriverOptions.proposal), host buffers --------------
-    cfg = D.DriverConfig(w.state_dim, w.control_dim, w.horizon, PROPOSAL_K, w.lam,
-                         D.ControlNoiseConfig(D.CovarianceForm.kDiagonal, w.sigma, w.sigma_inv,
-                                              w.control_dim),
-                         D.ControlBounds(w.u_min, w.u_max, w.control_dim))
-    drv = D.MPPIDriver(cfg, D.DriverOptions(proposal=net, proposal_samples=PROPOSAL_SAMPLES))
+    cfg = D.DriverConfig(n, m, H, K, w.lam,
+                         D.ControlNoiseConfig(D.CovarianceForm.kDiagonal, w.sigma, w.sigma_inv, m),
+                         D.ControlBounds(w.u_min, w.u_max, m))
+    drv = D.MPPIDriver(cfg, D.DriverOptions(proposal=net, proposal_samples=KS))
     err = D.ErrorRef()
-    spec = D.ModelPluginSpec(plugin_path(w.plugin),
-                             D.CallableNames("mppi_dynamics", "mppi_stage_cost",
-                                             "mppi_terminal_cost"),
-                             D.ParamLayout(len(w.model_params), 4, w.cost_stride, 4),
-                             D.RngConfig(w.seed))
-    assert drv.initialize(spec, err), err.value
+    dspec = D.ModelPluginSpec(plugin_path(w.plugin),
+                              D.CallableNames("mppi_dynamics", "mppi_stage_cost",
+                                              "mppi_terminal_cost"),
+                              D.ParamLayout(len(w.model_params), 4, w.cost_stride, 4),
+                              D.RngConfig(w.seed))
+    assert drv.initialize(dspec, err), err.value
     assert drv.set_problem_params(D.ProblemParams(D.ByteView.of(w.model_params),
                                                   D.ByteView.of(w.cost_params[0])), err), err.value
     ap = D.BatchAgentParams(cost_params=w.cost_params_packed, cost_params_stride=w.cost_stride,
                             sigma=w.agent_sigma)
-    outs = D.BatchSimulationResults(np.zeros((T, N, 4), np.float32),
-                                    np.zeros((T, N, 2), np.float32), np.zeros((T, N), np.float32),
-                                    np.zeros((N, 4), np.float32), N, T)
+    outs = D.BatchSimulationResults(np.zeros((T, N, n), np.float32),
+                                    np.zeros((T, N, m), np.float32), np.zeros((T, N), np.float32),
+                                    np.zeros((N, n), np.float32), N, T)
     for _ in range(args.warmup):
         assert drv.reset(None, err)
         assert drv.simulate_batch(N, T, w.x0, outs, ap, err), err.value
@@ -623,14 +649,15 @@ def run_proposal(args):
     e2e_total = max_over_ranks(sum(e2e_times))
     e2e_cost = models.executed_cost(w, outs.states_out, outs.controls_out,
                                     outs.terminal_states_out)
-    h2d = (N * 4 + N * PROPOSAL_H * 2 + 4) * 4 + N * ((w.cost_stride + 15) // 16 * 16) + N * 2 * 4
-    d2h = (T * N * (4 + 2 + 1) + N * 4) * 4
+    sig_len = m if w.agent_sigma is not None else 0
+    h2d = (N * n + N * H * m + 4) * 4 + N * ((w.cost_stride + 15) // 16 * 16) + N * sig_len * 4
+    d2h = (T * N * (n + m + 1) + N * n) * 4
 
     if rank != 0:
         dist.finish(R)
         return 0
-    # proposal network forward: 2 * rows * (32*256 + 2*256*256 + 256*P) FLOPs
-    out_pad = (PROPOSAL_H * 2 + 2 + 15) // 16 * 16
+    # network forward: 2 * rows * (32*256 + 2*256*256 + 256*P) FLOPs
+    out_pad = (spec["net_H"] * m + m + 15) // 16 * 16
     mlp_flops = 2 * N * (32 * 256 + 2 * 256 * 256 + 256 * out_pad)
     peaks = {}
     try:
@@ -645,19 +672,19 @@ def run_proposal(args):
         "dtype": "fp32 rollout, bf16 network (fp32 accumulate)",
         "data": "synthetic (seeded PCG64 workload generator, mppi_metal_b200/models.py)",
         "config": {
-            "workload": (f"proposal: {N} unicycle agents per GPU (16 moving obstacles, sigma "
-                         f"U[0.2,0.8]), H={PROPOSAL_H}, {T} closed-loop steps; proposal-MPPI "
-                         f"K={PROPOSAL_K} ({PROPOSAL_SAMPLES} samples around the network's "
-                         f"prediction) against plain MPPI K={PROPOSAL_PLAIN_K}"),
-            "agents_per_gpu": N, "samples": PROPOSAL_K, "proposal_samples": PROPOSAL_SAMPLES,
-            "plain_samples": PROPOSAL_PLAIN_K, "horizon": PROPOSAL_H, "closed_loop_steps": T,
-            "network": "MLP 31->256->256->256->130, GELU, bf16 weights, fp32 accumulate",
-            "step": "one simulate_batch closed loop (300 control steps for every agent)",
+            "workload": (f"{args.workload}: {spec['desc']}, H={H}, {T} closed-loop steps; "
+                         f"proposal-MPPI K={K} ({KS} samples around the network's prediction) "
+                         f"against plain MPPI K={spec['plain_K']}"),
+            "agents_per_gpu": N, "samples": K, "proposal_samples": KS,
+            "plain_samples": spec["plain_K"], "horizon": H, "closed_loop_steps": T,
+            "network": (f"MLP {spec['features']}->256->256->256->{spec['net_H'] * m + m}, GELU, "
+                        f"bf16 weights, fp32 accumulate; predicts {spec['net_H']} steps"),
+            "step": f"one simulate_batch closed loop ({T} control steps for every agent)",
             "l2": "flushed between timed iterations (256 MiB device write)",
             "parallelism": "agent-sharded replicas, no data-path collective",
         },
-        "rollout_steps_per_s": value * PROPOSAL_K * PROPOSAL_H,
-        "plain": {"control_steps_per_s": plain_value, "samples": PROPOSAL_PLAIN_K,
+        "rollout_steps_per_s": value * K * H,
+        "plain": {"control_steps_per_s": plain_value, "samples": spec["plain_K"],
                   "ms_per_step": plain_ms / args.steps,
                   "closed_loop_cost_mean": float(plain_cost.mean())},
         "closed_loop_cost": {"mean": float(prop_cost.mean()), "agents": N,
@@ -668,15 +695,18 @@ def run_proposal(args):
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": 1e3 * e2e_total / args.steps,
                 "closed_loop_cost_mean": float(e2e_cost.mean())},
-        "gpu_launches": 4 * T * args.steps,
+        "gpu_launches": (3 * T + 1) * args.steps,
         "kernel_ms_per_pass": {"rollout": rollout_ms, "combine": combine_ms,
-                               "features": feat_ms, "network": net_ms},
-        "roofline": {"kernel": "mlp_fused_kernel (proposal network forward)", "bound": "tensor",
+                               "features_kernel": feat_ms, "network": net_ms},
+        "roofline": {"kernel": "mlp_forward_cluster_kernel (proposal network forward)",
+                     "bound": "tensor",
                      "achieved": mlp_flops / (net_ms / 1e3) / 1e12, "peak": bf16_peak,
                      "unit": "TFLOP/s", "frac": mlp_flops / (net_ms / 1e3) / 1e12 / bf16_peak,
                      "traffic": None,
-                     "note": "M = 128 rows: one CTA, latency-bound; peak = measured bf16 "
-                             "burst" + ("" if peaks.get("bf16_tflops") else " (fallback)")},
+                     "note": f"M = {N} rows: one 4-CTA cluster, latency-bound; the dominant "
+                             "kernel of the step is the rollout (issue-bound, see the batch "
+                             "workload); peak = measured bf16 burst"
+                             + ("" if peaks.get("bf16_tflops") else " (fallback)")},
         "clocks": clk,
     }
     print(json.dumps(line))
@@ -690,7 +720,7 @@ def main():
         return run_reference(args)
     if args.mode == "kernels":
         return run_kernels_only(args)
-    if args.workload == "proposal":
+    if args.workload in ("proposal", "quadrotor_proposal"):
         return run_proposal(args)
     return run_b200(args)
 

@@ -153,6 +153,8 @@ struct mppi_backend {
   mppi_b200::ModuleSpec spec;  // what `mod` was compiled from
   int num_sms = 148;
   size_t max_smem_optin = 0;
+  size_t smem_per_sm = 233472;   // shared memory of one SM
+  size_t smem_reserved = 1024;   // reserved by the system in every CTA
 
   // ---- constant device data ----
   DevBuf d_consts;  // [sigma m*m][sigma_inv m*m][u_min m][u_max m] padded
@@ -231,6 +233,14 @@ struct mppi_backend {
 
 namespace {
 
+// Dynamic shared memory one rollout CTA may use so that four fit on an SM.
+size_t rollout_dynamic_share(const mppi_backend* b, size_t static_smem, size_t budget) {
+  const size_t quarter = b->smem_per_sm / 4;
+  const size_t overhead = b->smem_reserved + static_smem;
+  const size_t share = quarter > overhead + 4096 ? quarter - overhead : 4096;
+  return std::min(share, budget);
+}
+
 // Shared memory of a rollout CTA in front of the noise staging: the nominal
 // sequence, plus the proposal's mean shift in modules compiled for one.
 size_t nominal_bytes(const mppi_backend* b) {
@@ -274,10 +284,11 @@ LaunchGeom choose_geometry(const mppi_backend* b) {
   // Four 128-thread CTAs per SM (16 warps) hide this kernel's dependency
   // latencies; staging the whole horizon is used only while it keeps that
   // residency, otherwise the noise is staged (and regenerated) in chunks that
-  // fill the same per-CTA share of shared memory.
-  const size_t per_cta = budget / 4 - 1024;
+  // fill the same per-CTA share of shared memory (the SM's shared memory /
+  // 4, less what the system reserves per CTA and the kernel's static part).
   for (int vi : order) {
     const uint32_t block = mppi_b200::kRolloutBlocks[vi];
+    const size_t per_cta = rollout_dynamic_share(b, b->mod->rollout_static_smem[vi], budget);
     const size_t fixed = nominal_bytes(b) + (size_t)block * 4;
     const size_t full = fixed + HM * block * el;
     g.variant = vi;
@@ -809,6 +820,8 @@ int mppi_backend_initialize(mppi_backend* b, const mppi_backend_plugin* plugin,
   }
   b->num_sms = prop.multiProcessorCount;
   b->max_smem_optin = prop.sharedMemPerBlockOptin;
+  b->smem_per_sm = prop.sharedMemPerMultiprocessor;
+  b->smem_reserved = prop.reservedSharedMemPerBlock;
 
   b->n = cfg->state_dim;
   b->m = cfg->control_dim;

@@ -214,13 +214,14 @@ __device__ __forceinline__ void copy_words(uint32_t* dst, const uint8_t* src, in
 
 // Proposal samples replace the plain draw eps = sigma n by
 // (mu - u_nom) + exp(s) n on the same standard normals n (rounded like the
-// plain draw in the FP16 modes).
+// plain draw in the FP16 modes).  The branch is uniform over a warp (the
+// proposal samples are a prefix of k).
 #if MPPI_PROPOSAL
 #define MPPI_PROPOSAL_EPS()                                                       \
   do {                                                                            \
     if (k < pcount) {                                                             \
       _Pragma("unroll") for (int d_ = 0; d_ < kM; ++d_) eps[d_] =                 \
-          from_stage(to_stage(fmaf(ps[d_], n[d_], sh_s[t * kM + d_])));            \
+          from_stage(to_stage(fmaf(ps_s[d_], n[d_], sh_s[t * kM + d_])));          \
     }                                                                             \
   } while (0)
 #else
@@ -271,19 +272,17 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
 
   for (uint32_t i = tid; i < HM; i += BLOCK) un_s[i] = un_g[i];
 #if MPPI_PROPOSAL
-  // samples k < pcount draw around the network's predicted sequence
+  // samples k < pcount draw around the network's predicted sequence; the
+  // shift and the scales live in shared memory, not in registers, so the
+  // rollout's register budget stays the plain kernel's
+  __shared__ float ps_s[kM];
   const uint32_t pcount = a.prop_out ? a.prop_count : 0u;
-  float ps[kM];
   if (pcount) {
     const float* po = a.prop_out + (size_t)agent * a.prop_stride;
     for (uint32_t i = tid; i < HM; i += BLOCK)
       sh_s[i] = i < a.prop_ls_offset ? po[i] - un_g[i] : 0.0f;
-#pragma unroll
-    for (int d = 0; d < kM; ++d)
-      ps[d] = expf(clampf(po[a.prop_ls_offset + d], a.prop_ls_min, a.prop_ls_max));
-  } else {
-#pragma unroll
-    for (int d = 0; d < kM; ++d) ps[d] = 1.0f;
+    if (tid < (uint32_t)kM)
+      ps_s[tid] = expf(clampf(po[a.prop_ls_offset + tid], a.prop_ls_min, a.prop_ls_max));
   }
 #endif
   const uint8_t* mp_g = a.model_params + a.model_stride * agent;

@@ -277,6 +277,16 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->noise, mod->library, "mppi_noise");
   if (ce == cudaSuccess && !spec.features.empty())
     ce = cudaLibraryGetKernel(&mod->features, mod->library, "mppi_features");
+  for (int i = 0; i < 3 && ce == cudaSuccess; ++i) {
+    cudaFuncAttributes fa{};
+    ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout[i]));
+    mod->rollout_static_smem[i] = fa.sharedSizeBytes;
+  }
+  if (ce == cudaSuccess) {
+    cudaFuncAttributes fa{};
+    ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout_work));
+    mod->work_static_smem = fa.sharedSizeBytes;
+  }
   if (ce != cudaSuccess) {
     *error = std::string("Required library kernel missing from the module: ") +
              cudaGetErrorString(ce);

@@ -45,6 +45,10 @@ struct KernelModule {
   cudaKernel_t weights = nullptr;
   cudaKernel_t noise = nullptr;
   cudaKernel_t features = nullptr;  // only when ModuleSpec::features is set
+  // static shared memory of the rollout kernels (their dynamic share is
+  // sized so that this plus the dynamic part keeps the target residency)
+  size_t rollout_static_smem[3] = {0, 0, 0};
+  size_t work_static_smem = 0;
   std::string build_log;  // NVRTC log of the compile (warnings, ptxas info)
 };
 

@@ -252,19 +252,42 @@ def train_unicycle_proposal(seeds=(100, 101, 102, 103), agents: int = 1024, step
     return net, hist, X.shape[0]
 
 
+def train_quadrotor_proposal(seeds=(500, 501, 502, 503), agents: int = 256, steps: int = 100,
+                             sample_count: int = 65536, horizon: int = 100,
+                             net_horizon: int = 60, epochs: int = 30, batch: int = 8192,
+                             seed: int = 0):
+    """The quadrotor recipe: (features, first net_horizon steps of u*) pairs
+    from plain MPPI at K = 65536, H = 100 (4 seeds x 256 agents x 100 steps
+    = 102,400 pairs); the network predicts 60 of the 100 steps (H m + m =
+    244 outputs), the later steps keep the warm start as their mean."""
+    X, Y = collect_pairs_for(
+        lambda s: models.quadrotor_batch(seed=s, N=agents, K=sample_count, H=horizon, T=steps),
+        seeds, QUADROTOR_FEATURES, target_steps=net_horizon)
+    net, hist = train(X, Y, net_horizon, 4, epochs=epochs, batch=batch, seed=seed)
+    return net, hist, X.shape[0]
+
+
 if __name__ == "__main__":
     import argparse
     import json
     import time
-    ap = argparse.ArgumentParser(description="Train the unicycle proposal network on the GPU.")
+    ap = argparse.ArgumentParser(description="Train a proposal network on the GPU.")
     ap.add_argument("--out", required=True, help="weights file (.npz)")
-    ap.add_argument("--seeds", default="100,101,102,103")
-    ap.add_argument("--agents", type=int, default=1024)
-    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--model", choices=["unicycle", "quadrotor"], default="unicycle")
+    ap.add_argument("--seeds", default="")
+    ap.add_argument("--agents", type=int, default=0)
+    ap.add_argument("--epochs", type=int, default=0)
     a = ap.parse_args()
     t0 = time.time()
-    net, hist, pairs = train_unicycle_proposal(tuple(int(s) for s in a.seeds.split(",")),
-                                               agents=a.agents, epochs=a.epochs)
+    kw = {}
+    if a.seeds:
+        kw["seeds"] = tuple(int(s) for s in a.seeds.split(","))
+    if a.agents:
+        kw["agents"] = a.agents
+    if a.epochs:
+        kw["epochs"] = a.epochs
+    fn = train_unicycle_proposal if a.model == "unicycle" else train_quadrotor_proposal
+    net, hist, pairs = fn(**kw)
     net.save(a.out)
-    print(json.dumps({"pairs": pairs, "epochs": a.epochs, "final_loss": hist[-1],
+    print(json.dumps({"pairs": pairs, "epochs": len(hist), "final_loss": hist[-1],
                       "seconds": round(time.time() - t0, 1), "out": a.out}))

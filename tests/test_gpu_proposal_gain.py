@@ -41,3 +41,23 @@ def test_proposal_gains_over_plain_mppi(trained):
     prop_256 = P.closed_loop(w, trained, 128, sample_count=256)["cost"].mean()
     assert prop_256 <= 0.97 * plain_256, (prop_256, plain_256)
     assert prop_256 <= 1.02 * plain_4096, (prop_256, plain_4096)
+
+
+@pytest.fixture(scope="module")
+def trained_quadrotor():
+    from mppi_metal_b200 import proposal as P
+    net, hist, pairs = P.train_quadrotor_proposal(seeds=(510, 511), agents=128,
+                                                  sample_count=16384, epochs=30)
+    assert pairs == 2 * 128 * 100
+    return net
+
+
+def test_quadrotor_proposal_gains_over_plain_mppi(trained_quadrotor):
+    """configs[4]'s proposal arm: K = 4096 with 1024 samples around a
+    60-step prediction, against plain MPPI at the same K on held-out
+    quadrotors (other waypoints and obstacle fields)."""
+    from mppi_metal_b200 import proposal as P
+    w = models.quadrotor_batch(seed=610, N=32, K=65536, H=100, T=100)
+    plain_4096 = P.closed_loop(w, sample_count=4096)["cost"].mean()
+    prop_4096 = P.closed_loop(w, trained_quadrotor, 1024, sample_count=4096)["cost"].mean()
+    assert prop_4096 <= 0.985 * plain_4096, (prop_4096, plain_4096)

@@ -213,3 +213,50 @@ def test_fused_next_step_features_match_the_feature_kernel():
         x, un = r["x"], r["u_nom"]
     assert np.array_equal(whole["states"], np.stack(states))
     assert np.array_equal(whole["terminal"], x)
+
+
+def test_quadrotor_features_match_oracle():
+    w = models.quadrotor_batch(seed=5, N=16, K=256, H=20, T=2)
+    b = _batch_backend(w)
+    b.set_features(FEATURES, 29)
+    rng = np.random.default_rng(1)
+    R = 16 * 4
+    st = np.zeros((R, 12), np.float32)
+    st[:, :3] = rng.uniform(-5, 5, (R, 3))
+    st[:, 3:] = rng.normal(size=(R, 9)) * 0.5
+    f = b.features(st, agents_mod=16)
+    ref = np.stack([mo.quadrotor_features(st[r], w.cost_params[r % 16]) for r in range(R)])
+    d = np.abs(f - ref).max(axis=1)
+    assert f.shape == (R, 29)
+    assert np.mean(d <= 1e-5) >= 0.99, np.sort(d)[-5:]
+    assert np.abs(f[:, :13] - ref[:, :13]).max() <= 1e-5
+
+
+def test_short_network_horizon_shifts_only_its_steps(oracle):
+    """A network predicting fewer steps than the horizon: proposal samples
+    get the mean shift on those steps only (checked against the oracle on
+    the device's noise layout)."""
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.unicycle_batch(seed=6, N=1, K=512, H=40, T=1)
+    b = backend_for(w)
+    b.set_features(FEATURES, 31)
+    shape = mo.Shape(31, 16, 2)
+    net = ProposalNet(31, 16, 2, max_batch=128, seed=1)
+    net.set_params(mo.init_params(shape, 8))
+    b.set_proposal(net, 256)
+    x0 = w.x0[0].copy()
+    u_nom = (np.random.default_rng(2).normal(size=80) * 0.3).astype(np.float32)
+    u_out, _ = b.dispatch_rollout(3, x0, u_nom)
+    costs = b.last_costs()[0]
+    feats = b.features(x0[None, :], agents_mod=1)
+    out = net.forward(torch.from_numpy(np.ascontiguousarray(feats)).cuda()).cpu().numpy()[0]
+    ps = np.exp(np.clip(out[32:34].astype(np.float32), -3.0, 1.0)).astype(np.float64)
+    sh = np.zeros((40, 2))
+    sh[:16] = out[:32].astype(np.float64).reshape(16, 2) - u_nom[:32].astype(np.float64).reshape(16, 2)
+    p = oracle_problem(w)
+    eps = np.zeros((512, 40, 2))
+    for k in range(512):
+        n, e = oracle.noise(p, 3, w.seed, k)
+        eps[k] = sh + ps * n if k < 256 else e
+    ref = oracle.rollout_eps(p, x0, u_nom, eps)
+    assert rel_err(costs, ref) <= 1e-5
