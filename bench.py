@@ -517,11 +517,11 @@ PROPOSAL_H = 64
 
 
 def proposal_spec(name: str) -> dict:
-    """proposal          : configs[3] -- 128 unicycle agents x 300 steps, H 64;
-                          proposal-MPPI K 256 (128 around the prediction) vs plain K 4096
-    quadrotor_proposal : configs[4]'s third arm -- 32 quadrotors x 100 steps, H 100;
-                          proposal-MPPI K 4096 (1024 around the prediction, the network
-                          predicts 60 steps) vs plain K 65536"""
+    """proposal          : 128 unicycle agents x 300 steps, H 64; proposal-MPPI
+                          K 256 (128 around the prediction) vs plain K 4096
+    quadrotor_proposal : 32 quadrotors x 100 steps, H 100; proposal-MPPI K 4096
+                          (1024 around the prediction, the network predicts 60
+                          steps) vs plain K 65536"""
     from mppi_metal_b200 import models
     from mppi_metal_b200 import proposal as P
     if name == "quadrotor_proposal":

@@ -53,8 +53,8 @@ def trained_quadrotor():
 
 
 def test_quadrotor_proposal_gains_over_plain_mppi(trained_quadrotor):
-    """configs[4]'s proposal arm: K = 4096 with 1024 samples around a
-    60-step prediction, against plain MPPI at the same K on held-out
+    """The large-rollout quadrotor problem: K = 4096 with 1024 samples around
+    a 60-step prediction, against plain MPPI at the same K on held-out
     quadrotors (other waypoints and obstacle fields)."""
     from mppi_metal_b200 import proposal as P
     w = models.quadrotor_batch(seed=610, N=32, K=65536, H=100, T=100)
