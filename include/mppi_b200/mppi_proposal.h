@@ -26,9 +26,15 @@
  * >= H*m + m are padding and stay zero.  Row n of W_l maps the layer's
  * input to its output n (y = W x + b).
  *
- * All x / target / out pointers are DEVICE pointers; entry points run on
- * the proposal's own stream and return when their results are ready.
- * Return codes are MPPI_OK or an MPPI_ERR_* of mppi_backend.h.
+ * All x / target / out / index pointers are DEVICE pointers; entry points
+ * run on the proposal's own stream and return when their results are ready
+ * (train_step without loss_out returns once its kernels are queued).  Every
+ * index must be below the row count of x and target.  Return codes are
+ * MPPI_OK or an MPPI_ERR_* of mppi_backend.h.
+ *
+ * Sharing: several backends may run one network at the same time (its
+ * weights are only read there), but training it while a backend that has
+ * it attached is running races with that backend's reads.
  */
 #ifndef MPPI_B200_PROPOSAL_H
 #define MPPI_B200_PROPOSAL_H
