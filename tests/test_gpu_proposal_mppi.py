@@ -260,3 +260,70 @@ def test_short_network_horizon_shifts_only_its_steps(oracle):
         eps[k] = sh + ps * n if k < 256 else e
     ref = oracle.rollout_eps(p, x0, u_nom, eps)
     assert rel_err(costs, ref) <= 1e-5
+
+
+def test_proposal_with_uneven_shapes_matches_uniform():
+    """A proposal attached to an uneven batch whose agents all have the same
+    K and H (the persistent work-list kernel) gives the uniform batch's
+    bits; with truly uneven shapes it stays deterministic across the
+    autotuner's choices."""
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.unicycle_batch(seed=11, N=12, K=384, H=64, T=3)
+    net = ProposalNet(31, 64, 2, max_batch=256, seed=5)
+
+    def run(ks=None, hs=None):
+        b = backend_for(w, bind=True)
+        b.set_features(FEATURES, 31)
+        b.set_proposal(net, 128)
+        b.prepare(12, 3, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+                  sigma=w.agent_sigma, sample_counts=ks, horizons=hs)
+        b.run(0)
+        return b, b.fetch()
+
+    b_u, uniform = run()
+    if b_u.launch_info()["block"] != 128:
+        pytest.skip("uniform path chose another CTA size for this shape")
+    _, ragged = run(np.full(12, 384, np.uint32), np.full(12, 64, np.uint32))
+    for k in ("states", "controls", "costs", "terminal"):
+        assert np.array_equal(uniform[k], ragged[k]), k
+    ks = np.array([128, 384, 200, 256] * 3, np.uint32)
+    hs = np.array([64, 32, 48, 16] * 3, np.uint32)
+    _, r1 = run(ks, hs)
+    _, r2 = run(ks, hs)
+    assert np.array_equal(r1["states"], r2["states"])
+    assert np.all(np.isfinite(r1["states"]))
+
+
+def test_proposal_in_mixed_numeric_mode_matches_oracle(oracle):
+    """FP16 noise mode: the proposal draw (mu - u_nom) + exp(s) n is rounded
+    to FP16 like the plain draw, on the fast-transcendental normals."""
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.unicycle_batch(seed=12, N=1, K=512, H=32, T=1)
+    w.numeric_mode = 2
+    b = backend_for(w)
+    b.set_features(FEATURES, 31)
+    shape = mo.Shape(31, 32, 2)
+    net = ProposalNet(31, 32, 2, max_batch=128, seed=6)
+    net.set_params(mo.init_params(shape, 9))
+    b.set_proposal(net, 256)
+    x0 = w.x0[0].copy()
+    u_nom = (np.random.default_rng(3).normal(size=64) * 0.3).astype(np.float32)
+    u_out, _ = b.dispatch_rollout(4, x0, u_nom)
+    costs = b.last_costs()[0]
+    feats = b.features(x0[None, :], agents_mod=1)
+    out = net.forward(torch.from_numpy(np.ascontiguousarray(feats)).cuda()).cpu().numpy()[0]
+    ps = np.exp(np.clip(out[64:66].astype(np.float32), -3.0, 1.0)).astype(np.float32)
+    sh = (out[:64] - u_nom).astype(np.float32).reshape(32, 2)
+    p = oracle_problem(w)
+    # the device's own normals of this step (fast Box-Muller) and, for the
+    # plain samples, its own FP16-rounded draws
+    nrm, plain_eps = b.sample_noise(4, 0, 0, 512)
+    eps = np.zeros((512, 32, 2))
+    for k in range(512):
+        if k < 256:  # fmaf(scale, n, shift) in FP32, then rounded to FP16
+            e = (ps.astype(np.float64) * nrm[k] + sh.astype(np.float64)).astype(np.float32)
+            eps[k] = e.astype(np.float16).astype(np.float64)
+        else:
+            eps[k] = plain_eps[k]
+    ref = oracle.rollout_eps(p, x0, u_nom, eps)
+    assert rel_err(costs, ref) <= 1e-5
