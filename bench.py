@@ -492,17 +492,21 @@ def run_kernels_only(args):
                           "train_loss": loss, "train_ms": net.last_train_ms()}))
         return 0
     from mppi_metal_b200.backend import Backend
-    w = workload_for_rank(0)
+    w = workload_for_rank(0, args.workload, args.numeric)
+    ks, hs = agent_shapes(w)
     b = Backend(w.plugin, w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam, w.sigma,
-                w.u_min, w.u_max, sigma_inv=w.sigma_inv, control_cost=w.control_cost,
-                model_params_size=len(w.model_params), cost_params_size=w.cost_stride,
-                seed=w.seed)
+                w.u_min, w.u_max, sigma_inv=w.sigma_inv, cov_full=w.cov_full,
+                control_cost=w.control_cost, model_params_size=len(w.model_params),
+                cost_params_size=w.cost_stride, seed=w.seed, numeric_mode=w.numeric_mode)
     b.bind_params(w.model_params, w.cost_params[0])
     b.prepare(w.num_agents, 1, w.x0, cost_params=w.cost_params_packed,
-              cost_stride=w.cost_stride, sigma=w.agent_sigma)
+              cost_stride=w.cost_stride, sigma=w.agent_sigma, sample_counts=ks, horizons=hs)
+    if ks is not None:
+        b.run(0)  # the autotuner picks the persistent-launch geometry on the first run
     r, c = b.time_passes(args.iters)
-    print(json.dumps({"mode": "kernels", "rollout_ms": r, "combine_ms": c,
-                      "geometry": b.launch_info()}))
+    print(json.dumps({"mode": "kernels", "workload": args.workload, "rollout_ms": r,
+                      "combine_ms": c, "geometry": b.launch_info(),
+                      "tuning": b.tuning_info() or None}))
     return 0
 
 

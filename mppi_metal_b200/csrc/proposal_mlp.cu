@@ -423,16 +423,36 @@ __device__ __forceinline__ void cluster_slice(uint32_t N, uint32_t c, uint32_t& 
   ncols = 16 * (q + (c < rem ? 1u : 0u));
 }
 
-// Activations ping-pong between two A tiles: layer g reads A[g % 2] and its
-// epilogue writes A[(g + 1) % 2] in all four CTAs.  A CTA last read that
-// tile in layer g - 1, which it finished before the cluster barrier that
-// ends layer g - 1, so no write can reach a tile still being read.
+// Remote asynchronous store: 16 bytes into another CTA's shared memory,
+// counted on that CTA's mbarrier (complete_tx) -- the async proxy, like a
+// bulk copy, so the receiving tensor core may read the data once the
+// barrier's phase completes, with no proxy fence or cluster barrier.
+__device__ __forceinline__ void st_async_v4(uint32_t addr, uint4 v, uint32_t mbar) {
+  asm volatile(
+      "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, "
+      "[%5];" ::"r"(addr),
+      "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w), "r"(mbar)
+      : "memory");
+}
+
+// Activations ping-pong between two A tiles, each with its own "full"
+// mbarrier: layer g reads A[g % 2]; its epilogue stores the CTA's column
+// slice of the next activations into A[(g + 1) % 2] of all four CTAs with
+// st.async, completing 64 KB per layer on each receiver's full barrier,
+// which the receiver arms (arrive.expect_tx) and waits on before its next
+// MMA.  Reuse is safe by causality: a CTA writes A[(g + 1) % 2] of a peer
+// only after its own MMA g, which needed that peer's slice of layer g's
+// input, which the peer sent after its MMA g - 1 -- the last reader of the
+// buffer being overwritten -- had completed.  Only the start (every
+// barrier initialised before any remote arrival) and the end (no CTA
+// leaves while a peer may still write into it) synchronise the cluster.
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
     mlp_forward_cluster_kernel(const FusedArgs a) {
   extern __shared__ __align__(128) uint8_t smem[];
   bf16* as0 = reinterpret_cast<bf16*>(smem);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * kSmemA + kCSmemW);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+  // bars: [0] weights, [1] MMA, [2..3] full A[0] / A[1]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 4);
   volatile uint32_t* abort_s = tslot + 1;
   float* bias_s = reinterpret_cast<float*>(smem + 2 * kSmemA + kCSmemW + kSmemBar);  // [4][256]
 
@@ -447,11 +467,12 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
   const uint32_t row = (blockIdx.x / kCluster) * kTile + r;
   const bool valid = row < a.rows;
   const uint32_t bar_w = tc::smem_addr(&bars[0]), bar_m = tc::smem_addr(&bars[1]);
+  const uint32_t bar_full0 = tc::smem_addr(&bars[2]);
   const uint32_t a_s0 = tc::smem_addr(as0), w_s = a_s0 + 2 * kSmemA;
+  constexpr uint32_t kTileBytes = kTile * kHid * 2;  // one exchanged activation tile
 
   if (tid == 0) {
-    tc::mbar_init(bar_w, 1);
-    tc::mbar_init(bar_m, 1);
+    for (uint32_t i = 0; i < 4; ++i) tc::mbar_init(bar_w + 8 * i, 1);
     *abort_s = 0;
     tc::mbar_init_fence();
   }
@@ -464,10 +485,10 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
   tc::fence_after_sync();
   const uint32_t tmem = *tslot;
   const uint32_t t_row = tmem + ((quarter * 32u) << 16);
-  cluster_sync_all();  // every CTA of the cluster is running before any DSMEM write
+  cluster_sync_all();  // every CTA's barriers exist before any remote arrival
 
   bool w_pending = false;
-  uint32_t ph_w = 0, ph_m = 0;
+  uint32_t ph_w = 0, ph_m = 0, ph_f[2] = {0, 0};
   {
     uint32_t c0, nc;
     cluster_slice(kHid, crank, c0, nc);
@@ -476,7 +497,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
       w_pending = true;
     }
   }
-  // input rows -> A[0] (every CTA stages the whole tile)
+  // input rows -> A[0] (every CTA stages the whole tile itself)
 #pragma unroll
   for (uint32_t j = grp; j < kIn / 16; j += kGroups) {
     float v[16];
@@ -492,14 +513,27 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
     const uint32_t K = g == 0 ? kIn : kHid, N = g == 3 ? a.out_pad : kHid;
     uint32_t col0, nc;
     cluster_slice(N, crank, col0, nc);
-    const uint32_t a_in = a_s0 + (g & 1u) * kSmemA;
-    if (tid == 0 && w_pending) {
-      if (tc::mbar_wait(bar_w, ph_w)) {
-        w_pending = false;
-        ph_w ^= 1u;
-      } else {
-        atomicOr(a.err, 1);
-        *abort_s = 1;
+    const uint32_t buf = g & 1u;
+    const uint32_t a_in = a_s0 + buf * kSmemA;
+    if (tid == 0) {
+      // weights of this layer, then (past layer 0) the exchanged input tile
+      if (w_pending) {
+        if (tc::mbar_wait(bar_w, ph_w)) {
+          w_pending = false;
+          ph_w ^= 1u;
+        } else {
+          atomicOr(a.err, 1);
+          *abort_s = 1;
+        }
+      }
+      if (g > 0) {
+        const uint32_t full = bar_full0 + 8 * buf;
+        tc::mbar_expect_tx(full, kTileBytes);
+        if (!tc::mbar_wait(full, ph_f[buf])) {
+          atomicOr(a.err, 8);
+          *abort_s = 1;
+        }
+        ph_f[buf] ^= 1u;
       }
     }
     tc::fence_async_shared();
@@ -507,13 +541,12 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
     __syncthreads();
     const bool run = !*abort_s && nc > 0;
     if (run && tid == 0) {
-      tc::fence_async_shared();
       tc::fence_after_sync();
       const uint32_t idesc = tc::idesc_bf16(kTile, nc);
       const uint32_t sbo = K * 16;
-      for (uint32_t s = 0; s < K / 16; ++s)
-        tc::mma_bf16(tmem, tc::sdesc(a_in + s * 256, 128, sbo), tc::sdesc(w_s + s * 256, 128, sbo),
-                     idesc, s > 0 ? 1u : 0u);
+      for (uint32_t s2 = 0; s2 < K / 16; ++s2)
+        tc::mma_bf16(tmem, tc::sdesc(a_in + s2 * 256, 128, sbo),
+                     tc::sdesc(w_s + s2 * 256, 128, sbo), idesc, s2 > 0 ? 1u : 0u);
       tc::mma_commit(bar_m);
     }
     bool done = true;
@@ -540,9 +573,11 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
       }
     }
     if (ok && g < 3) {
-      // h = GELU(acc + b) for this CTA's columns, into A[(g + 1) % 2] of all CTAs
+      // h = GELU(acc + b) for this CTA's columns -> A[(g + 1) % 2] of every CTA
       const float* bias = bias_s + g * kHid + col0;
-      const uint32_t a_out = a_s0 + ((g + 1) & 1u) * kSmemA;
+      const uint32_t nbuf = (g + 1) & 1u;
+      const uint32_t off = a_s0 + nbuf * kSmemA;
+      const uint32_t full = bar_full0 + 8 * nbuf;
       for (uint32_t j = grp; j < nc / 16; j += kGroups) {
         float v[16];
         tc::tmem_ld16(t_row + 16 * j, v);
@@ -552,12 +587,12 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
                                     pack2(v[6], v[7]));
         const uint4 hi = make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]),
                                     pack2(v[14], v[15]));
-        const uint32_t off = a_out + 2 * canon(r, col0 + 16 * j, kHid);
+        const uint32_t dst = off + 2 * canon(r, col0 + 16 * j, kHid);
 #pragma unroll
         for (uint32_t q = 0; q < kCluster; ++q) {
-          const uint32_t dst = map_to_rank(off, q);
-          st_cluster_v4(dst, lo);
-          st_cluster_v4(dst + 128, hi);
+          const uint32_t rd = map_to_rank(dst, q), rb = map_to_rank(full, q);
+          st_async_v4(rd, lo, rb);
+          st_async_v4(rd + 128, hi, rb);
         }
       }
     } else if (ok) {
@@ -573,14 +608,11 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
         }
       }
     }
-    fence_async_cluster();
-    tc::fence_before_sync();
-    cluster_sync_all();
   }
 
   if (tid == 0 && w_pending && !tc::mbar_wait(bar_w, ph_w)) atomicOr(a.err, 4);
   tc::fence_before_sync();
-  __syncthreads();
+  cluster_sync_all();  // no CTA leaves while a peer may still store into it
   if (warp == 0) {
     tc::fence_after_sync();
     tc::tmem_dealloc(tmem, kCTmemCols);
