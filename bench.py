@@ -43,15 +43,20 @@ HORIZON = 50
 CLOSED_LOOP_STEPS = 300
 L2_FLUSH_BYTES = 256 << 20
 
-# Rollout-kernel instruction count per rollout-step (warp-level instructions
-# issued per sample-timestep / 32 lanes), from an ncu capture of the same
-# kernel build: profiles/rollout_unicycle_batch.txt.  Used only to express
-# the live-timed kernel against the SM issue-rate roofline.
-ROLLOUT_WARP_INST_PER_ROLLOUT_STEP = 732651532 / 52428800  # 13.97
-
-
-# DRAM bytes (read + write) per rollout launch of the same capture.
-ROLLOUT_DRAM_BYTES_PER_LAUNCH = 240128
+# Rollout-kernel instructions per rollout-step (warp-level instructions issued
+# per sample-timestep, i.e. / 32 lanes) and DRAM bytes (read + write) per
+# launch, from ncu captures of the same kernel builds (profiles/
+# rollout_kernels_all_workloads.txt): smsp__inst_executed.sum / rollout-steps
+# of the launch.  Used only to express the live-timed kernel against the SM
+# issue-rate roofline.
+ROLLOUT_COUNTERS = {
+    # workload: (warp-inst per rollout-step, DRAM bytes per launch)
+    "batch": (733569036 / 52428800, 238592),          # 13.99
+    "uneven": (205879094 / 16410677, 119296),         # 12.55
+    "single": (330776 / 30720, 41216),                # 10.77
+    "quadrotor/fp32": (8313199985 / 209715200, 328704),   # 39.64
+    "quadrotor/mixed": (7115466818 / 209715200, 135936),  # 33.93
+}
 
 
 def parse():
@@ -433,19 +438,22 @@ def run_b200(args):
 
     rollout_units = rollout_steps_per_control_step(w)  # rollout-steps per rollout launch
     kname = "mppi_rollout_work_b128" if ks is not None else "mppi_rollout_b%d" % geom["block"]
+    key = args.workload + ("/" + args.numeric if args.workload == "quadrotor" else "")
+    inst, dram = ROLLOUT_COUNTERS.get(key, (None, None))
     roof = {"kernel": kname, "bound": "issue",
             "launch_ms": rollout_ms, "combine_launch_ms": combine_ms,
             "rollout_steps_per_launch": rollout_units,
-            "traffic": ROLLOUT_DRAM_BYTES_PER_LAUNCH, "unit": "Gwarp-inst/s",
+            "traffic": dram, "unit": "Gwarp-inst/s",
             "note": "issue-bound kernel (no HBM or tensor-core bound applies): "
                     "achieved = ncu-counted warp-instructions per rollout-step x "
                     "rollout-steps per launch / live CUDA-event launch time"}
     clk = clocks.summary()
-    if ROLLOUT_WARP_INST_PER_ROLLOUT_STEP is not None and args.workload == "batch":
-        achieved = ROLLOUT_WARP_INST_PER_ROLLOUT_STEP * rollout_units / (rollout_ms / 1e3) / 1e9
+    if inst is not None:
+        achieved = inst * rollout_units / (rollout_ms / 1e3) / 1e9
         mhz = clk.get("sm_mhz") or 1965.0
         peak = 148 * 4 * mhz * 1e6 / 1e9
         roof.update({"achieved": achieved, "peak": peak, "frac": achieved / peak,
+                     "warp_inst_per_rollout_step": inst,
                      "peak_basis": f"148 SMs x 4 warp-inst/clk x {mhz:.0f} MHz (sampled)"})
     line = {
         "metric": METRIC, "value": value, "unit": "rollout-steps/s", "n_gpus": world,
