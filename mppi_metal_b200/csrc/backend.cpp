@@ -205,9 +205,14 @@ struct mppi_backend {
   // ---- closed-loop graph cache ----
   cudaGraphExec_t graph = nullptr;
   std::string graph_key;
+  // one control step (dispatch_rollout): uploads, kernels, download
+  cudaGraphExec_t step_graph = nullptr;
+  std::string step_key;
+  std::string shape_key;  // shape of the last ensure_shape (uniform batches)
 
   ~mppi_backend() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (step_graph) cudaGraphExecDestroy(step_graph);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -316,6 +321,13 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
                  char* err, size_t err_len) {
   bool grew = false;
   CK(cudaStreamSynchronize(b->stream));  // buffers below may be in use
+  // the same uniform shape as the previous call (a control loop of steps):
+  // buffers and geometry stand
+  char key[160];
+  snprintf(key, sizeof(key), "%u/%u/%d%d%d%d/%d/%p/%u/%p", N, T, ws, wc, wk, wt, b->record_ustar,
+           (const void*)b->proposal, b->prop_samples, (const void*)b->mod.get());
+  if (!b->ragged && b->N == N && b->T == T && b->shape_key == key) return MPPI_OK;
+  b->shape_key.clear();
   b->N = N;
   b->T = T;
   b->geom = choose_geometry(b);
@@ -362,6 +374,7 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
                             : (const void*)b->mod->rollout[b->geom.variant];
   if (b->geom.smem > 48 * 1024)
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem));
+  if (!b->ragged) b->shape_key = key;
   return MPPI_OK;
 }
 
@@ -625,12 +638,11 @@ int check_init(mppi_backend* b, char* err, size_t err_len) {
   return MPPI_OK;
 }
 
-// Uploads [step_base][x][u_nom] (and blob overrides) with one pinned copy each.
-int upload_state(mppi_backend* b, uint64_t start_step, const float* x, const float* u_nom,
-                 const void* mp_ovr, size_t mp_bytes, const void* cp_ovr, size_t cp_bytes,
-                 char* err, size_t err_len) {
-  // the pinned staging buffer may still feed an earlier asynchronous copy
-  CK(cudaStreamSynchronize(b->stream));
+// Stages [step_base][x][u_nom] (and blob overrides) in the pinned upload
+// buffer; issue_upload then copies them with one transfer each.  The
+// caller has synchronised the stream (the buffer may still feed a copy).
+void stage_upload(mppi_backend* b, uint64_t start_step, const float* x, const float* u_nom,
+                  const void* mp_ovr, size_t mp_bytes, const void* cp_ovr, size_t cp_bytes) {
   float* up = b->h_up.as<float>();
   const size_t nx = (size_t)b->N * b->n, nu = (size_t)b->N * b->HM();
   uint32_t sb = (uint32_t)start_step;
@@ -640,23 +652,45 @@ int upload_state(mppi_backend* b, uint64_t start_step, const float* x, const flo
     memcpy(up + b->off_unom(), u_nom, nu * 4);
   else
     memset(up + b->off_unom(), 0, nu * 4);
-  CK(cudaMemcpyAsync(b->io(), up, b->off_uout() * 4, cudaMemcpyHostToDevice, b->stream));
   uint8_t* tail = reinterpret_cast<uint8_t*>(up + b->off_uout());
   if (mp_ovr && mp_bytes) {
-    CK(b->d_mp_ovr.ensure(pad16(b->mp_size)));
     memset(tail, 0, pad16(b->mp_size));
     memcpy(tail, mp_ovr, mp_bytes);
-    CK(cudaMemcpyAsync(b->d_mp_ovr.p, tail, pad16(b->mp_size), cudaMemcpyHostToDevice,
-                       b->stream));
     tail += pad16(b->mp_size);
   }
   if (cp_ovr && cp_bytes) {
-    CK(b->d_cp_ovr.ensure(pad16(b->cp_size)));
     memset(tail, 0, pad16(b->cp_size));
     memcpy(tail, cp_ovr, cp_bytes);
-    CK(cudaMemcpyAsync(b->d_cp_ovr.p, tail, pad16(b->cp_size), cudaMemcpyHostToDevice,
-                       b->stream));
   }
+}
+
+cudaError_t issue_upload(mppi_backend* b, bool mp_ovr, bool cp_ovr) {
+  float* up = b->h_up.as<float>();
+  cudaError_t e =
+      cudaMemcpyAsync(b->io(), up, b->off_uout() * 4, cudaMemcpyHostToDevice, b->stream);
+  uint8_t* tail = reinterpret_cast<uint8_t*>(up + b->off_uout());
+  if (e == cudaSuccess && mp_ovr) {
+    e = cudaMemcpyAsync(b->d_mp_ovr.p, tail, pad16(b->mp_size), cudaMemcpyHostToDevice,
+                        b->stream);
+    tail += pad16(b->mp_size);
+  }
+  if (e == cudaSuccess && cp_ovr)
+    e = cudaMemcpyAsync(b->d_cp_ovr.p, tail, pad16(b->cp_size), cudaMemcpyHostToDevice,
+                        b->stream);
+  return e;
+}
+
+// Uploads [step_base][x][u_nom] (and blob overrides) with one pinned copy each.
+int upload_state(mppi_backend* b, uint64_t start_step, const float* x, const float* u_nom,
+                 const void* mp_ovr, size_t mp_bytes, const void* cp_ovr, size_t cp_bytes,
+                 char* err, size_t err_len) {
+  // the pinned staging buffer may still feed an earlier asynchronous copy
+  CK(cudaStreamSynchronize(b->stream));
+  const bool mo = mp_ovr && mp_bytes, co = cp_ovr && cp_bytes;
+  if (mo) CK(b->d_mp_ovr.ensure(pad16(b->mp_size)));
+  if (co) CK(b->d_cp_ovr.ensure(pad16(b->cp_size)));
+  stage_upload(b, start_step, x, u_nom, mp_ovr, mp_bytes, cp_ovr, cp_bytes);
+  CK(issue_upload(b, mo, co));
   return MPPI_OK;
 }
 
@@ -944,14 +978,48 @@ int mppi_backend_dispatch_rollout(mppi_backend* b, uint64_t step_index, const fl
   b->run_mp_stride = b->run_cp_stride = 0;
   b->run_sigma = b->c_sigma();
   b->run_sigma_stride = 0;
-  if (int rc = upload_state(b, step_index, x0, u_nominal, mp, mp_bytes, cp, cp_bytes, err,
-                            err_len))
-    return rc;
-  CK(launch_rollout(b, 0));
-  CK(launch_combine(b, 0, false));
+  const bool mo = mp && mp_bytes, co = cp && cp_bytes;
+  if (mo) CK(b->d_mp_ovr.ensure(pad16(b->mp_size)));
+  if (co) CK(b->d_cp_ovr.ensure(pad16(b->cp_size)));
+  stage_upload(b, step_index, x0, u_nominal, mp, mp_bytes, cp, cp_bytes);
   float* down = b->h_down.as<float>();
   const size_t nd = b->off_stats() - b->off_uout();
-  CK(cudaMemcpyAsync(down, b->io() + b->off_uout(), nd * 4, cudaMemcpyDeviceToHost, b->stream));
+  // The whole step -- uploads from the pinned staging buffer, the proposal
+  // stage if attached, rollout, combine, download -- is one CUDA graph,
+  // captured once per (buffers, parameter pointers, module) and replayed:
+  // one launch per control step instead of four or five API calls.
+  char keybuf[256];
+  snprintf(keybuf, sizeof(keybuf), "%llu/%p/%p/%d%d/%p/%u/%p/%p/%p",
+           (unsigned long long)b->generation, (const void*)b->run_mp, (const void*)b->run_cp,
+           mo, co, (const void*)b->proposal, b->prop_samples, (const void*)b->mod.get(),
+           b->h_up.p, b->h_down.p);
+  if (b->step_graph == nullptr || b->step_key != keybuf) {
+    if (b->step_graph) {
+      cudaGraphExecDestroy(b->step_graph);
+      b->step_graph = nullptr;
+    }
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t le = issue_upload(b, mo, co);
+    if (le == cudaSuccess) le = launch_rollout(b, 0);
+    if (le == cudaSuccess) le = launch_combine(b, 0, false);
+    if (le == cudaSuccess)
+      le = cudaMemcpyAsync(down, b->io() + b->off_uout(), nd * 4, cudaMemcpyDeviceToHost,
+                           b->stream);
+    cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+    if (le != cudaSuccess || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      set_err(err, err_len, std::string("step graph capture failed: ") +
+                                cudaGetErrorString(le != cudaSuccess ? le : ce));
+      return MPPI_ERR_CUDA;
+    }
+    cudaError_t ie = cudaGraphInstantiate(&b->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    CK(ie);
+    b->step_key = keybuf;
+  }
+  CK(cudaGraphLaunch(b->step_graph, b->stream));
   CK(cudaStreamSynchronize(b->stream));
   memcpy(u_out, down, b->HM() * 4);
   if (diag3) memcpy(diag3, down + (b->off_diag() - b->off_uout()), 3 * 4);

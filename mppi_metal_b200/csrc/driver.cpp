@@ -39,6 +39,8 @@ public:
 	std::vector<float> u_max_storage;
 	std::vector<float> u_nominal;  // horizon * control_dim warm start
 	std::string proposal_features;  // owned copy of options.proposal_features
+	std::vector<float> u_updated;   // step(): the updated sequence (reused, no per-step allocation)
+	std::vector<char> step_err;     // step(): error text buffer (reused)
 
 	ParamLayout param_layout{};
 	bool params_bound = false;
@@ -279,9 +281,12 @@ bool MPPIDriver::step(
 
 	// ---- dispatch (reference :291-321); bytes == 0 selects the bound blob ----
 	const size_t seq = static_cast<size_t>(cfg.horizon) * cfg.control_dim;
-	std::vector<float> u_updated(seq, 0.0f);
+	std::vector<float>& u_updated = impl_->u_updated;
+	u_updated.resize(seq);
 	float diag[3] = {0.0f, 0.0f, 0.0f};
-	std::vector<char> err(kErrLen, '\0');
+	std::vector<char>& err = impl_->step_err;
+	if (err.size() != kErrLen) err.assign(kErrLen, '\0');
+	err[0] = '\0';
 	const ByteView& mo = inputs.model_params_override;
 	const ByteView& co = inputs.cost_params_override;
 	if (mppi_backend_dispatch_rollout(impl_->backend, impl_->step_index, inputs.x0.data,
