@@ -51,11 +51,11 @@ L2_FLUSH_BYTES = 256 << 20
 # issue-rate roofline.
 ROLLOUT_COUNTERS = {
     # workload: (warp-inst per rollout-step, DRAM bytes per launch)
-    "batch": (733569036 / 52428800, 238592),          # 13.99
-    "uneven": (205879094 / 16410677, 119296),         # 12.55
-    "single": (330776 / 30720, 41216),                # 10.77
-    "quadrotor/fp32": (8313199985 / 209715200, 328704),   # 39.64
-    "quadrotor/mixed": (7115466818 / 209715200, 135936),  # 33.93
+    "batch": (613867520 / 52428800, 235008),          # 11.71
+    "uneven": (186346246 / 16410677, 117248),         # 11.36
+    "single": (284120 / 30720, 36864),                # 9.25
+    "quadrotor/fp32": (7110760676 / 209715200, 116736),   # 33.91
+    "quadrotor/mixed": (6388229149 / 209715200, 160512),  # 30.46
 }
 
 

@@ -14,8 +14,9 @@
 //   - Philox-2x32-10, the uint -> (0,1) map and Box-Muller, the CUDA form of
 //     shaders/philox.h:19-50.  Words are bit-exact with the reference.  The
 //     normals use correctly-rounded float ops for the uniform map (identical
-//     bits to the reference) and CUDA's accurate logf / sqrtf / sincospif
-//     for the transcendental part.
+//     bits to the reference), CUDA's logf, the SM's square root and the
+//     library's own quarter-turn sine / cosine (errors of order 1e-7);
+//   - mppi_sincosf, the library's own sin / cos for plugins.
 #pragma once
 
 #if defined(__CUDACC_RTC__)
@@ -107,15 +108,89 @@ __device__ __forceinline__ float mppi_uint_to_01(uint32_t x) {
   return __fmul_rn(f, 2.3283064365386962890625e-10f);
 }
 
+// Square root by the SM's approximate square-root instruction (PTX
+// sqrt.approx.ftz.f32, relative error of order 2^-23), exact zero at zero.
+// Subnormal inputs (below 2^-126) flush to zero and give 0: that keeps it a
+// single instruction -- the form without .ftz adds a rescaling path for
+// subnormals, which measured about four more instructions per call.  Used
+// for the Box-Muller radius and by plugins for cost terms.
+__device__ __forceinline__ float mppi_sqrt_approx(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// The library's own sine / cosine.  Both reduce the argument exactly (or with
+// an error far below float rounding) to a quarter turn around zero and
+// evaluate near-minimax polynomials there.  The coefficients were fitted for
+// this library (csrc/device/derive_poly.py: Lawson's iteratively reweighted
+// least squares, then rounded to float); that script also reports the error
+// of the float32 FMA evaluation below against float64 sin / cos.
+// Quadrant q (x = q * pi/2 + r):  q%4 = 0: ( s,  c)  1: ( c, -s)
+//                                        2: (-s, -c)  3: (-c,  s)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mppi_quadrant(uint32_t q, float s, float c, float* so,
+                                              float* co) {
+  const bool swap = (q & 1u) != 0u;
+  const float a = swap ? c : s, b = swap ? s : c;
+  *so = __uint_as_float(__float_as_uint(a) ^ ((q & 2u) << 30));
+  *co = __uint_as_float(__float_as_uint(b) ^ (((q + 1u) & 2u) << 30));
+}
+
+// (sin(pi/2 v), cos(pi/2 v)) for |v| < 2^22: q = rint(v) by the 1.5 * 2^23
+// rounding constant, and f = v - q is exact (|f| <= 1/2, Sterbenz), so the
+// only errors are the polynomials' (at most 8.3e-8 for sin and 5.8e-8 for cos,
+// absolute).
+__device__ __forceinline__ void mppi_sincos_quarter(float v, float* so, float* co) {
+  const float t = __fadd_rn(v, 0x1.8p23f);
+  const float q = __fsub_rn(t, 0x1.8p23f);
+  const float f = __fsub_rn(v, q);
+  const float z = __fmul_rn(f, f);
+  float ps = fmaf(-0x1.2d930ep-8f, z, 0x1.465e92p-4f);
+  ps = fmaf(ps, z, -0x1.4abbbap-1f);
+  ps = fmaf(ps, z, 0x1.921fb6p+0f);
+  float pc = fmaf(0x1.d9f7c8p-11f, z, -0x1.55c664p-6f);
+  pc = fmaf(pc, z, 0x1.03c1dep-2f);
+  pc = fmaf(pc, z, -0x1.3bd3ccp+0f);
+  mppi_quadrant(__float_as_uint(t), __fmul_rn(f, ps), fmaf(pc, z, 1.0f), so, co);
+}
+
+// sin and cos of x (radians), for plugins.  Cody and Waite's reduction by
+// pi/2 (W. J. Cody, W. Waite, "Software Manual for the Elementary Functions",
+// 1980) with FMAs and pi/2 split into two floats: |x| < 65536 keeps the
+// reduction error below 1.2e-10; beyond that the call falls back to CUDA's
+// sincosf.  Error at most 4.4e-8 (sin) and 5.3e-8 (cos) absolute on the
+// reduced argument.
+__device__ __forceinline__ void mppi_sincosf(float x, float* so, float* co) {
+  if (!(fabsf(x) < 65536.0f)) {
+    sincosf(x, so, co);
+    return;
+  }
+  const float t = fmaf(x, 0x1.45f306p-1f, 0x1.8p23f);  // x * 2/pi + 1.5 * 2^23
+  const float q = __fsub_rn(t, 0x1.8p23f);
+  float r = fmaf(-q, 0x1.921fb6p+0f, x);
+  r = fmaf(-q, -0x1.777a5cp-25f, r);
+  const float z = __fmul_rn(r, r);
+  float ps = fmaf(-0x1.9943f2p-13f, z, 0x1.11073cp-7f);
+  ps = fmaf(ps, z, -0x1.555546p-3f);
+  float pc = fmaf(0x1.99343ap-16f, z, -0x1.6c087ep-10f);
+  pc = fmaf(pc, z, 0x1.55553ep-5f);
+  pc = fmaf(pc, z, -0.5f);
+  mppi_quadrant(__float_as_uint(t), fmaf(ps, __fmul_rn(r, z), r), fmaf(pc, z, 1.0f), so, co);
+}
+
 // Box-Muller (shaders/philox.h:44-50): r = sqrt(-2 ln u1), theta = 2 pi u2.
-// sincospif(2 u2) evaluates sin/cos(2 pi u2) without rounding 2 pi u2 to a
-// float first, so it stays closer to the exact value the oracle computes.
+// The angle is taken as a quarter-turn count, 4 u2 = (x2 + 0.5) * 2^-30 --
+// exactly 4 times the reference's u2 -- so 2 pi u2 is never rounded to a
+// float; CUDA's logf gives ln u1 and the SM's square root the radius (relative
+// error of order 2^-23).
 __device__ __forceinline__ float2 mppi_box_muller(uint2 w) {
   const float u1 = mppi_uint_to_01(w.x);
-  const float u2 = mppi_uint_to_01(w.y);
-  const float r = sqrtf(-2.0f * logf(u1));
+  const float v = __fmul_rn(__fadd_rn(__uint2float_rn(w.y), 0.5f), 0x1p-30f);
+  const float r = mppi_sqrt_approx(-2.0f * logf(u1));
   float s, c;
-  sincospif(2.0f * u2, &s, &c);
+  mppi_sincos_quarter(v, &s, &c);
   return make_float2(r * c, r * s);
 }
 
@@ -133,14 +208,6 @@ __device__ __forceinline__ float mppi_f16_to_f32(uint16_t h) {
   return f;
 }
 
-// Square root by the SM's approximate square-root instruction (PTX
-// sqrt.approx.f32, relative error of order 2^-23): one instruction, exact
-// zero at zero.  For plugin cost terms where a few ulps do not matter.
-__device__ __forceinline__ float mppi_sqrt_approx(float x) {
-  float r;
-  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return r;
-}
 
 // Box-Muller with the SM's approximate log2 / sqrt / sin / cos (relative
 // errors of order 2^-21), for the half-precision noise mode whose output is

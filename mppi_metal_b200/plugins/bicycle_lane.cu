@@ -12,7 +12,7 @@ __device__ void mppi_dynamics(uint8_t* state_raw, const float* control,
   const float dt = p->dt;
   const float th = s[2], v = s[3], de = s[4];
   float sn, cs;
-  sincosf(th, &sn, &cs);
+  mppi_sincosf(th, &sn, &cs);
   s[0] += v * cs * dt;
   s[1] += v * sn * dt;
   s[2] += v / p->wheelbase * tanf(de) * dt;

@@ -20,9 +20,9 @@ __device__ void mppi_dynamics(uint8_t* state_raw, const float* u,
   const float ty = mp->arm * (u[2] - u[0]);
   const float tz = mp->yaw_coef * (u[0] - u[1] + u[2] - u[3]);
   float sph, cph, sth, cth, sps, cps;
-  sincosf(ph, &sph, &cph);
-  sincosf(th, &sth, &cth);
-  sincosf(ps, &sps, &cps);
+  mppi_sincosf(ph, &sph, &cph);
+  mppi_sincosf(th, &sth, &cth);
+  mppi_sincosf(ps, &sps, &cps);
   const float zx = cph * sth * cps + sph * sps;
   const float zy = cph * sth * sps - sph * cps;
   const float zz = cph * cth;

@@ -6,7 +6,8 @@
 // branch-free (approximate square root), in a loop unrolled to a
 // compile-time bound chosen by one uniform branch on num_obs, so the
 // obstacles form independent instruction streams the compiler can
-// interleave; the terms are summed as a tree.
+// interleave; the terms are summed as a tree.  The heading's sine and cosine
+// come from the library's mppi_sincosf (about 1e-7 absolute).
 //
 // mppi_proposal_features gives the learned proposal its 31 inputs.
 #include "mppi_core.h"
@@ -19,7 +20,7 @@ __device__ void mppi_dynamics(uint8_t* state_raw, const float* control,
   float* s = reinterpret_cast<float*>(state_raw);
   const float dt = p->dt;
   float sn, cs;
-  sincosf(s[2], &sn, &cs);
+  mppi_sincosf(s[2], &sn, &cs);
   s[0] += control[0] * cs * dt;
   s[1] += control[0] * sn * dt;
   s[2] += control[1] * dt;
