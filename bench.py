@@ -51,9 +51,9 @@ L2_FLUSH_BYTES = 256 << 20
 # issue-rate roofline.
 ROLLOUT_COUNTERS = {
     # workload: (warp-inst per rollout-step, DRAM bytes per launch)
-    "batch": (613867520 / 52428800, 235008),          # 11.71
+    "batch": (517988352 / 52428800, 231424),          # 9.88
     "uneven": (186346246 / 16410677, 117248),         # 11.36
-    "single": (284120 / 30720, 36864),                # 9.25
+    "single": (259640 / 30720, 33792),                # 8.45
     "quadrotor/fp32": (7110760676 / 209715200, 116736),   # 33.91
     "quadrotor/mixed": (6388229149 / 209715200, 160512),  # 30.46
 }

@@ -190,6 +190,14 @@ int mppi_backend_tuning_info(mppi_backend* b, uint32_t* grid, uint32_t* num_work
 int mppi_device_philox(uint64_t n, const uint32_t* ctr0, const uint32_t* ctr1,
                        const uint32_t* key, uint32_t* out_pairs, char* err, size_t err_len);
 
+/* The library's own sine / cosine evaluated on the device (accuracy tests;
+ * no counterpart in the reference, whose Metal build uses the platform's
+ * fast-math sin / cos): quarter == 0 gives (sin x, cos x) of mppi_sincosf,
+ * quarter != 0 gives (sin(pi/2 x), cos(pi/2 x)) of mppi_sincos_quarter, the
+ * Box-Muller angle's form. */
+int mppi_device_sincos(uint64_t n, const float* x, int quarter, float* sin_out,
+                       float* cos_out, char* err, size_t err_len);
+
 /* ---- allocation-free control step --------------------------------------
  * No counterpart in the reference.  For callers that must not allocate
  * device memory once running (a fixed-rate control loop, where cudaMalloc /

@@ -303,6 +303,19 @@ def device_philox(c0, c1, key) -> np.ndarray:
     return out
 
 
+def device_sincos(x, quarter: bool = False):
+    """(sin, cos) by the library's own device functions: mppi_sincosf of x in
+    radians, or (quarter=True) mppi_sincos_quarter, i.e. of pi/2 * x."""
+    lib = _lib.load()
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    s = np.zeros_like(x)
+    c = np.zeros_like(x)
+    eb = _lib.err_buf()
+    _check(lib.mppi_device_sincos(x.size, _p(x), int(bool(quarter)), _p(s), _p(c), eb, len(eb)),
+           eb)
+    return s, c
+
+
 def compile_check(plugin: str, state_dim: int, control_dim: int, cov_full: bool = False,
                   control_cost: bool = False, stage_cost: str = "mppi_stage_cost",
                   terminal_cost: str = "mppi_terminal_cost", dynamics: str = "mppi_dynamics",

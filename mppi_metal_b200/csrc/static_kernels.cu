@@ -1,5 +1,6 @@
 // static_kernels.cu — kernels compiled ahead of time by nvcc for sm_100a
-// (no plugin dependency): the Philox-2x32-10 known-answer path.
+// (no plugin dependency): the Philox-2x32-10 known-answer path and the
+// accuracy path of the library's own sine / cosine.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -15,6 +16,19 @@ __global__ void __launch_bounds__(256)
                         uint2* out) {
   const uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
   if (i < n) out[i] = mppi_philox2x32_10(make_uint2(c0[i], c1[i]), key[i]);
+}
+
+__global__ void __launch_bounds__(256)
+    sincos_kernel(uint64_t n, const float* x, int quarter, float* so, float* co) {
+  const uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
+  if (i >= n) return;
+  float s, c;
+  if (quarter)
+    mppi_sincos_quarter(x[i], &s, &c);
+  else
+    mppi_sincosf(x[i], &s, &c);
+  so[i] = s;
+  co[i] = c;
 }
 
 void set_err(char* err, size_t len, const std::string& msg) {
@@ -56,6 +70,41 @@ extern "C" int mppi_device_philox(uint64_t n, const uint32_t* c0, const uint32_t
     philox_words_kernel<<<(unsigned)((n + 255) / 256), 256>>>(n, dc0, dc0 + n, dc0 + 2 * n, o);
     e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpy(out, o, 2 * in_bytes, cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+  }
+  if (e != cudaSuccess) {
+    set_err(err, err_len, std::string("CUDA error: ") + cudaGetErrorString(e));
+    return MPPI_ERR_CUDA;
+  }
+  return MPPI_OK;
+}
+
+extern "C" int mppi_device_sincos(uint64_t n, const float* x, int quarter, float* sin_out,
+                                  float* cos_out, char* err, size_t err_len) {
+  if (n == 0) return MPPI_OK;
+  if (!x || !sin_out || !cos_out) {
+    set_err(err, err_len, "null argument to mppi_device_sincos.");
+    return MPPI_ERR_INVALID;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_err(err, err_len, "No CUDA device available.");
+    return MPPI_ERR_NO_DEVICE;
+  }
+  void* buf = nullptr;
+  const size_t bytes = n * 4;
+  cudaError_t e = cudaMalloc(&buf, 3 * bytes);
+  if (e == cudaSuccess) {
+    float* dx = static_cast<float*>(buf);  // [x n][sin n][cos n]
+    e = cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      sincos_kernel<<<(unsigned)((n + 255) / 256), 256>>>(n, dx, quarter ? 1 : 0, dx + n,
+                                                          dx + 2 * n);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(sin_out, dx + n, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(cos_out, dx + 2 * n, bytes, cudaMemcpyDeviceToHost);
     cudaFree(buf);
   }
   if (e != cudaSuccess) {

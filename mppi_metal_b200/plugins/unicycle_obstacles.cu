@@ -3,10 +3,11 @@
 // control [v, omega].
 //
 // The penetration max(0, r - |p - c(t)|) of every obstacle is evaluated
-// branch-free (approximate square root), in a loop unrolled to a
-// compile-time bound chosen by one uniform branch on num_obs, so the
-// obstacles form independent instruction streams the compiler can
-// interleave; the terms are summed as a tree.  The heading's sine and cosine
+// branch-free (approximate square root), two obstacles per packed FP32x2
+// instruction, in a loop unrolled to a compile-time bound chosen by one
+// uniform branch on num_obs, so the obstacle pairs form independent
+// instruction streams the compiler can interleave; the terms are summed as a
+// tree.  The heading's sine and cosine
 // come from the library's mppi_sincosf (about 1e-7 absolute).
 //
 // mppi_proposal_features gives the learned proposal its 31 inputs.
@@ -32,27 +33,45 @@ __device__ __forceinline__ float unicycle_goal(const float* s, const UnicycleCos
   return c->w_goal * (dx * dx + dy * dy);
 }
 
-// Sum over obstacles [0, N) of max(0, r_i - |p - c_i(t)|).  MASK: obstacles
-// at or beyond num_obs contribute nothing (not needed when num_obs == N).
+// Sum over obstacles [0, N) of max(0, r_i - |p - c_i(t)|), two obstacles per
+// packed FP32x2 instruction (sm_100 FFMA2 / FADD2 / FMUL2, each lane rounded
+// like the scalar operation, so the sum is the scalar loop's): the centre
+// c = c0 + v t, the offset c - p, the squared distance, and the penetration
+// as r - min(d, r).  MASK: obstacles at or beyond num_obs contribute nothing
+// (not needed when num_obs == N).  The parameter arrays are 8-byte aligned
+// in the blob, and the library passes blobs 16-byte aligned.
 template <int N, bool MASK>
 __device__ __forceinline__ float unicycle_penetration(const float* s, const UnicycleCostParams* c) {
+  static_assert(N % 2 == 0, "obstacles come in pairs");
   const float t = s[3];
   const unsigned n = c->num_obs;
-  float pen[N];
+  const float2 tt = make_float2(t, t);
+  const float2 nx = make_float2(-s[0], -s[0]), ny = make_float2(-s[1], -s[1]);
+  const float2* cx2 = reinterpret_cast<const float2*>(c->obs_cx);
+  const float2* cy2 = reinterpret_cast<const float2*>(c->obs_cy);
+  const float2* vx2 = reinterpret_cast<const float2*>(c->obs_vx);
+  const float2* vy2 = reinterpret_cast<const float2*>(c->obs_vy);
+  const float2* r2 = reinterpret_cast<const float2*>(c->obs_r);
+  float2 pen[N / 2];
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    const float cx = fmaf(c->obs_vx[i], t, c->obs_cx[i]);
-    const float cy = fmaf(c->obs_vy[i], t, c->obs_cy[i]);
-    const float ex = s[0] - cx, ey = s[1] - cy;
-    const float d = mppi_sqrt_approx(fmaf(ex, ex, ey * ey));
-    const float r = (!MASK || (unsigned)i < n) ? c->obs_r[i] : 0.0f;
-    pen[i] = fmaxf(r - d, 0.0f);
+  for (int j = 0; j < N / 2; ++j) {
+    const float2 ex = __fadd2_rn(__ffma2_rn(vx2[j], tt, cx2[j]), nx);
+    const float2 ey = __fadd2_rn(__ffma2_rn(vy2[j], tt, cy2[j]), ny);
+    const float2 d2 = __ffma2_rn(ex, ex, __fmul2_rn(ey, ey));
+    float2 r = r2[j];
+    if (MASK) {
+      r.x = (unsigned)(2 * j) < n ? r.x : 0.0f;
+      r.y = (unsigned)(2 * j + 1) < n ? r.y : 0.0f;
+    }
+    const float2 m = make_float2(fminf(mppi_sqrt_approx(d2.x), r.x),
+                                 fminf(mppi_sqrt_approx(d2.y), r.y));
+    pen[j] = __fadd2_rn(r, make_float2(-m.x, -m.y));
   }
 #pragma unroll
-  for (int w = 1; w < N; w *= 2)
+  for (int w = 1; w < N / 2; w *= 2)
 #pragma unroll
-    for (int i = 0; i + w < N; i += 2 * w) pen[i] += pen[i + w];
-  return pen[0];
+    for (int i = 0; i + w < N / 2; i += 2 * w) pen[i] = __fadd2_rn(pen[i], pen[i + w]);
+  return pen[0].x + pen[0].y;
 }
 
 __device__ float mppi_stage_cost(const float* s, const float* control,

@@ -21,7 +21,7 @@ import pytest
 
 from helpers import abs_err, backend_for, nonholonomic_example, oracle_problem, rel_err
 from mppi_metal_b200 import models
-from mppi_metal_b200.backend import Backend, device_philox
+from mppi_metal_b200.backend import Backend, device_philox, device_sincos
 
 pytestmark = pytest.mark.gpu
 
@@ -41,6 +41,47 @@ def test_device_philox_matches_oracle_large(oracle):
     rng = np.random.default_rng(5)
     c = rng.integers(0, 2 ** 32, size=(3, 1 << 16), dtype=np.uint64).astype(np.uint32)
     assert np.array_equal(device_philox(c[0], c[1], c[2]), oracle.philox(c[0], c[1], c[2]))
+
+
+# The library's own sin / cos (mppi_prelude.cuh): polynomial error about 8e-8
+# plus the float rounding of the reduced argument, against float64 of the
+# same float inputs.
+TOL_SINCOS = 1.5e-7
+
+
+def test_device_sincos_radians_accuracy():
+    rng = np.random.default_rng(11)
+    q = np.arange(-2000, 2001, dtype=np.float64)
+    x = np.concatenate([
+        np.linspace(-50.0, 50.0, 400001),
+        rng.uniform(-65535.0, 65535.0, 200000),
+        q * (np.pi / 2), q * (np.pi / 2) + 1e-4, q * (np.pi / 4),   # quadrant edges
+        [0.0, -0.0, 1e-30, -1e-30, 1e-8, np.pi, -np.pi],
+    ]).astype(np.float32)
+    s, c = device_sincos(x)
+    xd = x.astype(np.float64)
+    assert np.max(np.abs(s - np.sin(xd))) < TOL_SINCOS
+    assert np.max(np.abs(c - np.cos(xd))) < TOL_SINCOS
+    # beyond the reduction's range the call falls back to CUDA's sincosf
+    big = np.array([65536.0, -1e5, 3.0e6, 1.0e30], np.float32)
+    s, c = device_sincos(big)
+    assert np.max(np.abs(s - np.sin(big.astype(np.float64)))) < 1e-6
+    assert np.max(np.abs(c - np.cos(big.astype(np.float64)))) < 1e-6
+    s, c = device_sincos(np.array([np.inf, np.nan], np.float32))
+    assert np.all(np.isnan(s)) and np.all(np.isnan(c))
+
+
+def test_device_sincos_quarter_turn_accuracy():
+    # Box-Muller's angle: v = 4 u2 = (x + 0.5) 2^-30 for every Philox word x
+    rng = np.random.default_rng(12)
+    w = np.concatenate([rng.integers(0, 2 ** 32, 1 << 20, dtype=np.uint64),
+                        [0, 1, 2 ** 30 - 1, 2 ** 30, 2 ** 31, 3 * 2 ** 30, 2 ** 32 - 1]])
+    v = ((w.astype(np.float32) + np.float32(0.5)) * np.float32(2.0 ** -30)).astype(np.float32)
+    s, c = device_sincos(v, quarter=True)
+    vd = v.astype(np.float64) * (np.pi / 2)
+    assert np.max(np.abs(s - np.sin(vd))) < TOL_SINCOS
+    assert np.max(np.abs(c - np.cos(vd))) < TOL_SINCOS
+    assert s[-1] == 0.0 and c[-1] == 1.0  # u2 rounds to 1: a full turn
 
 
 def test_noise_normals_match_oracle(oracle):
