@@ -277,8 +277,9 @@ bool valid_identifier(const char* s) {
 // Launch geometry for N agents (fixed K, H): block size and how the noise
 // is kept for the weighted sums.  Staging the whole horizon during the
 // rollout avoids regenerating it; it needs H*m*block*4 bytes per CTA, so it
-// is used while that keeps >= 2 CTAs per SM, otherwise the noise is
-// regenerated in chunks after the costs are known.
+// is used while that keeps four CTAs per SM, or when every CTA of the launch
+// is resident at once with it; otherwise the noise is regenerated in chunks
+// after the costs are known.
 LaunchGeom choose_geometry(const mppi_backend* b) {
   LaunchGeom g;
   const size_t HM = b->HM();
@@ -302,6 +303,20 @@ LaunchGeom choose_geometry(const mppi_backend* b) {
       g.stage_rows = (uint32_t)HM;
       g.smem = full;
       break;
+    }
+    // A launch whose CTAs are all resident at once with the whole horizon
+    // staged (few agents x few samples: one partial wave) gains nothing from
+    // the fourth CTA per SM, and chunked staging would regenerate every
+    // noise value after the costs are known: stage the whole horizon.
+    if (full <= budget && b->N > 0) {
+      const size_t per_sm = b->smem_reserved + b->mod->rollout_static_smem[vi] + full;
+      const size_t fit = std::min<size_t>(512 / block, b->smem_per_sm / per_sm);
+      const size_t ctas = (size_t)b->N * ((b->K + block - 1) / block);
+      if (fit >= 1 && ctas <= fit * (size_t)b->num_sms) {
+        g.stage_rows = (uint32_t)HM;
+        g.smem = full;
+        break;
+      }
     }
     const size_t room = per_cta > fixed + (size_t)block * el * b->m ? per_cta - fixed
                                                                      : (size_t)block * el * b->m;
