@@ -51,11 +51,11 @@ L2_FLUSH_BYTES = 256 << 20
 # issue-rate roofline.
 ROLLOUT_COUNTERS = {
     # workload: (warp-inst per rollout-step, DRAM bytes per launch)
-    "batch": (517988352 / 52428800, 231424),          # 9.88
-    "uneven": (186346246 / 16410677, 117248),         # 11.36
-    "single": (259640 / 30720, 33792),                # 8.45
-    "quadrotor/fp32": (7110760676 / 209715200, 116736),   # 33.91
-    "quadrotor/mixed": (6388229149 / 209715200, 160512),  # 30.46
+    "batch": (509501440 / 52428800, 238336),          # 9.72
+    "uneven": (186096022 / 16410677, 123136),         # 11.34
+    "single": (255224 / 30720, 40960),                # 8.31
+    "quadrotor/fp32": (7108453214 / 209715200, 487168),   # 33.90
+    "quadrotor/mixed": (6401390457 / 209715200, 124416),  # 30.52
 }
 
 

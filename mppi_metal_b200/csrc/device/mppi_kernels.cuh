@@ -332,7 +332,7 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   for (uint32_t t0 = 0; t0 < H; t0 += TC) {
     const uint32_t t1 = min(H, t0 + TC);
     const uint32_t row0 = staged ? 0u : t0;  // staging row of step t is (t - row0) * m + d
-#pragma unroll 2
+#pragma unroll 4
     for (uint32_t t = t0; t < t1; ++t) {
       float n[2 * kP], eps[kM];
       if (active) {

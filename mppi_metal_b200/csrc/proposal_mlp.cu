@@ -94,13 +94,38 @@ __host__ __device__ __forceinline__ size_t timg(uint32_t r, uint32_t col, uint32
          (col & 7);
 }
 
+// GELU(z) = z Phi(z) with Phi(z) = (1 + erf(z / sqrt 2)) / 2, and its
+// derivative Phi(z) + z phi(z).  erf by Abramowitz and Stegun, "Handbook of
+// Mathematical Functions", eq. 7.1.26 (Hastings' approximation): for x >= 0,
+// erf x = 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2) with
+// t = 1 / (1 + p x), |error| <= 1.5e-7; the reciprocal and the exponential
+// come from the SM's approximate instructions (relative errors of order
+// 2^-22).  The exp(-x^2) = exp(-z^2 / 2) it computes is the Gaussian factor of
+// the derivative as well.  The activations are rounded to BF16 (8 significant
+// bits) before they feed the next GEMM, far above this error.
+__device__ __forceinline__ void gelu_phi(float z, float& cdf, float& gauss) {
+  const float x = fabsf(z) * 0.70710678118654752f;
+  float t;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(t) : "f"(fmaf(0.3275911f, x, 1.0f)));
+  float p = fmaf(1.061405429f, t, -1.453152027f);
+  p = fmaf(p, t, 1.421413741f);
+  p = fmaf(p, t, -0.284496736f);
+  p = fmaf(p, t, 0.254829592f);
+  p *= t;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(gauss) : "f"(-1.44269504088896341f * x * x));
+  cdf = fmaf(0.5f, copysignf(fmaf(-p, gauss, 1.0f), z), 0.5f);
+}
+
 __device__ __forceinline__ float gelu(float z) {
-  return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f));
+  float cdf, g;
+  gelu_phi(z, cdf, g);
+  return z * cdf;
 }
 
 __device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) +
-         z * 0.39894228040143268f * expf(-0.5f * z * z);
+  float cdf, g;
+  gelu_phi(z, cdf, g);
+  return fmaf(z * 0.39894228040143268f, g, cdf);
 }
 
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
@@ -401,18 +426,10 @@ __device__ __forceinline__ uint32_t map_to_rank(uint32_t saddr, uint32_t rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(saddr), "r"(rank));
   return out;
 }
-__device__ __forceinline__ void st_cluster_v4(uint32_t addr, uint4 v) {
-  asm volatile("st.shared::cluster.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x),
-               "r"(v.y), "r"(v.z), "r"(v.w)
-               : "memory");
-}
 // Every thread of every CTA of the cluster arrives; all pass together.
 __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
   asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void fence_async_cluster() {
-  asm volatile("fence.proxy.async.shared::cluster;" ::: "memory");
 }
 
 // 16-column chunks of an N-wide layer dealt to the cluster's CTAs.
@@ -421,6 +438,12 @@ __device__ __forceinline__ void cluster_slice(uint32_t N, uint32_t c, uint32_t& 
   const uint32_t chunks = N / 16, q = chunks / kCluster, rem = chunks % kCluster;
   col0 = 16 * (c * q + min(c, rem));
   ncols = 16 * (q + (c < rem ? 1u : 0u));
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint4 v) {
+  asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(v.x), "r"(v.y),
+               "r"(v.z), "r"(v.w)
+               : "memory");
 }
 
 // Remote asynchronous store: 16 bytes into another CTA's shared memory,
@@ -437,10 +460,10 @@ __device__ __forceinline__ void st_async_v4(uint32_t addr, uint4 v, uint32_t mba
 
 // Activations ping-pong between two A tiles, each with its own "full"
 // mbarrier: layer g reads A[g % 2]; its epilogue stores the CTA's column
-// slice of the next activations into A[(g + 1) % 2] of all four CTAs with
-// st.async, completing 64 KB per layer on each receiver's full barrier,
-// which the receiver arms (arrive.expect_tx) and waits on before its next
-// MMA.  Reuse is safe by causality: a CTA writes A[(g + 1) % 2] of a peer
+// slice of the next activations into its own A[(g + 1) % 2] with plain
+// stores and into the three peers' with st.async, completing 48 KB per layer
+// on each receiver's full barrier, which the receiver arms (arrive.expect_tx)
+// and waits on before its next MMA.  Reuse is safe by causality: a CTA writes A[(g + 1) % 2] of a peer
 // only after its own MMA g, which needed that peer's slice of layer g's
 // input, which the peer sent after its MMA g - 1 -- the last reader of the
 // buffer being overwritten -- had completed.  Only the start (every
@@ -527,8 +550,12 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
         }
       }
       if (g > 0) {
+        // the peers' column slices of layer g - 1's output (this CTA's own
+        // slice was stored locally)
         const uint32_t full = bar_full0 + 8 * buf;
-        tc::mbar_expect_tx(full, kTileBytes);
+        uint32_t oc0, onc;
+        cluster_slice(kHid, crank, oc0, onc);
+        tc::mbar_expect_tx(full, kTileBytes - kTile * onc * 2);
         if (!tc::mbar_wait(full, ph_f[buf])) {
           atomicOr(a.err, 8);
           *abort_s = 1;
@@ -588,9 +615,15 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
         const uint4 hi = make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]),
                                     pack2(v[14], v[15]));
         const uint32_t dst = off + 2 * canon(r, col0 + 16 * j, kHid);
+        // this CTA's own slice by plain local stores (made visible to the
+        // tensor core by the proxy fence and barrier at the next layer's
+        // start), the peers' copies by remote asynchronous stores
+        st_shared_v4(dst, lo);
+        st_shared_v4(dst + 128, hi);
 #pragma unroll
-        for (uint32_t q = 0; q < kCluster; ++q) {
-          const uint32_t rd = map_to_rank(dst, q), rb = map_to_rank(full, q);
+        for (uint32_t q = 1; q < kCluster; ++q) {
+          const uint32_t peer = (crank + q) % kCluster;
+          const uint32_t rd = map_to_rank(dst, peer), rb = map_to_rank(full, peer);
           st_async_v4(rd, lo, rb);
           st_async_v4(rd + 128, hi, rb);
         }
