@@ -467,7 +467,7 @@ def run_b200(args):
                              "mean_first_agents": float(cost[:8].mean())},
         "e2e": {"value": e2e_value, "unit": "rollout-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e2e_total / args.steps},
-        "gpu_launches": 2 * T * args.steps,
+        "gpu_launches": geom["kernels_per_step"] * T * args.steps,
         "launch_geometry": geom,
         "autotuner": tuning or None,
         "roofline": roof,
@@ -621,6 +621,7 @@ def run_proposal(args):
     prop.set_features(P.FEATURES_CALLABLE, spec["features"])
     prop.set_proposal(net, KS)
     prop_ms, prop_cost, clk = timed_arm(prop)
+    kernels_per_step = prop.launch_info()["kernels_per_step"]  # network + rollout(+combine)
     rollout_ms, combine_ms = prop.time_passes(20)
     feat_ms, net_ms = prop.time_proposal(20)
     prop.set_proposal(None)
@@ -707,7 +708,7 @@ def run_proposal(args):
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": 1e3 * e2e_total / args.steps,
                 "closed_loop_cost_mean": float(e2e_cost.mean())},
-        "gpu_launches": (3 * T + 1) * args.steps,
+        "gpu_launches": (kernels_per_step * T + 1) * args.steps,
         "kernel_ms_per_pass": {"rollout": rollout_ms, "combine": combine_ms,
                                "features_kernel": feat_ms, "network": net_ms},
         "roofline": {"kernel": "mlp_forward_cluster_kernel (proposal network forward)",

@@ -174,7 +174,10 @@ int mppi_backend_sample_noise(mppi_backend* b, uint64_t step_index, uint32_t age
  * the backend's stream. */
 int mppi_backend_time_passes(mppi_backend* b, uint32_t iters, float* rollout_ms,
                              float* combine_ms, char* err, size_t err_len);
-/* Launch geometry chosen for the prepared batch shape. */
+/* Launch geometry chosen for the prepared batch shape; kernels_per_step =
+ * kernel launches of one closed-loop control step (the rollout, which runs
+ * the combine in each agent's last CTA for uniform batches, or rollout and
+ * combine kernels; plus the network when a proposal is attached). */
 int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
                              uint32_t* stage_rows, uint32_t* smem_bytes,
                              uint32_t* kernels_per_step);

@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -165,6 +166,10 @@ struct mppi_backend {
   uint32_t N = 0, T = 0;
   LaunchGeom geom;
   DevBuf d_io, d_costs, d_partials;
+  DevBuf d_done;  // [N] per-agent count of finished rollout CTAs (fused combine)
+  // Uniform batches run the combine inside the rollout launch (its agent's
+  // last CTA); MPPI_B200_SEPARATE_COMBINE=1 keeps the separate combine kernel.
+  bool fuse_combine = true;
   DevBuf d_hs, d_hc, d_hk, d_term;
   DevBuf d_agent_sigma, d_agent_mp, d_agent_cp;
   bool want_s = false, want_c = false, want_k = false, want_t = false;
@@ -332,6 +337,8 @@ LaunchGeom choose_geometry(const mppi_backend* b) {
   return g;
 }
 
+size_t combine_smem(const mppi_backend* b);
+
 int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool wk, bool wt,
                  char* err, size_t err_len) {
   bool grew = false;
@@ -368,6 +375,15 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
   CK(b->d_costs.ensure((size_t)N * b->K * 4, &grew));
   const size_t records = b->ragged ? b->total_records : (size_t)N * b->geom.nblk;
   CK(b->d_partials.ensure(records * b->geom.pstride * 4, &grew));
+  {
+    // the fused combine's counters start at zero (the kernel leaves them so)
+    bool fresh = false;
+    CK(b->d_done.ensure((size_t)N * 4, &fresh));
+    if (fresh) {
+      grew = true;
+      CK(cudaMemsetAsync(b->d_done.p, 0, b->d_done.bytes, b->stream));
+    }
+  }
   b->want_s = ws;
   b->want_c = wc;
   b->want_k = wk;
@@ -387,6 +403,7 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
   if (grew) ++b->generation;
   const void* k = b->ragged ? (const void*)b->mod->rollout_work
                             : (const void*)b->mod->rollout[b->geom.variant];
+  if (!b->ragged) b->geom.smem = std::max(b->geom.smem, combine_smem(b));
   if (b->geom.smem > 48 * 1024)
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem));
   if (!b->ragged) b->shape_key = key;
@@ -624,6 +641,24 @@ cudaError_t launch_combine(mppi_backend* b, uint32_t step_local, bool propagate)
                           combine_smem(b), b->stream);
 }
 
+bool fused_combine(const mppi_backend* b) { return b->fuse_combine && !b->ragged; }
+
+// One step's kernels after the proposal stage: the rollout with the combine
+// fused into it (uniform batches), or the rollout and combine kernels.
+cudaError_t launch_rollout_combine(mppi_backend* b, uint32_t step_local, bool propagate) {
+  if (!fused_combine(b)) {
+    cudaError_t e = launch_rollout_kernel(b, step_local);
+    return e == cudaSuccess ? launch_combine(b, step_local, propagate) : e;
+  }
+  MppiRolloutArgs a = rollout_args(b, step_local);
+  a.agent_done = b->d_done.as<uint32_t>();
+  a.comb = combine_args(b, step_local, propagate);
+  void* args[] = {&a};
+  return cudaLaunchKernel((const void*)b->mod->rollout[b->geom.variant],
+                          dim3(b->geom.nblk, b->N), dim3(b->geom.block), args, b->geom.smem,
+                          b->stream);
+}
+
 // Resolves the parameter blob pointers of a run: per-agent blobs, an
 // override, the bound blob, or a zero word (the reference binds a 1-byte zero
 // buffer when nothing is bound, metal_backend.mm:595-600).
@@ -769,8 +804,7 @@ int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
     if (prop) le = launch_features(b);
     for (uint32_t s = 0; s < b->T && le == cudaSuccess; ++s) {
       if (prop) le = launch_network(b);
-      if (le == cudaSuccess) le = launch_rollout_kernel(b, s);
-      if (le == cudaSuccess) le = launch_combine(b, s, true);
+      if (le == cudaSuccess) le = launch_rollout_combine(b, s, true);
     }
     cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
     if (le != cudaSuccess || ce != cudaSuccess) {
@@ -798,6 +832,10 @@ const char* mppi_b200_version(void) { return "mppi_metal_b200 0.1.0 (sm_100a)"; 
 int mppi_backend_create(mppi_backend** out) {
   if (!out) return MPPI_ERR_INVALID;
   *out = new (std::nothrow) mppi_backend();
+  if (*out) {
+    const char* sep = getenv("MPPI_B200_SEPARATE_COMBINE");
+    (*out)->fuse_combine = !(sep && *sep && *sep != '0');
+  }
   return *out ? MPPI_OK : MPPI_ERR_INVALID;
 }
 
@@ -1016,8 +1054,8 @@ int mppi_backend_dispatch_rollout(mppi_backend* b, uint64_t step_index, const fl
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t le = issue_upload(b, mo, co);
-    if (le == cudaSuccess) le = launch_rollout(b, 0);
-    if (le == cudaSuccess) le = launch_combine(b, 0, false);
+    if (le == cudaSuccess && b->proposal && b->spec.proposal) le = launch_proposal(b);
+    if (le == cudaSuccess) le = launch_rollout_combine(b, 0, false);
     if (le == cudaSuccess)
       le = cudaMemcpyAsync(down, b->io() + b->off_uout(), nd * 4, cudaMemcpyDeviceToHost,
                            b->stream);
@@ -1472,7 +1510,8 @@ int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
   if (nblk) *nblk = b->geom.nblk;
   if (stage_rows) *stage_rows = b->geom.stage_rows;
   if (smem_bytes) *smem_bytes = (uint32_t)b->geom.smem;
-  if (kernels_per_step) *kernels_per_step = 2;
+  if (kernels_per_step)
+    *kernels_per_step = (fused_combine(b) ? 1u : 2u) + (b->proposal && b->spec.proposal ? 1u : 0u);
   return MPPI_OK;
 }
 

@@ -438,12 +438,31 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   }
 }
 
+template <int CB>
+__device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t agent,
+                                              float* dsm);
+
 // Uniform batch: grid (nblk, num_agents), every agent K samples, horizon H.
+// With a.agent_done the agent's last CTA to finish also runs its combine
+// (the "last block" pattern: every CTA publishes its partial record with a
+// device-scope fence before it counts itself done, so the CTA that sees the
+// count reach nblk reads every record complete; no CTA waits on another).
 template <int BLOCK>
 __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   const uint32_t agent = blockIdx.y, blk = blockIdx.x;
   rollout_item<BLOCK>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
                       a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
+  if (a.agent_done == nullptr) return;
+  __shared__ uint32_t last_s;
+  __threadfence();  // this CTA's partial record (written by several threads)
+  __syncthreads();  // ... complete, and the staging memory free for reuse
+  if (threadIdx.x == 0) last_s = atomicAdd(a.agent_done + agent, 1u) + 1u == a.nblk;
+  __syncthreads();
+  if (!last_s) return;
+  __threadfence();  // the other CTAs' records, published before their counts
+  extern __shared__ __align__(16) float dsm_c[];
+  combine_agent<BLOCK>(a.comb, agent, dsm_c);
+  if (threadIdx.x == 0) a.agent_done[agent] = 0u;
 }
 
 // Uneven batch: work items (agent, CTA-of-agent), longest horizons first.
@@ -468,15 +487,18 @@ __device__ __forceinline__ void rollout_work(const MppiRolloutArgs& a) {
 }
 
 // --------------------------------------------------------------------------
-// Combine: one CTA per agent.  Dynamic shared memory: scale[nblk] | u[H*m].
+// Combine of one agent by a CTA of CB threads: the combine kernel (one CTA
+// per agent) or, fused, the agent's last rollout CTA.  Shared memory at dsm:
+// scale[nblk] | u[H*m].  The partial records come from other CTAs of this or
+// the previous launch and are read through L2 (ld.global.cg).
 // --------------------------------------------------------------------------
 constexpr int kCombineBlock = 256;
 
-__device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
-  constexpr int NW = kCombineBlock / 32;
-  extern __shared__ __align__(16) float dsm[];
+template <int CB>
+__device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t agent,
+                                              float* dsm) {
+  constexpr int NW = CB / 32;
   __shared__ float red_s[3 * NW];
-  const uint32_t agent = blockIdx.x;
   const uint32_t tid = threadIdx.x;
   const bool ragged = a.agent_K != nullptr;
   const uint32_t K = ragged ? a.agent_K[agent] : a.K;
@@ -489,26 +511,26 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
   const float* P = a.partials + blk0 * ps;
 
   float lm = pos_inf();
-  for (uint32_t b = tid; b < nblk; b += kCombineBlock) lm = fminf(lm, P[(size_t)b * ps]);
+  for (uint32_t b = tid; b < nblk; b += CB) lm = fminf(lm, __ldcg(P + (size_t)b * ps));
   const float M = block_min<NW>(lm, red_s);
   float S = 0.0f, Q = 0.0f, C = 0.0f;
-  for (uint32_t b = tid; b < nblk; b += kCombineBlock) {
+  for (uint32_t b = tid; b < nblk; b += CB) {
     const float* pb = P + (size_t)b * ps;
-    const float sc = expf(-(pb[0] - M) / a.lambda);
+    const float sc = expf(-(__ldcg(pb) - M) / a.lambda);
     scale_s[b] = sc;
-    S = fmaf(sc, pb[1], S);
-    Q = fmaf(sc * sc, pb[2], Q);
-    C += pb[3];
+    S = fmaf(sc, __ldcg(pb + 1), S);
+    Q = fmaf(sc * sc, __ldcg(pb + 2), Q);
+    C += __ldcg(pb + 3);
   }
   block_sum3<NW>(S, Q, C, red_s);  // ends with a barrier: scale_s visible
 
   const float invS = 1.0f / S;
   float* un = a.u_nom + (size_t)agent * a.H * kM;  // agent stride: the largest horizon
   float* uo = a.u_out + (size_t)agent * a.H * kM;
-  for (uint32_t j = tid; j < HM; j += kCombineBlock) {
+  for (uint32_t j = tid; j < HM; j += CB) {
     float v = 0.0f;
     for (uint32_t b = 0; b < nblk; ++b)
-      v = fmaf(scale_s[b], P[(size_t)b * ps + MPPI_PARTIAL_HEAD + j], v);
+      v = fmaf(scale_s[b], __ldcg(P + (size_t)b * ps + MPPI_PARTIAL_HEAD + j), v);
     const uint32_t d = j % kM;
     const float u = clampf(un[j] + v * invS, a.u_min[d], a.u_max[d]);
     u_s[j] = u;
@@ -516,7 +538,7 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
   }
   if (a.hist_ustar) {
     float* hu = a.hist_ustar + ((size_t)a.step_local * a.num_agents + agent) * a.H * kM;
-    for (uint32_t j = tid; j < HM; j += kCombineBlock) hu[j] = u_s[j];
+    for (uint32_t j = tid; j < HM; j += CB) hu[j] = u_s[j];
   }
   if (tid == 0) {
     a.diag[agent * 3 + 0] = M;
@@ -573,7 +595,7 @@ __device__ __forceinline__ void combine_body(const MppiCombineArgs& a) {
     }
 #endif
   }
-  for (uint32_t j = tid; j < HM; j += kCombineBlock) {
+  for (uint32_t j = tid; j < HM; j += CB) {
     const uint32_t t = j / kM, d = j % kM;
     un[j] = (t + 1 < H) ? u_s[j + kM] : u_s[(H - 1) * kM + d];  // shift left, hold last
   }
@@ -602,7 +624,8 @@ extern "C" __global__ void __launch_bounds__(128, 4) mppi_rollout_work_b128(cons
 
 extern "C" __global__ void __launch_bounds__(mppi::kCombineBlock)
     mppi_combine(const MppiCombineArgs a) {
-  mppi::combine_body(a);
+  extern __shared__ __align__(16) float dsm[];
+  mppi::combine_agent<mppi::kCombineBlock>(a, blockIdx.x, dsm);
 }
 
 extern "C" __global__ void __launch_bounds__(256) mppi_weights(const MppiWeightsArgs a) {

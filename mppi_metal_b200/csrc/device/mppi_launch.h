@@ -12,6 +12,49 @@
 // [block min cost, sum e, sum e^2, sum cost].
 #define MPPI_PARTIAL_HEAD 4
 
+// One launch of the combine (+ optional propagate & shift) kernel.
+// Grid = num_agents, one CTA per agent.
+struct MppiCombineArgs {
+  uint32_t num_agents;
+  uint32_t K;
+  uint32_t H;
+  uint32_t nblk;
+  uint32_t pstride;
+  uint32_t step_local;  // history row written by the propagate stage
+  float lambda;
+  uint32_t propagate;   // 1: propagate x with u*[0], write history, shift u_nom
+  const uint32_t* step_base;
+  const float* partials;
+  const float* u_min;
+  const float* u_max;
+  const uint8_t* model_params;
+  uint64_t model_stride;
+  float* u_nom;        // [N][H*m] read; shifted in place when propagating
+  float* u_out;        // [N][H*m]
+  float* diag;         // [N][3]: best cost, mean cost, effective sample size
+  float* stats;        // [N][4]: min, sum e, sum e^2, sum cost (may be null)
+  float* x;            // [N][n] state, propagated in place
+  float* hist_states;  // [T][N][n] (may be null)
+  float* hist_controls;  // [T][N][m] (may be null)
+  float* hist_costs;   // [T][N] (may be null)
+  float* terminal;     // [N][n] (may be null)
+  // Uneven batches (null for a uniform batch): per-agent sample count,
+  // horizon and first partial record; `block` = rollout CTA size.
+  const uint32_t* agent_K;
+  const uint32_t* agent_H;
+  const uint32_t* agent_blk0;
+  uint32_t block;
+  uint32_t pad0;
+  float* hist_ustar;   // [T][N][H*m] the updated sequence u* of every step (may be null)
+  // Proposal features of the propagated state, for the next step's network
+  // (modules compiled with MPPI_FEATURES_FN; null = none).
+  const uint8_t* cost_params;
+  uint64_t cost_stride;
+  float* features;          // [N][feature_stride]
+  uint32_t feature_stride;  // <= MPPI_MAX_FEATURES
+  uint32_t pad1;
+};
+
 // One launch of the fused rollout kernel: every agent of the batch, every
 // sample of every agent.  Grid = (nblk, num_agents), one thread per sample.
 struct MppiRolloutArgs {
@@ -70,50 +113,15 @@ struct MppiRolloutArgs {
   float prop_ls_min;
   float prop_ls_max;
   uint32_t pad2;
+  // Combine fused into the rollout (uniform batches; null = the separate
+  // combine kernel runs).  Every CTA counts itself done in agent_done[agent]
+  // once its partial record is written; the last CTA of an agent runs that
+  // agent's combine with `comb` and sets the count back to zero, so the
+  // words are zero between launches.  No CTA waits for another.
+  uint32_t* agent_done;  // [N]
+  MppiCombineArgs comb;
 };
 
-// One launch of the combine (+ optional propagate & shift) kernel.
-// Grid = num_agents, one CTA per agent.
-struct MppiCombineArgs {
-  uint32_t num_agents;
-  uint32_t K;
-  uint32_t H;
-  uint32_t nblk;
-  uint32_t pstride;
-  uint32_t step_local;  // history row written by the propagate stage
-  float lambda;
-  uint32_t propagate;   // 1: propagate x with u*[0], write history, shift u_nom
-  const uint32_t* step_base;
-  const float* partials;
-  const float* u_min;
-  const float* u_max;
-  const uint8_t* model_params;
-  uint64_t model_stride;
-  float* u_nom;        // [N][H*m] read; shifted in place when propagating
-  float* u_out;        // [N][H*m]
-  float* diag;         // [N][3]: best cost, mean cost, effective sample size
-  float* stats;        // [N][4]: min, sum e, sum e^2, sum cost (may be null)
-  float* x;            // [N][n] state, propagated in place
-  float* hist_states;  // [T][N][n] (may be null)
-  float* hist_controls;  // [T][N][m] (may be null)
-  float* hist_costs;   // [T][N] (may be null)
-  float* terminal;     // [N][n] (may be null)
-  // Uneven batches (null for a uniform batch): per-agent sample count,
-  // horizon and first partial record; `block` = rollout CTA size.
-  const uint32_t* agent_K;
-  const uint32_t* agent_H;
-  const uint32_t* agent_blk0;
-  uint32_t block;
-  uint32_t pad0;
-  float* hist_ustar;   // [T][N][H*m] the updated sequence u* of every step (may be null)
-  // Proposal features of the propagated state, for the next step's network
-  // (modules compiled with MPPI_FEATURES_FN; null = none).
-  const uint8_t* cost_params;
-  uint64_t cost_stride;
-  float* features;          // [N][feature_stride]
-  uint32_t feature_stride;  // <= MPPI_MAX_FEATURES
-  uint32_t pad1;
-};
 
 // Proposal features of state rows: row r is a state of agent r % agents_mod
 // (its parameter blobs), out[r][0..out_stride) = the plugin's feature
