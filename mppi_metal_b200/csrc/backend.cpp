@@ -403,7 +403,7 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
   if (grew) ++b->generation;
   const void* k = b->ragged ? (const void*)b->mod->rollout_work
                             : (const void*)b->mod->rollout[b->geom.variant];
-  if (!b->ragged) b->geom.smem = std::max(b->geom.smem, combine_smem(b));
+  b->geom.smem = std::max(b->geom.smem, combine_smem(b));  // the fused combine reuses it
   if (b->geom.smem > 48 * 1024)
     CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem));
   if (!b->ragged) b->shape_key = key;
@@ -535,9 +535,9 @@ cudaError_t launch_proposal(mppi_backend* b) {
   return e == cudaSuccess ? launch_network(b) : e;
 }
 
-// The rollout kernel alone (the proposal's outputs already in place).
-cudaError_t launch_rollout_kernel(mppi_backend* b, uint32_t step_local) {
-  MppiRolloutArgs a = rollout_args(b, step_local);
+// A rollout launch with prepared arguments (uniform grid, or the uneven
+// batch's work items).
+cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a) {
   void* args[] = {&a};
   if (b->ragged) {
     if (b->grid) {
@@ -551,6 +551,12 @@ cudaError_t launch_rollout_kernel(mppi_backend* b, uint32_t step_local) {
   return cudaLaunchKernel((const void*)b->mod->rollout[b->geom.variant],
                           dim3(b->geom.nblk, b->N), dim3(b->geom.block), args, b->geom.smem,
                           b->stream);
+}
+
+// The rollout kernel alone (the proposal's outputs already in place).
+cudaError_t launch_rollout_kernel(mppi_backend* b, uint32_t step_local) {
+  MppiRolloutArgs a = rollout_args(b, step_local);
+  return launch_rollout_args(b, a);
 }
 
 // One rollout pass: the proposal's features and network first when one is
@@ -596,7 +602,7 @@ int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
   for (uint32_t rows : stage_options) {
     LaunchGeom g = base;
     g.stage_rows = rows;
-    g.smem = nominal_bytes(b) + 128 * 4 + (size_t)rows * 128 * el;
+    g.smem = std::max(nominal_bytes(b) + 128 * 4 + (size_t)rows * 128 * el, combine_smem(b));
     b->geom = g;
     CK(cudaFuncSetAttribute((const void*)b->mod->rollout_work,
                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem));
@@ -641,10 +647,10 @@ cudaError_t launch_combine(mppi_backend* b, uint32_t step_local, bool propagate)
                           combine_smem(b), b->stream);
 }
 
-bool fused_combine(const mppi_backend* b) { return b->fuse_combine && !b->ragged; }
+bool fused_combine(const mppi_backend* b) { return b->fuse_combine; }
 
 // One step's kernels after the proposal stage: the rollout with the combine
-// fused into it (uniform batches), or the rollout and combine kernels.
+// fused into it, or the rollout and combine kernels.
 cudaError_t launch_rollout_combine(mppi_backend* b, uint32_t step_local, bool propagate) {
   if (!fused_combine(b)) {
     cudaError_t e = launch_rollout_kernel(b, step_local);
@@ -653,10 +659,7 @@ cudaError_t launch_rollout_combine(mppi_backend* b, uint32_t step_local, bool pr
   MppiRolloutArgs a = rollout_args(b, step_local);
   a.agent_done = b->d_done.as<uint32_t>();
   a.comb = combine_args(b, step_local, propagate);
-  void* args[] = {&a};
-  return cudaLaunchKernel((const void*)b->mod->rollout[b->geom.variant],
-                          dim3(b->geom.nblk, b->N), dim3(b->geom.block), args, b->geom.smem,
-                          b->stream);
+  return launch_rollout_args(b, a);
 }
 
 // Resolves the parameter blob pointers of a run: per-agent blobs, an

@@ -442,27 +442,34 @@ template <int CB>
 __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t agent,
                                               float* dsm);
 
-// Uniform batch: grid (nblk, num_agents), every agent K samples, horizon H.
-// With a.agent_done the agent's last CTA to finish also runs its combine
-// (the "last block" pattern: every CTA publishes its partial record with a
-// device-scope fence before it counts itself done, so the CTA that sees the
-// count reach nblk reads every record complete; no CTA waits on another).
+// The combine fused into the rollout launch (a.agent_done set): after its
+// partial record, the CTA counts itself done for its agent, and the agent's
+// last CTA (the one that brings the count to nblk) runs the agent's combine
+// and resets the count.  The "last block" pattern: every CTA publishes its
+// record with a device-scope fence before it counts, so the last one reads
+// every record complete; no CTA waits on another.
 template <int BLOCK>
-__device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
-  const uint32_t agent = blockIdx.y, blk = blockIdx.x;
-  rollout_item<BLOCK>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
-                      a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
-  if (a.agent_done == nullptr) return;
+__device__ __forceinline__ void fused_combine_tail(const MppiRolloutArgs& a, uint32_t agent,
+                                                   uint32_t nblk) {
   __shared__ uint32_t last_s;
   __threadfence();  // this CTA's partial record (written by several threads)
   __syncthreads();  // ... complete, and the staging memory free for reuse
-  if (threadIdx.x == 0) last_s = atomicAdd(a.agent_done + agent, 1u) + 1u == a.nblk;
+  if (threadIdx.x == 0) last_s = atomicAdd(a.agent_done + agent, 1u) + 1u == nblk;
   __syncthreads();
   if (!last_s) return;
   __threadfence();  // the other CTAs' records, published before their counts
   extern __shared__ __align__(16) float dsm_c[];
   combine_agent<BLOCK>(a.comb, agent, dsm_c);
   if (threadIdx.x == 0) a.agent_done[agent] = 0u;
+}
+
+// Uniform batch: grid (nblk, num_agents), every agent K samples, horizon H.
+template <int BLOCK>
+__device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
+  const uint32_t agent = blockIdx.y, blk = blockIdx.x;
+  rollout_item<BLOCK>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
+                      a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
+  if (a.agent_done) fused_combine_tail<BLOCK>(a, agent, a.nblk);
 }
 
 // Uneven batch: work items (agent, CTA-of-agent), longest horizons first.
@@ -483,6 +490,7 @@ __device__ __forceinline__ void rollout_work(const MppiRolloutArgs& a) {
     rollout_item<BLOCK>(a, agent, blk, a.agent_K[agent], a.agent_H[agent],
                         a.u_nom + (size_t)agent * a.H * kM,
                         a.partials + ((size_t)a.agent_blk0[agent] + blk) * a.pstride);
+    if (a.agent_done) fused_combine_tail<BLOCK>(a, agent, (a.agent_K[agent] + BLOCK - 1) / BLOCK);
   }
 }
 
