@@ -170,6 +170,9 @@ struct mppi_backend {
   // Uniform batches run the combine inside the rollout launch (its agent's
   // last CTA); MPPI_B200_SEPARATE_COMBINE=1 keeps the separate combine kernel.
   bool fuse_combine = true;
+  // Uniform rollout launches (and the proposal network's) use programmatic
+  // dependent launch; MPPI_B200_NO_PDL=1 launches them plainly.
+  bool pdl = true;
   DevBuf d_hs, d_hc, d_hk, d_term;
   DevBuf d_agent_sigma, d_agent_mp, d_agent_cp;
   bool want_s = false, want_c = false, want_k = false, want_t = false;
@@ -526,13 +529,34 @@ cudaError_t launch_features(mppi_backend* b) {
 // The network's forward pass on the current features.
 cudaError_t launch_network(mppi_backend* b) {
   return mppi_b200::proposal_enqueue_forward(b->proposal, b->stream, b->d_feat.as<float>(),
-                                             kFeatureStride, b->N, b->d_prop.as<float>());
+                                             kFeatureStride, b->N, b->d_prop.as<float>(),
+                                             b->pdl);
 }
 
 // Features, then the network (both on the backend stream).
 cudaError_t launch_proposal(mppi_backend* b) {
   cudaError_t e = launch_features(b);
   return e == cudaSuccess ? launch_network(b) : e;
+}
+
+// A launch on the backend stream that may start while the previous kernel
+// finishes (programmatic stream serialisation): the kernel's CTAs run their
+// loop-constant prologue and then wait (griddepcontrol.wait) for the
+// previous grid to complete before they read anything it writes.
+cudaError_t launch_dependent(const mppi_backend* b, const void* func, dim3 grid, dim3 block,
+                             size_t smem, void** args) {
+  if (!b->pdl) return cudaLaunchKernel(func, grid, block, args, smem, b->stream);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = b->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelExC(&cfg, func, args);
 }
 
 // A rollout launch with prepared arguments (uniform grid, or the uneven
@@ -548,9 +572,8 @@ cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a) {
                             dim3(b->grid ? b->grid : b->num_work), dim3(128), args,
                             b->geom.smem, b->stream);
   }
-  return cudaLaunchKernel((const void*)b->mod->rollout[b->geom.variant],
-                          dim3(b->geom.nblk, b->N), dim3(b->geom.block), args, b->geom.smem,
-                          b->stream);
+  return launch_dependent(b, (const void*)b->mod->rollout[b->geom.variant],
+                          dim3(b->geom.nblk, b->N), dim3(b->geom.block), b->geom.smem, args);
 }
 
 // The rollout kernel alone (the proposal's outputs already in place).
@@ -838,6 +861,8 @@ int mppi_backend_create(mppi_backend** out) {
   if (*out) {
     const char* sep = getenv("MPPI_B200_SEPARATE_COMBINE");
     (*out)->fuse_combine = !(sep && *sep && *sep != '0');
+    const char* nopdl = getenv("MPPI_B200_NO_PDL");
+    (*out)->pdl = !(nopdl && *nopdl && *nopdl != '0');
   }
   return *out ? MPPI_OK : MPPI_ERR_INVALID;
 }

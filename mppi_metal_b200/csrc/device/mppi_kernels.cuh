@@ -102,6 +102,18 @@ typedef typename mppi_first_arg<decltype(&MPPI_TERMINAL_COST_FN)>::type TermStat
 
 __device__ __forceinline__ float pos_inf() { return __int_as_float(0x7f800000); }
 
+// Programmatic dependent launch (launches with the programmatic stream
+// serialisation attribute): a CTA lets the next kernel in the stream be
+// scheduled as soon as it has started, and the next kernel's CTAs run their
+// loop-constant prologue before they wait for this grid to complete and its
+// memory to be visible.  Both are no-ops in launches without the attribute.
+__device__ __forceinline__ void mppi_allow_dependent_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void mppi_grid_dependency_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // Element type of the shared-memory noise staging buffer.
 #if MPPI_NOISE_HALF
 typedef uint16_t stage_t;
@@ -270,21 +282,6 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
 #endif
   float* e_s = reinterpret_cast<float*>(stage_s + (size_t)a.stage_rows * BLOCK);
 
-  for (uint32_t i = tid; i < HM; i += BLOCK) un_s[i] = un_g[i];
-#if MPPI_PROPOSAL
-  // samples k < pcount draw around the network's predicted sequence; the
-  // shift and the scales live in shared memory, not in registers, so the
-  // rollout's register budget stays the plain kernel's
-  __shared__ float ps_s[kM];
-  const uint32_t pcount = a.prop_out ? a.prop_count : 0u;
-  if (pcount) {
-    const float* po = a.prop_out + (size_t)agent * a.prop_stride;
-    for (uint32_t i = tid; i < HM; i += BLOCK)
-      sh_s[i] = i < a.prop_ls_offset ? po[i] - un_g[i] : 0.0f;
-    if (tid < (uint32_t)kM)
-      ps_s[tid] = expf(clampf(po[a.prop_ls_offset + tid], a.prop_ls_min, a.prop_ls_max));
-  }
-#endif
   const uint8_t* mp_g = a.model_params + a.model_stride * agent;
   const uint8_t* cp_g = a.cost_params + a.cost_stride * agent;
 #if MPPI_MP_SMEM
@@ -309,6 +306,24 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
 #if MPPI_CONTROL_COST
   float sinv[kSig];
   load_sigma(a.sigma_inv + (size_t)a.sigma_inv_stride * agent, sinv);
+#endif
+  // Everything above is constant over a closed loop; the nominal, the state
+  // and the proposal's output below are written by the previous launches.
+  mppi_grid_dependency_wait();
+  for (uint32_t i = tid; i < HM; i += BLOCK) un_s[i] = un_g[i];
+#if MPPI_PROPOSAL
+  // samples k < pcount draw around the network's predicted sequence; the
+  // shift and the scales live in shared memory, not in registers, so the
+  // rollout's register budget stays the plain kernel's
+  __shared__ float ps_s[kM];
+  const uint32_t pcount = a.prop_out ? a.prop_count : 0u;
+  if (pcount) {
+    const float* po = a.prop_out + (size_t)agent * a.prop_stride;
+    for (uint32_t i = tid; i < HM; i += BLOCK)
+      sh_s[i] = i < a.prop_ls_offset ? po[i] - un_g[i] : 0.0f;
+    if (tid < (uint32_t)kM)
+      ps_s[tid] = expf(clampf(po[a.prop_ls_offset + tid], a.prop_ls_min, a.prop_ls_max));
+  }
 #endif
   __syncthreads();
 
@@ -466,6 +481,7 @@ __device__ __forceinline__ void fused_combine_tail(const MppiRolloutArgs& a, uin
 // Uniform batch: grid (nblk, num_agents), every agent K samples, horizon H.
 template <int BLOCK>
 __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
+  mppi_allow_dependent_launch();
   const uint32_t agent = blockIdx.y, blk = blockIdx.x;
   rollout_item<BLOCK>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
                       a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);

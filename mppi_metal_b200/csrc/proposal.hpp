@@ -25,9 +25,13 @@ ProposalShape proposal_shape(const mppi_proposal* p);
 
 // Enqueues the network's forward pass for `rows` feature rows on `stream`
 // (capturable into a CUDA graph): out[r][0..H*m) predicted u*, then m raw
-// log-scales.  Returns cudaSuccess or the launch error.
+// log-scales.  programmatic: launched with programmatic stream
+// serialisation, so it may start while the stream's previous kernel
+// finishes (it waits for that grid before it reads x).  Returns cudaSuccess
+// or the launch error.
 cudaError_t proposal_enqueue_forward(mppi_proposal* p, cudaStream_t stream, const float* x,
-                                     uint32_t x_stride, uint32_t rows, float* out);
+                                     uint32_t x_stride, uint32_t rows, float* out,
+                                     bool programmatic = false);
 
 // Reads and clears the device error word of the network's kernels (a
 // bounded wait that gave up).  False with a message when one is set.

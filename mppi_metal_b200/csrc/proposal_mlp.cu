@@ -520,6 +520,9 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
       w_pending = true;
     }
   }
+  // the features come from the previous kernel (programmatic launches run
+  // everything above while it finishes; a no-op otherwise)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   // input rows -> A[0] (every CTA stages the whole tile itself)
 #pragma unroll
   for (uint32_t j = grp; j < kIn / 16; j += kGroups) {
@@ -537,6 +540,11 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
     uint32_t col0, nc;
     cluster_slice(N, crank, col0, nc);
     const uint32_t buf = g & 1u;
+    // The next kernel (the rollout that reads this output) may be scheduled
+    // from the last layer on: it runs its loop-constant prologue meanwhile.
+    // Not earlier -- its CTAs would land on SMs still busy with the kernel
+    // before this one and crowd those that free up first.
+    if (g == 3) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const uint32_t a_in = a_s0 + buf * kSmemA;
     if (tid == 0) {
       // weights of this layer, then (past layer 0) the exchanged input tile
@@ -1081,7 +1089,8 @@ ProposalShape proposal_shape(const mppi_proposal* p) {
 }
 
 cudaError_t proposal_enqueue_forward(mppi_proposal* p, cudaStream_t stream, const float* x,
-                                     uint32_t x_stride, uint32_t rows, float* out) {
+                                     uint32_t x_stride, uint32_t rows, float* out,
+                                     bool programmatic) {
   if (rows == 0) return cudaSuccess;
   FusedArgs f{};
   for (int l = 0; l < 4; ++l) {
@@ -1102,8 +1111,24 @@ cudaError_t proposal_enqueue_forward(mppi_proposal* p, cudaStream_t stream, cons
   f.hm = p->hm;
   f.m = p->cfg.control_dim;
   f.train = 0;
-  mlp_forward_cluster_kernel<<<(f.mp / kTile) * kCluster, kCThreads, kClusterSmem, stream>>>(f);
-  return cudaGetLastError();
+  if (!programmatic) {
+    mlp_forward_cluster_kernel<<<(f.mp / kTile) * kCluster, kCThreads, kClusterSmem, stream>>>(f);
+    return cudaGetLastError();
+  }
+  // may start while the previous kernel finishes: the kernel sets up TMEM,
+  // barriers, biases and the first weights, then waits for that grid before
+  // it reads the features
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((f.mp / kTile) * kCluster);
+  cfg.blockDim = dim3(kCThreads);
+  cfg.dynamicSmemBytes = kClusterSmem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, mlp_forward_cluster_kernel, f);
 }
 
 bool proposal_check_device_error(mppi_proposal* p, std::string* msg) {
