@@ -170,6 +170,8 @@ struct mppi_backend {
   // Uniform batches run the combine inside the rollout launch (its agent's
   // last CTA); MPPI_B200_SEPARATE_COMBINE=1 keeps the separate combine kernel.
   bool fuse_combine = true;
+  bool use_fused = false;     // the form chosen for combine_key's launch shape
+  std::string combine_key;
   // Uniform rollout launches (and the proposal network's) use programmatic
   // dependent launch; MPPI_B200_NO_PDL=1 launches them plainly.
   bool pdl = true;
@@ -342,6 +344,22 @@ LaunchGeom choose_geometry(const mppi_backend* b) {
 
 size_t combine_smem(const mppi_backend* b);
 
+// Dynamic shared memory limit of the current rollout kernels (plain and
+// fused forms) for the prepared geometry.
+cudaError_t set_rollout_smem(const mppi_backend* b) {
+  if (b->geom.smem <= 48 * 1024) return cudaSuccess;
+  const void* k[2] = {b->ragged ? (const void*)b->mod->rollout_work
+                                : (const void*)b->mod->rollout[b->geom.variant],
+                      b->ragged ? (const void*)b->mod->rollout_work_fused
+                                : (const void*)b->mod->rollout_fused[b->geom.variant]};
+  for (const void* f : k) {
+    cudaError_t e =
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool wk, bool wt,
                  char* err, size_t err_len) {
   bool grew = false;
@@ -404,11 +422,8 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
   CK(b->h_up.ensure((b->off_uout() + 64) * 4 + 2 * pad16(b->mp_size + b->cp_size) + 64));
   CK(b->h_down.ensure((b->io_floats() + 64) * 4));
   if (grew) ++b->generation;
-  const void* k = b->ragged ? (const void*)b->mod->rollout_work
-                            : (const void*)b->mod->rollout[b->geom.variant];
   b->geom.smem = std::max(b->geom.smem, combine_smem(b));  // the fused combine reuses it
-  if (b->geom.smem > 48 * 1024)
-    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem));
+  CK(set_rollout_smem(b));
   if (!b->ragged) b->shape_key = key;
   return MPPI_OK;
 }
@@ -563,16 +578,19 @@ cudaError_t launch_dependent(const mppi_backend* b, const void* func, dim3 grid,
 // batch's work items).
 cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a) {
   void* args[] = {&a};
+  const bool fused = a.agent_done != nullptr;
   if (b->ragged) {
     if (b->grid) {
       cudaError_t e = cudaMemsetAsync(b->d_queue.p, 0, 4, b->stream);
       if (e != cudaSuccess) return e;
     }
-    return cudaLaunchKernel((const void*)b->mod->rollout_work,
+    return cudaLaunchKernel(fused ? (const void*)b->mod->rollout_work_fused
+                                  : (const void*)b->mod->rollout_work,
                             dim3(b->grid ? b->grid : b->num_work), dim3(128), args,
                             b->geom.smem, b->stream);
   }
-  return launch_dependent(b, (const void*)b->mod->rollout[b->geom.variant],
+  return launch_dependent(b, fused ? (const void*)b->mod->rollout_fused[b->geom.variant]
+                                   : (const void*)b->mod->rollout[b->geom.variant],
                           dim3(b->geom.nblk, b->N), dim3(b->geom.block), b->geom.smem, args);
 }
 
@@ -653,6 +671,7 @@ int tune_ragged(mppi_backend* b, char* err, size_t err_len) {
   b->tuned_grid = best_grid;
   CK(cudaFuncSetAttribute((const void*)b->mod->rollout_work,
                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)best_g.smem));
+  CK(set_rollout_smem(b));
   return MPPI_OK;
 }
 
@@ -670,12 +689,13 @@ cudaError_t launch_combine(mppi_backend* b, uint32_t step_local, bool propagate)
                           combine_smem(b), b->stream);
 }
 
-bool fused_combine(const mppi_backend* b) { return b->fuse_combine; }
+bool fused_combine(const mppi_backend* b) { return b->fuse_combine && b->use_fused; }
 
-// One step's kernels after the proposal stage: the rollout with the combine
-// fused into it, or the rollout and combine kernels.
-cudaError_t launch_rollout_combine(mppi_backend* b, uint32_t step_local, bool propagate) {
-  if (!fused_combine(b)) {
+// One step's kernels after the proposal stage in either form: the rollout
+// with the combine run by each agent's last CTA (mppi_rollout_fused_*), or
+// the rollout and combine kernels.
+cudaError_t launch_step_form(mppi_backend* b, uint32_t step_local, bool propagate, bool fused) {
+  if (!fused) {
     cudaError_t e = launch_rollout_kernel(b, step_local);
     return e == cudaSuccess ? launch_combine(b, step_local, propagate) : e;
   }
@@ -683,6 +703,55 @@ cudaError_t launch_rollout_combine(mppi_backend* b, uint32_t step_local, bool pr
   a.agent_done = b->d_done.as<uint32_t>();
   a.comb = combine_args(b, step_local, propagate);
   return launch_rollout_args(b, a);
+}
+
+cudaError_t launch_rollout_combine(mppi_backend* b, uint32_t step_local, bool propagate) {
+  return launch_step_form(b, step_local, propagate, fused_combine(b));
+}
+
+// Chooses the form of a step for the prepared launch shape by timing both
+// (after a warm-up, three steps each -- the proposal stage first when a
+// network is attached, as in the loop -- without propagation so no state
+// changes), once per shape, as the uneven-batch tuner does.  The two forms
+// compute the same bits; the fused one saves the combine launch, but its
+// combine tail can cost a model's rollout registers (spills), so neither
+// wins everywhere.  MPPI_B200_FUSED_COMBINE=1 takes the fused form untimed.
+int decide_combine(mppi_backend* b, char* err, size_t err_len) {
+  if (!b->fuse_combine) {
+    b->use_fused = false;
+    return MPPI_OK;
+  }
+  char kb[192];
+  snprintf(kb, sizeof(kb), "%u/%u/%u/%d/%u/%u/%u/%u/%p/%p/%u/%d/", b->N, b->K, b->H,
+           b->geom.variant, b->geom.block, b->geom.stage_rows, b->geom.nblk, b->grid,
+           (const void*)b->mod.get(), (const void*)b->proposal, b->prop_samples, (int)b->ragged);
+  const std::string key = std::string(kb) + (b->ragged ? b->tuned_key : std::string());
+  if (b->combine_key == key) return MPPI_OK;
+  if (const char* f = getenv("MPPI_B200_FUSED_COMBINE"); f && *f && *f != '0') {
+    b->use_fused = true;
+    b->combine_key = key;
+    return MPPI_OK;
+  }
+  CK(set_rollout_smem(b));
+  float t[2] = {0.0f, 0.0f};
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int form = 0; form < 2; ++form) {
+      const int reps = pass ? 3 : 1;
+      CK(cudaEventRecord(b->ev0, b->stream));
+      for (int i = 0; i < reps; ++i) {
+        if (b->proposal && b->spec.proposal) CK(launch_proposal(b));
+        CK(launch_step_form(b, 0, false, form == 1));
+      }
+      CK(cudaEventRecord(b->ev1, b->stream));
+      CK(cudaEventSynchronize(b->ev1));
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+      if (pass) t[form] = ms;
+    }
+  }
+  b->use_fused = t[1] <= t[0];
+  b->combine_key = key;
+  return MPPI_OK;
 }
 
 // Resolves the parameter blob pointers of a run: per-agent blobs, an
@@ -808,14 +877,15 @@ int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
       // prepare() re-derived the default geometry; restore the tuned one
       b->geom = b->tuned_geom;
       b->grid = b->tuned_grid;
-      CK(cudaFuncSetAttribute((const void*)b->mod->rollout_work,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem));
+      CK(set_rollout_smem(b));
     }
   }
+  if (int rc = decide_combine(b, err, err_len)) return rc;
   const std::string key = std::string(keybuf) + (b->ragged ? "/r" + std::to_string(b->grid) + "/" +
                                                                  std::to_string(b->geom.stage_rows) +
                                                                  "/" + b->tuned_key
-                                                           : std::string());
+                                                           : std::string()) +
+                          (fused_combine(b) ? "/fused" : "/separate");
   if (b->graph == nullptr || b->graph_key != key) {
     if (b->graph) {
       cudaGraphExecDestroy(b->graph);
@@ -1062,6 +1132,7 @@ int mppi_backend_dispatch_rollout(mppi_backend* b, uint64_t step_index, const fl
   const bool mo = mp && mp_bytes, co = cp && cp_bytes;
   if (mo) CK(b->d_mp_ovr.ensure(pad16(b->mp_size)));
   if (co) CK(b->d_cp_ovr.ensure(pad16(b->cp_size)));
+  if (int rc = decide_combine(b, err, err_len)) return rc;
   stage_upload(b, step_index, x0, u_nominal, mp, mp_bytes, cp, cp_bytes);
   float* down = b->h_down.as<float>();
   const size_t nd = b->off_stats() - b->off_uout();
@@ -1070,7 +1141,7 @@ int mppi_backend_dispatch_rollout(mppi_backend* b, uint64_t step_index, const fl
   // captured once per (buffers, parameter pointers, module) and replayed:
   // one launch per control step instead of four or five API calls.
   char keybuf[256];
-  snprintf(keybuf, sizeof(keybuf), "%llu/%p/%p/%d%d/%p/%u/%p/%p/%p",
+  snprintf(keybuf, sizeof(keybuf), "%d/%llu/%p/%p/%d%d/%p/%u/%p/%p/%p", (int)fused_combine(b),
            (unsigned long long)b->generation, (const void*)b->run_mp, (const void*)b->run_cp,
            mo, co, (const void*)b->proposal, b->prop_samples, (const void*)b->mod.get(),
            b->h_up.p, b->h_down.p);

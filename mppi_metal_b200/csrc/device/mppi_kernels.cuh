@@ -22,6 +22,8 @@
 // Kernels (extern "C" names are looked up by the backend):
 //   mppi_rollout_b{64,128,256}  fused rollout + per-CTA softmax partials +
 //                               weighted-noise partial sums
+//   mppi_rollout_fused_b{...}   the same + each agent's combine in its last CTA
+//   mppi_rollout_work[_fused]_b128  the same for uneven batches (work items)
 //   mppi_combine                per-agent combine -> u_out, diagnostics,
 //                               optional propagate & shift (closed loop)
 //   mppi_weights                normalised weights (inspection only)
@@ -479,19 +481,21 @@ __device__ __forceinline__ void fused_combine_tail(const MppiRolloutArgs& a, uin
 }
 
 // Uniform batch: grid (nblk, num_agents), every agent K samples, horizon H.
-template <int BLOCK>
+// FUSED: the kernel form with the combine tail (a separate entry point, so
+// the plain form keeps its register allocation).
+template <int BLOCK, bool FUSED>
 __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   mppi_allow_dependent_launch();
   const uint32_t agent = blockIdx.y, blk = blockIdx.x;
   rollout_item<BLOCK>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
                       a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
-  if (a.agent_done) fused_combine_tail<BLOCK>(a, agent, a.nblk);
+  if (FUSED && a.agent_done) fused_combine_tail<BLOCK>(a, agent, a.nblk);
 }
 
 // Uneven batch: work items (agent, CTA-of-agent), longest horizons first.
 // A persistent grid pulls items from an atomic queue (no CTA ever waits on
 // another); without a queue each CTA runs item blockIdx.x.
-template <int BLOCK>
+template <int BLOCK, bool FUSED>
 __device__ __forceinline__ void rollout_work(const MppiRolloutArgs& a) {
   __shared__ uint32_t item_s;
   for (uint32_t pass = 0;; ++pass) {
@@ -506,7 +510,8 @@ __device__ __forceinline__ void rollout_work(const MppiRolloutArgs& a) {
     rollout_item<BLOCK>(a, agent, blk, a.agent_K[agent], a.agent_H[agent],
                         a.u_nom + (size_t)agent * a.H * kM,
                         a.partials + ((size_t)a.agent_blk0[agent] + blk) * a.pstride);
-    if (a.agent_done) fused_combine_tail<BLOCK>(a, agent, (a.agent_K[agent] + BLOCK - 1) / BLOCK);
+    if (FUSED && a.agent_done)
+      fused_combine_tail<BLOCK>(a, agent, (a.agent_K[agent] + BLOCK - 1) / BLOCK);
   }
 }
 
@@ -521,8 +526,7 @@ constexpr int kCombineBlock = 256;
 template <int CB>
 __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t agent,
                                               float* dsm) {
-  constexpr int NW = CB / 32;
-  __shared__ float red_s[3 * NW];
+  __shared__ float stat_s[4];
   const uint32_t tid = threadIdx.x;
   const bool ragged = a.agent_K != nullptr;
   const uint32_t K = ragged ? a.agent_K[agent] : a.K;
@@ -534,26 +538,42 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   float* u_s = dsm + ((a.nblk + 3) & ~3u);  // a.nblk: the largest agent's CTA count
   const float* P = a.partials + blk0 * ps;
 
-  float lm = pos_inf();
-  for (uint32_t b = tid; b < nblk; b += CB) lm = fminf(lm, __ldcg(P + (size_t)b * ps));
-  const float M = block_min<NW>(lm, red_s);
-  float S = 0.0f, Q = 0.0f, C = 0.0f;
-  for (uint32_t b = tid; b < nblk; b += CB) {
-    const float* pb = P + (size_t)b * ps;
-    const float sc = expf(-(__ldcg(pb) - M) / a.lambda);
-    scale_s[b] = sc;
-    S = fmaf(sc, __ldcg(pb + 1), S);
-    Q = fmaf(sc * sc, __ldcg(pb + 2), Q);
-    C += __ldcg(pb + 3);
+  // Statistics over the CTA records by warp 0 alone (lane l takes records
+  // l, l + 32, ...), so the summation order -- and every bit of the result --
+  // is the same whichever CTA size runs the combine.
+  if (tid < 32) {
+    float lm = pos_inf();
+    for (uint32_t b = tid; b < nblk; b += 32) lm = fminf(lm, __ldcg(P + (size_t)b * ps));
+    const float Mw = warp_min(lm);
+    float S = 0.0f, Q = 0.0f, C = 0.0f;
+    for (uint32_t b = tid; b < nblk; b += 32) {
+      const float* pb = P + (size_t)b * ps;
+      const float sc = expf(-(__ldcg(pb) - Mw) / a.lambda);
+      scale_s[b] = sc;
+      S = fmaf(sc, __ldcg(pb + 1), S);
+      Q = fmaf(sc * sc, __ldcg(pb + 2), Q);
+      C += __ldcg(pb + 3);
+    }
+    S = warp_sum(S);
+    Q = warp_sum(Q);
+    C = warp_sum(C);
+    if (tid == 0) {
+      stat_s[0] = Mw;
+      stat_s[1] = S;
+      stat_s[2] = Q;
+      stat_s[3] = C;
+    }
   }
-  block_sum3<NW>(S, Q, C, red_s);  // ends with a barrier: scale_s visible
+  __syncthreads();  // statistics and scale_s visible
+  const float M = stat_s[0], S = stat_s[1], Q = stat_s[2], C = stat_s[3];
 
   const float invS = 1.0f / S;
   float* un = a.u_nom + (size_t)agent * a.H * kM;  // agent stride: the largest horizon
   float* uo = a.u_out + (size_t)agent * a.H * kM;
   for (uint32_t j = tid; j < HM; j += CB) {
     float v = 0.0f;
-    for (uint32_t b = 0; b < nblk; ++b)
+#pragma unroll 8
+    for (uint32_t b = 0; b < nblk; ++b)  // in record order: loads run ahead of the sum
       v = fmaf(scale_s[b], __ldcg(P + (size_t)b * ps + MPPI_PARTIAL_HEAD + j), v);
     const uint32_t d = j % kM;
     const float u = clampf(un[j] + v * invS, a.u_min[d], a.u_max[d]);
@@ -630,10 +650,17 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
 // Residency is bounded by the noise staging buffer (H*m floats per thread),
 // not by registers: 512 resident threads per SM lets the compiler use up to
 // 128 registers for instruction-level parallelism.
+// mppi_rollout_fused_b<B> carries the combine tail (MppiRolloutArgs::
+// agent_done); the backend times both forms on a new shape and keeps the
+// faster -- the tail's extra live state can cost some models registers.
 #define MPPI_ROLLOUT_ENTRY(B)                                                      \
   extern "C" __global__ void __launch_bounds__(B, 512 / B)                        \
       mppi_rollout_b##B(const MppiRolloutArgs a) {                                \
-    mppi::rollout_body<B>(a);                                                     \
+    mppi::rollout_body<B, false>(a);                                              \
+  }                                                                               \
+  extern "C" __global__ void __launch_bounds__(B, 512 / B)                        \
+      mppi_rollout_fused_b##B(const MppiRolloutArgs a) {                          \
+    mppi::rollout_body<B, true>(a);                                               \
   }
 MPPI_ROLLOUT_ENTRY(64)
 MPPI_ROLLOUT_ENTRY(128)
@@ -643,7 +670,11 @@ MPPI_ROLLOUT_ENTRY(256)
 // CTAs -- and therefore every floating-point sum -- does not depend on the
 // tuned grid size or staging mode.
 extern "C" __global__ void __launch_bounds__(128, 4) mppi_rollout_work_b128(const MppiRolloutArgs a) {
-  mppi::rollout_work<128>(a);
+  mppi::rollout_work<128, false>(a);
+}
+extern "C" __global__ void __launch_bounds__(128, 4)
+    mppi_rollout_work_fused_b128(const MppiRolloutArgs a) {
+  mppi::rollout_work<128, true>(a);
 }
 
 extern "C" __global__ void __launch_bounds__(mppi::kCombineBlock)

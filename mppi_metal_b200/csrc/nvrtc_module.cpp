@@ -8,6 +8,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <dirent.h>
 #include <fstream>
@@ -266,26 +267,37 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
                                                                          : MPPI_ERR_CUDA;
   }
   const char* names[3] = {"mppi_rollout_b64", "mppi_rollout_b128", "mppi_rollout_b256"};
+  const char* fused_names[3] = {"mppi_rollout_fused_b64", "mppi_rollout_fused_b128",
+                                "mppi_rollout_fused_b256"};
   for (int i = 0; i < 3; ++i) {
     ce = cudaLibraryGetKernel(&mod->rollout[i], mod->library, names[i]);
+    if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->rollout_fused[i], mod->library,
+                                                     fused_names[i]);
     if (ce != cudaSuccess) break;
   }
   if (ce == cudaSuccess)
     ce = cudaLibraryGetKernel(&mod->rollout_work, mod->library, "mppi_rollout_work_b128");
+  if (ce == cudaSuccess)
+    ce = cudaLibraryGetKernel(&mod->rollout_work_fused, mod->library,
+                              "mppi_rollout_work_fused_b128");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->combine, mod->library, "mppi_combine");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->weights, mod->library, "mppi_weights");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->noise, mod->library, "mppi_noise");
   if (ce == cudaSuccess && !spec.features.empty())
     ce = cudaLibraryGetKernel(&mod->features, mod->library, "mppi_features");
   for (int i = 0; i < 3 && ce == cudaSuccess; ++i) {
-    cudaFuncAttributes fa{};
+    cudaFuncAttributes fa{}, ff{};
     ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout[i]));
-    mod->rollout_static_smem[i] = fa.sharedSizeBytes;
+    if (ce == cudaSuccess)
+      ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_fused[i]));
+    mod->rollout_static_smem[i] = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
   }
   if (ce == cudaSuccess) {
-    cudaFuncAttributes fa{};
+    cudaFuncAttributes fa{}, ff{};
     ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout_work));
-    mod->work_static_smem = fa.sharedSizeBytes;
+    if (ce == cudaSuccess)
+      ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_work_fused));
+    mod->work_static_smem = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
   }
   if (ce != cudaSuccess) {
     *error = std::string("Required library kernel missing from the module: ") +

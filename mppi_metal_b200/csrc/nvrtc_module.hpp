@@ -41,12 +41,16 @@ struct KernelModule {
   cudaLibrary_t library = nullptr;
   cudaKernel_t rollout[3] = {nullptr, nullptr, nullptr};
   cudaKernel_t rollout_work = nullptr;  // uneven batches (128-thread CTAs)
+  // the same with each agent's combine run by its last CTA
+  cudaKernel_t rollout_fused[3] = {nullptr, nullptr, nullptr};
+  cudaKernel_t rollout_work_fused = nullptr;
   cudaKernel_t combine = nullptr;
   cudaKernel_t weights = nullptr;
   cudaKernel_t noise = nullptr;
   cudaKernel_t features = nullptr;  // only when ModuleSpec::features is set
-  // static shared memory of the rollout kernels (their dynamic share is
-  // sized so that this plus the dynamic part keeps the target residency)
+  // static shared memory of the rollout kernels, the larger of the plain and
+  // fused forms (their dynamic share is sized so that this plus the dynamic
+  // part keeps the target residency)
   size_t rollout_static_smem[3] = {0, 0, 0};
   size_t work_static_smem = 0;
   std::string build_log;  // NVRTC log of the compile (warnings, ptxas info)

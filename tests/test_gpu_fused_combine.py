@@ -1,9 +1,11 @@
 """The combine fused into the rollout launch (each agent's last rollout CTA
 runs the agent's weighted update, diagnostics, propagate and shift) against
-the separate combine kernel (MPPI_B200_SEPARATE_COMBINE=1, read when a
-backend is created): closed loops of uniform batches, uneven batches and a
-proposal closed loop give the same bits, and a single step's u_next and
-diagnostics are the same too."""
+the separate combine kernel: closed loops of uniform batches (up to 157
+rollout CTAs per agent, past one CTA's worth of records) and of uneven
+batches give the same bits, and so do a single step's u_next and
+diagnostics.  The backend picks the form per launch shape by timing;
+MPPI_B200_FUSED_COMBINE=1 / MPPI_B200_SEPARATE_COMBINE=1 (read when a
+backend is created) pin it here."""
 from __future__ import annotations
 
 import os
@@ -17,17 +19,26 @@ from mppi_metal_b200 import models
 pytestmark = pytest.mark.gpu
 
 
-def _separate(fn):
-    """Runs fn() with backends created under MPPI_B200_SEPARATE_COMBINE=1."""
-    old = os.environ.get("MPPI_B200_SEPARATE_COMBINE")
-    os.environ["MPPI_B200_SEPARATE_COMBINE"] = "1"
+def _with_env(name, fn):
+    old = os.environ.get(name)
+    os.environ[name] = "1"
     try:
         return fn()
     finally:
         if old is None:
-            del os.environ["MPPI_B200_SEPARATE_COMBINE"]
+            del os.environ[name]
         else:
-            os.environ["MPPI_B200_SEPARATE_COMBINE"] = old
+            os.environ[name] = old
+
+
+def _separate(fn):
+    """Runs fn() with backends that use the separate combine kernel."""
+    return _with_env("MPPI_B200_SEPARATE_COMBINE", fn)
+
+
+def _fused(fn):
+    """Runs fn() with backends that use the fused form, untimed."""
+    return _with_env("MPPI_B200_FUSED_COMBINE", fn)
 
 
 def _uniform_loop(w):
@@ -45,13 +56,15 @@ def _assert_same(r1, r2):
             assert np.array_equal(r1[key], r2[key]), key
 
 
-@pytest.mark.parametrize("K", [1000, 4096])
-def test_fused_combine_matches_separate_uniform(K):
-    w = models.unicycle_batch(seed=21, N=24, K=K, H=20, T=12)
-    fused, kf = _uniform_loop(w)
+@pytest.mark.parametrize("N,K", [(24, 1000), (24, 4096), (3, 20000)])
+def test_fused_combine_matches_separate_uniform(N, K):
+    w = models.unicycle_batch(seed=21, N=N, K=K, H=20, T=12)
+    fused, kf = _fused(lambda: _uniform_loop(w))
     sep, ks = _separate(lambda: _uniform_loop(w))
     assert kf == 1 and ks == 2
     _assert_same(fused, sep)
+    auto, _ = _uniform_loop(w)  # the timed choice, either form: the same bits
+    _assert_same(auto, sep)
 
 
 def test_fused_combine_matches_separate_uneven():
@@ -65,7 +78,7 @@ def test_fused_combine_matches_separate_uneven():
         b.close()
         return r
 
-    _assert_same(run(), _separate(run))
+    _assert_same(_fused(run), _separate(run))
 
 
 def test_fused_combine_matches_separate_single_step():
@@ -79,5 +92,5 @@ def test_fused_combine_matches_separate_single_step():
         b.close()
         return out
 
-    (u1, d1), (u2, d2) = step(), _separate(step)
+    (u1, d1), (u2, d2) = _fused(step), _separate(step)
     assert np.array_equal(u1, u2) and np.array_equal(d1, d2)
