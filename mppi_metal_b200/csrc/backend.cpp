@@ -170,7 +170,10 @@ struct mppi_backend {
   // Uniform batches run the combine inside the rollout launch (its agent's
   // last CTA); MPPI_B200_SEPARATE_COMBINE=1 keeps the separate combine kernel.
   bool fuse_combine = true;
-  bool use_fused = false;     // the form chosen for combine_key's launch shape
+  // MPPI_B200_FUSED_COMBINE=1 / MPPI_B200_WS=1 or 0 pin the step form's
+  // combine and warp-specialisation choices (0 = timed)
+  int combine_pin = 0, ws_pin = 0;
+  uint32_t form = 0;          // for combine_key's launch shape: kFormFused | kFormWs
   std::string combine_key;
   // Uniform rollout launches (and the proposal network's) use programmatic
   // dependent launch; MPPI_B200_NO_PDL=1 launches them plainly.
@@ -356,6 +359,13 @@ cudaError_t set_rollout_smem(const mppi_backend* b) {
     cudaError_t e =
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem);
     if (e != cudaSuccess) return e;
+  }
+  if (!b->ragged) {
+    for (const void* f : {(const void*)b->mod->rollout_ws, (const void*)b->mod->rollout_ws_fused}) {
+      cudaError_t e =
+          cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem);
+      if (e != cudaSuccess) return e;
+    }
   }
   return cudaSuccess;
 }
@@ -576,9 +586,14 @@ cudaError_t launch_dependent(const mppi_backend* b, const void* func, dim3 grid,
 
 // A rollout launch with prepared arguments (uniform grid, or the uneven
 // batch's work items).
-cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a) {
+cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a, bool ws = false) {
   void* args[] = {&a};
   const bool fused = a.agent_done != nullptr;
+  if (ws && !b->ragged)
+    return launch_dependent(b, fused ? (const void*)b->mod->rollout_ws_fused
+                                     : (const void*)b->mod->rollout_ws,
+                            dim3(b->geom.nblk, b->N), dim3(2 * b->geom.block), b->geom.smem,
+                            args);
   if (b->ragged) {
     if (b->grid) {
       cudaError_t e = cudaMemsetAsync(b->d_queue.p, 0, 4, b->stream);
@@ -689,67 +704,86 @@ cudaError_t launch_combine(mppi_backend* b, uint32_t step_local, bool propagate)
                           combine_smem(b), b->stream);
 }
 
-bool fused_combine(const mppi_backend* b) { return b->fuse_combine && b->use_fused; }
+constexpr uint32_t kFormFused = 1;  // combine run by each agent's last rollout CTA
+constexpr uint32_t kFormWs = 2;     // warp-specialised rollout (noise drawn by extra warps)
 
-// One step's kernels after the proposal stage in either form: the rollout
-// with the combine run by each agent's last CTA (mppi_rollout_fused_*), or
-// the rollout and combine kernels.
-cudaError_t launch_step_form(mppi_backend* b, uint32_t step_local, bool propagate, bool fused) {
-  if (!fused) {
-    cudaError_t e = launch_rollout_kernel(b, step_local);
-    return e == cudaSuccess ? launch_combine(b, step_local, propagate) : e;
-  }
+bool fused_combine(const mppi_backend* b) { return (b->form & kFormFused) != 0; }
+
+// The warp-specialised rollout needs 128-sample CTAs with the whole horizon
+// staged, in a uniform batch.
+bool ws_possible(const mppi_backend* b) {
+  return !b->ragged && b->geom.block == 128 && b->geom.stage_rows >= b->HM();
+}
+
+// One step's kernels after the proposal stage in the given form: the rollout
+// (plain or warp-specialised) with the combine run by each agent's last CTA,
+// or the rollout and combine kernels.
+cudaError_t launch_step_form(mppi_backend* b, uint32_t step_local, bool propagate,
+                             uint32_t form) {
   MppiRolloutArgs a = rollout_args(b, step_local);
-  a.agent_done = b->d_done.as<uint32_t>();
-  a.comb = combine_args(b, step_local, propagate);
-  return launch_rollout_args(b, a);
+  if (form & kFormFused) {
+    a.agent_done = b->d_done.as<uint32_t>();
+    a.comb = combine_args(b, step_local, propagate);
+    return launch_rollout_args(b, a, (form & kFormWs) != 0);
+  }
+  cudaError_t e = launch_rollout_args(b, a, (form & kFormWs) != 0);
+  return e == cudaSuccess ? launch_combine(b, step_local, propagate) : e;
 }
 
 cudaError_t launch_rollout_combine(mppi_backend* b, uint32_t step_local, bool propagate) {
-  return launch_step_form(b, step_local, propagate, fused_combine(b));
+  return launch_step_form(b, step_local, propagate, b->form);
 }
 
-// Chooses the form of a step for the prepared launch shape by timing both
-// (after a warm-up, three steps each -- the proposal stage first when a
-// network is attached, as in the loop -- without propagation so no state
-// changes), once per shape, as the uneven-batch tuner does.  The two forms
-// compute the same bits; the fused one saves the combine launch, but its
-// combine tail can cost a model's rollout registers (spills), so neither
-// wins everywhere.  MPPI_B200_FUSED_COMBINE=1 takes the fused form untimed.
+// Chooses the form of a step for the prepared launch shape -- combine fused
+// into the rollout or not, warp-specialised rollout or not -- by timing the
+// candidates (after a warm-up, three steps each, the proposal stage first
+// when a network is attached, as in the loop; without propagation, so no
+// state changes), once per shape, as the uneven-batch tuner does.  Every form
+// computes the same bits.  The fused combine saves a launch but its tail can
+// cost a model's rollout registers; the warp-specialised rollout shortens
+// each sample's chain where few CTAs leave SMs idle, and only costs
+// instructions where the SMs are full -- so neither choice wins everywhere.
 int decide_combine(mppi_backend* b, char* err, size_t err_len) {
-  if (!b->fuse_combine) {
-    b->use_fused = false;
-    return MPPI_OK;
-  }
   char kb[192];
   snprintf(kb, sizeof(kb), "%u/%u/%u/%d/%u/%u/%u/%u/%p/%p/%u/%d/", b->N, b->K, b->H,
            b->geom.variant, b->geom.block, b->geom.stage_rows, b->geom.nblk, b->grid,
            (const void*)b->mod.get(), (const void*)b->proposal, b->prop_samples, (int)b->ragged);
   const std::string key = std::string(kb) + (b->ragged ? b->tuned_key : std::string());
   if (b->combine_key == key) return MPPI_OK;
-  if (const char* f = getenv("MPPI_B200_FUSED_COMBINE"); f && *f && *f != '0') {
-    b->use_fused = true;
-    b->combine_key = key;
-    return MPPI_OK;
-  }
-  CK(set_rollout_smem(b));
-  float t[2] = {0.0f, 0.0f};
-  for (int pass = 0; pass < 2; ++pass) {
-    for (int form = 0; form < 2; ++form) {
-      const int reps = pass ? 3 : 1;
-      CK(cudaEventRecord(b->ev0, b->stream));
-      for (int i = 0; i < reps; ++i) {
-        if (b->proposal && b->spec.proposal) CK(launch_proposal(b));
-        CK(launch_step_form(b, 0, false, form == 1));
-      }
-      CK(cudaEventRecord(b->ev1, b->stream));
-      CK(cudaEventSynchronize(b->ev1));
-      float ms = 0.0f;
-      CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
-      if (pass) t[form] = ms;
+  std::vector<uint32_t> forms;
+  for (uint32_t ws : {0u, kFormWs}) {
+    if (ws && (b->ws_pin < 0 || !ws_possible(b))) continue;
+    if (!ws && b->ws_pin > 0 && ws_possible(b)) continue;
+    for (uint32_t fu : {0u, kFormFused}) {
+      if (fu && b->combine_pin < 0) continue;
+      if (!fu && b->combine_pin > 0) continue;
+      forms.push_back(ws | fu);
     }
   }
-  b->use_fused = t[1] <= t[0];
+  uint32_t best = forms.front();
+  if (forms.size() > 1) {
+    CK(set_rollout_smem(b));
+    float best_ms = 1e30f;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (uint32_t f : forms) {
+        const int reps = pass ? 3 : 1;
+        CK(cudaEventRecord(b->ev0, b->stream));
+        for (int i = 0; i < reps; ++i) {
+          if (b->proposal && b->spec.proposal) CK(launch_proposal(b));
+          CK(launch_step_form(b, 0, false, f));
+        }
+        CK(cudaEventRecord(b->ev1, b->stream));
+        CK(cudaEventSynchronize(b->ev1));
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+        if (pass && ms < best_ms) {
+          best_ms = ms;
+          best = f;
+        }
+      }
+    }
+  }
+  b->form = best;
   b->combine_key = key;
   return MPPI_OK;
 }
@@ -885,7 +919,7 @@ int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
                                                                  std::to_string(b->geom.stage_rows) +
                                                                  "/" + b->tuned_key
                                                            : std::string()) +
-                          (fused_combine(b) ? "/fused" : "/separate");
+                          "/form" + std::to_string(b->form);
   if (b->graph == nullptr || b->graph_key != key) {
     if (b->graph) {
       cudaGraphExecDestroy(b->graph);
@@ -933,6 +967,10 @@ int mppi_backend_create(mppi_backend** out) {
     (*out)->fuse_combine = !(sep && *sep && *sep != '0');
     const char* nopdl = getenv("MPPI_B200_NO_PDL");
     (*out)->pdl = !(nopdl && *nopdl && *nopdl != '0');
+    const char* fc = getenv("MPPI_B200_FUSED_COMBINE");
+    if (fc && *fc && *fc != '0') (*out)->combine_pin = 1;
+    if (!(*out)->fuse_combine) (*out)->combine_pin = -1;
+    if (const char* ws = getenv("MPPI_B200_WS"); ws && *ws) (*out)->ws_pin = *ws == '0' ? -1 : 1;
   }
   return *out ? MPPI_OK : MPPI_ERR_INVALID;
 }
@@ -1141,7 +1179,7 @@ int mppi_backend_dispatch_rollout(mppi_backend* b, uint64_t step_index, const fl
   // captured once per (buffers, parameter pointers, module) and replayed:
   // one launch per control step instead of four or five API calls.
   char keybuf[256];
-  snprintf(keybuf, sizeof(keybuf), "%d/%llu/%p/%p/%d%d/%p/%u/%p/%p/%p", (int)fused_combine(b),
+  snprintf(keybuf, sizeof(keybuf), "%u/%llu/%p/%p/%d%d/%p/%u/%p/%p/%p", b->form,
            (unsigned long long)b->generation, (const void*)b->run_mp, (const void*)b->run_cp,
            mo, co, (const void*)b->proposal, b->prop_samples, (const void*)b->mod.get(),
            b->h_up.p, b->h_down.p);

@@ -24,6 +24,8 @@
 //                               weighted-noise partial sums
 //   mppi_rollout_fused_b{...}   the same + each agent's combine in its last CTA
 //   mppi_rollout_work[_fused]_b128  the same for uneven batches (work items)
+//   mppi_rollout_ws[_fused]_b128    warp-specialised form (noise drawn by a
+//                               second set of warps one chunk ahead)
 //   mppi_combine                per-agent combine -> u_out, diagnostics,
 //                               optional propagate & shift (closed loop)
 //   mppi_weights                normalised weights (inspection only)
@@ -249,12 +251,24 @@ __device__ __forceinline__ void copy_words(uint32_t* dst, const uint8_t* src, in
 // horizon H, nominal at un_g, partial record at part).  One thread per
 // sample.  Dynamic shared memory: u_nom[H*m] | staging[stage_rows][BLOCK] |
 // e[BLOCK] (sized for the launch's largest horizon).
+//
+// WS (warp-specialised form, 2 * BLOCK threads, whole horizon staged): the
+// second BLOCK threads draw the noise of sample column tid - BLOCK a chunk of
+// kWsChunk steps ahead while the first BLOCK threads run the state
+// recurrence of the previous chunk; one CTA barrier hands each chunk over.
+// Each sample's chain then carries only the dynamics and costs -- for launches
+// whose few CTAs leave SMs idle (latency-bound), not for full ones.  The
+// extra warps add exact zeros (and +inf to the minimum) to the CTA
+// statistics, so the results are the same bits as the plain form.
 // --------------------------------------------------------------------------
-template <int BLOCK>
+constexpr uint32_t kWsChunk = 4;
+
+template <int BLOCK, bool WS = false>
 __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t agent,
                                              uint32_t blk, uint32_t K, uint32_t H,
                                              const float* un_g, float* part) {
-  constexpr int NW = BLOCK / 32;
+  constexpr int NT = WS ? 2 * BLOCK : BLOCK;  // threads of the CTA
+  constexpr int NW = NT / 32;
   constexpr int PER_LANE = BLOCK / 32;
   extern __shared__ __align__(16) float dsm[];
   __shared__ float red_s[3 * NW];
@@ -267,8 +281,10 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
 
   const uint32_t tid = threadIdx.x;
   const uint32_t lane = tid & 31, warp = tid >> 5;
+  const bool producer = WS && tid >= (uint32_t)BLOCK;  // noise-drawing warp (WS form)
+  const uint32_t col = WS ? tid % BLOCK : tid;         // this thread's sample column
   const uint32_t HM = H * kM;
-  const uint32_t k = blk * BLOCK + tid;
+  const uint32_t k = blk * BLOCK + col;
   const bool active = k < K;
   const uint32_t step = *a.step_base + a.step_local;
   const uint32_t key = a.seed + agent;
@@ -312,7 +328,7 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   // Everything above is constant over a closed loop; the nominal, the state
   // and the proposal's output below are written by the previous launches.
   mppi_grid_dependency_wait();
-  for (uint32_t i = tid; i < HM; i += BLOCK) un_s[i] = un_g[i];
+  for (uint32_t i = tid; i < HM; i += NT) un_s[i] = un_g[i];
 #if MPPI_PROPOSAL
   // samples k < pcount draw around the network's predicted sequence; the
   // shift and the scales live in shared memory, not in registers, so the
@@ -321,7 +337,7 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   const uint32_t pcount = a.prop_out ? a.prop_count : 0u;
   if (pcount) {
     const float* po = a.prop_out + (size_t)agent * a.prop_stride;
-    for (uint32_t i = tid; i < HM; i += BLOCK)
+    for (uint32_t i = tid; i < HM; i += NT)
       sh_s[i] = i < a.prop_ls_offset ? po[i] - un_g[i] : 0.0f;
     if (tid < (uint32_t)kM)
       ps_s[tid] = expf(clampf(po[a.prop_ls_offset + tid], a.prop_ls_min, a.prop_ls_max));
@@ -338,75 +354,108 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   // sums, so neither phase needs a barrier.
   float J = 0.0f;
   __align__(16) float st[kNPad];
-  if (active) {
+  const bool runs = active && !producer;  // this thread runs a sample's recurrence
+  if (runs) {
     const float* xg = a.x + (size_t)agent * kN;
 #pragma unroll
     for (int d = 0; d < kN; ++d) st[d] = xg[d];
   }
 #pragma unroll
   for (int d = kN; d < kNPad; ++d) st[d] = 0.0f;
-  const uint32_t TC = staged ? H : a.stage_rows / kM;
-  for (uint32_t t0 = 0; t0 < H; t0 += TC) {
-    const uint32_t t1 = min(H, t0 + TC);
-    const uint32_t row0 = staged ? 0u : t0;  // staging row of step t is (t - row0) * m + d
-#pragma unroll 4
-    for (uint32_t t = t0; t < t1; ++t) {
-      float n[2 * kP], eps[kM];
-      if (active) {
-        sample_noise(step, key, k, H, t, sig, n, eps);
-        MPPI_PROPOSAL_EPS();
-      } else {
-#pragma unroll
-        for (int d = 0; d < kM; ++d) eps[d] = 0.0f;
-      }
-#pragma unroll
-      for (int d = 0; d < kM; ++d)
-        stage_s[(size_t)((t - row0) * kM + d) * BLOCK + tid] = to_stage(eps[d]);
-    }
+  // Noise of step t into this thread's staging column (row (t - row0) * m + d).
+  auto draw = [&](uint32_t t, uint32_t row0) {
+    float n[2 * kP], eps[kM];
     if (active) {
-      for (uint32_t t = t0; t < t1; ++t) {
-        float eps[kM], u[kM];
+      sample_noise(step, key, k, H, t, sig, n, eps);
+      MPPI_PROPOSAL_EPS();
+    } else {
 #pragma unroll
-        for (int d = 0; d < kM; ++d) {
-          eps[d] = from_stage(stage_s[(size_t)((t - row0) * kM + d) * BLOCK + tid]);
-          u[d] = clampf(un_s[t * kM + d] + eps[d], lo[d], hi[d]);
-        }
+      for (int d = 0; d < kM; ++d) eps[d] = 0.0f;
+    }
+#pragma unroll
+    for (int d = 0; d < kM; ++d)
+      stage_s[(size_t)((t - row0) * kM + d) * BLOCK + col] = to_stage(eps[d]);
+  };
+  // One step of the recurrence on the staged noise.
+  auto advance = [&](uint32_t t, uint32_t row0) {
+    float eps[kM], u[kM];
+#pragma unroll
+    for (int d = 0; d < kM; ++d) {
+      eps[d] = from_stage(stage_s[(size_t)((t - row0) * kM + d) * BLOCK + col]);
+      u[d] = clampf(un_s[t * kM + d] + eps[d], lo[d], hi[d]);
+    }
 #if MPPI_CONTROL_COST
-        {
-          float cc = 0.0f;
+    {
+      float cc = 0.0f;
 #if MPPI_COV_FULL
 #pragma unroll
-          for (int i = 0; i < kM; ++i) {
-            float r = 0.0f;
+      for (int i = 0; i < kM; ++i) {
+        float r = 0.0f;
 #pragma unroll
-            for (int j = 0; j < kM; ++j) r = fmaf(sinv[i * kM + j], eps[j], r);
-            cc = fmaf(un_s[t * kM + i], r, cc);
-          }
+        for (int j = 0; j < kM; ++j) r = fmaf(sinv[i * kM + j], eps[j], r);
+        cc = fmaf(un_s[t * kM + i], r, cc);
+      }
 #else
 #pragma unroll
-          for (int i = 0; i < kM; ++i) cc = fmaf(un_s[t * kM + i], sinv[i] * eps[i], cc);
+      for (int i = 0; i < kM; ++i) cc = fmaf(un_s[t * kM + i], sinv[i] * eps[i], cc);
 #endif
-          J = fmaf(a.lambda, cc, J);
+      J = fmaf(a.lambda, cc, J);
+    }
+#endif
+    MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u, mp,
+                     make_uint2(step, mppi_dyn_ctr(k, H, kP, t)), key);
+    J += MPPI_STAGE_COST_FN(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u, mp,
+                            cp);
+  };
+  if constexpr (WS) {
+    if (staged) {
+      // producers stay one chunk ahead; the barrier after each chunk makes
+      // the next chunk's rows visible to the recurrence warps
+      if (producer)
+        for (uint32_t t = 0; t < min(H, kWsChunk); ++t) draw(t, 0u);
+      __syncthreads();
+      for (uint32_t c0 = 0; c0 < H; c0 += kWsChunk) {
+        if (producer) {
+          const uint32_t n0 = c0 + kWsChunk, n1 = min(H, n0 + kWsChunk);
+#pragma unroll 4
+          for (uint32_t t = n0; t < n1; ++t) draw(t, 0u);
+        } else if (runs) {
+          const uint32_t c1 = min(H, c0 + kWsChunk);
+          for (uint32_t t = c0; t < c1; ++t) advance(t, 0u);
         }
-#endif
-        MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u, mp,
-                         make_uint2(step, mppi_dyn_ctr(k, H, kP, t)), key);
-        J += MPPI_STAGE_COST_FN(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u,
-                                mp, cp);
+        __syncthreads();
       }
+    } else {
+      J = __int_as_float(0x7fc00000);  // the host never runs this form chunked: NaN marks it
+    }
+  } else {
+    // Time is processed in chunks of TC steps (the whole horizon when the
+    // staging buffer holds it).  Phase A draws the chunk's noise into this
+    // thread's own staging column: Philox chains of different steps are
+    // independent, so they overlap.  Phase B runs the state recurrence,
+    // reading the noise back.  No thread touches another's column until the
+    // weighted sums, so neither phase needs a barrier.
+    const uint32_t TC = staged ? H : a.stage_rows / kM;
+    for (uint32_t t0 = 0; t0 < H; t0 += TC) {
+      const uint32_t t1 = min(H, t0 + TC);
+      const uint32_t row0 = staged ? 0u : t0;
+#pragma unroll 4
+      for (uint32_t t = t0; t < t1; ++t) draw(t, row0);
+      if (runs)
+        for (uint32_t t = t0; t < t1; ++t) advance(t, row0);
     }
   }
-  if (active) {
+  if (runs) {
     J += MPPI_TERMINAL_COST_FN(reinterpret_cast<TermStateT>(reinterpret_cast<void*>(st)), mp, cp);
     if (a.costs) a.costs[(size_t)agent * a.K + k] = J;  // agent stride: the largest K
   }
 
   // ---- CTA softmax statistics against the CTA minimum ----
-  const float bmin = block_min<NW>(active ? J : pos_inf(), red_s);
-  const float e = active ? expf(-(J - bmin) / a.lambda) : 0.0f;
-  float s_e = e, s_e2 = e * e, s_c = active ? J : 0.0f;
+  const float bmin = block_min<NW>(runs ? J : pos_inf(), red_s);
+  const float e = runs ? expf(-(J - bmin) / a.lambda) : 0.0f;
+  float s_e = e, s_e2 = e * e, s_c = runs ? J : 0.0f;
   block_sum3<NW>(s_e, s_e2, s_c, red_s);
-  e_s[tid] = e;
+  if (!producer) e_s[col] = e;
   if (tid == 0) {
     part[0] = bmin;
     part[1] = s_e;
@@ -427,19 +476,8 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
       // regenerate this chunk's noise (same counters, same values)
       __syncthreads();
       const uint32_t t0 = r0 / kM, t1 = (r0 + rows) / kM;
-      for (uint32_t t = t0; t < t1; ++t) {
-        float n[2 * kP], eps[kM];
-        if (active) {
-          sample_noise(step, key, k, H, t, sig, n, eps);
-          MPPI_PROPOSAL_EPS();
-        } else {
-#pragma unroll
-          for (int d = 0; d < kM; ++d) eps[d] = 0.0f;
-        }
-#pragma unroll
-        for (int d = 0; d < kM; ++d)
-          stage_s[(size_t)((t - t0) * kM + d) * BLOCK + tid] = to_stage(eps[d]);
-      }
+      if (!producer)
+        for (uint32_t t = t0; t < t1; ++t) draw(t, t0);
       __syncthreads();
     } else {
       base = stage_s + (size_t)r0 * BLOCK;
@@ -483,13 +521,13 @@ __device__ __forceinline__ void fused_combine_tail(const MppiRolloutArgs& a, uin
 // Uniform batch: grid (nblk, num_agents), every agent K samples, horizon H.
 // FUSED: the kernel form with the combine tail (a separate entry point, so
 // the plain form keeps its register allocation).
-template <int BLOCK, bool FUSED>
+template <int BLOCK, bool FUSED, bool WS = false>
 __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   mppi_allow_dependent_launch();
   const uint32_t agent = blockIdx.y, blk = blockIdx.x;
-  rollout_item<BLOCK>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
-                      a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
-  if (FUSED && a.agent_done) fused_combine_tail<BLOCK>(a, agent, a.nblk);
+  rollout_item<BLOCK, WS>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
+                          a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
+  if (FUSED && a.agent_done) fused_combine_tail<WS ? 2 * BLOCK : BLOCK>(a, agent, a.nblk);
 }
 
 // Uneven batch: work items (agent, CTA-of-agent), longest horizons first.
@@ -665,6 +703,16 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
 MPPI_ROLLOUT_ENTRY(64)
 MPPI_ROLLOUT_ENTRY(128)
 MPPI_ROLLOUT_ENTRY(256)
+
+// Warp-specialised forms for 128-sample CTAs (256 threads: 128 running the
+// recurrence, 128 drawing the noise ahead), whole horizon staged.
+extern "C" __global__ void __launch_bounds__(256, 2) mppi_rollout_ws_b128(const MppiRolloutArgs a) {
+  mppi::rollout_body<128, false, true>(a);
+}
+extern "C" __global__ void __launch_bounds__(256, 2)
+    mppi_rollout_ws_fused_b128(const MppiRolloutArgs a) {
+  mppi::rollout_body<128, true, true>(a);
+}
 
 // Uneven batches always use 128-thread CTAs, so the partition of samples into
 // CTAs -- and therefore every floating-point sum -- does not depend on the

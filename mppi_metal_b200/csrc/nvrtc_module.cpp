@@ -280,6 +280,9 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
   if (ce == cudaSuccess)
     ce = cudaLibraryGetKernel(&mod->rollout_work_fused, mod->library,
                               "mppi_rollout_work_fused_b128");
+  if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->rollout_ws, mod->library, "mppi_rollout_ws_b128");
+  if (ce == cudaSuccess)
+    ce = cudaLibraryGetKernel(&mod->rollout_ws_fused, mod->library, "mppi_rollout_ws_fused_b128");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->combine, mod->library, "mppi_combine");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->weights, mod->library, "mppi_weights");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->noise, mod->library, "mppi_noise");
@@ -291,6 +294,13 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
     if (ce == cudaSuccess)
       ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_fused[i]));
     mod->rollout_static_smem[i] = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
+  }
+  if (ce == cudaSuccess) {
+    cudaFuncAttributes fa{}, ff{};
+    ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout_ws));
+    if (ce == cudaSuccess)
+      ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_ws_fused));
+    mod->ws_static_smem = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
   }
   if (ce == cudaSuccess) {
     cudaFuncAttributes fa{}, ff{};

@@ -44,6 +44,10 @@ struct KernelModule {
   // the same with each agent's combine run by its last CTA
   cudaKernel_t rollout_fused[3] = {nullptr, nullptr, nullptr};
   cudaKernel_t rollout_work_fused = nullptr;
+  // warp-specialised 128-sample forms (256 threads), plain and fused
+  cudaKernel_t rollout_ws = nullptr;
+  cudaKernel_t rollout_ws_fused = nullptr;
+  size_t ws_static_smem = 0;
   cudaKernel_t combine = nullptr;
   cudaKernel_t weights = nullptr;
   cudaKernel_t noise = nullptr;

@@ -3,9 +3,11 @@ runs the agent's weighted update, diagnostics, propagate and shift) against
 the separate combine kernel: closed loops of uniform batches (up to 157
 rollout CTAs per agent, past one CTA's worth of records) and of uneven
 batches give the same bits, and so do a single step's u_next and
-diagnostics.  The backend picks the form per launch shape by timing;
-MPPI_B200_FUSED_COMBINE=1 / MPPI_B200_SEPARATE_COMBINE=1 (read when a
-backend is created) pin it here."""
+diagnostics.  The same holds for the warp-specialised rollout (a second set
+of warps draws the noise ahead), with either combine.  The backend picks the
+form per launch shape by timing; MPPI_B200_FUSED_COMBINE=1 /
+MPPI_B200_SEPARATE_COMBINE=1 and MPPI_B200_WS=1 / 0 (read when a backend is
+created) pin it here."""
 from __future__ import annotations
 
 import os
@@ -39,6 +41,11 @@ def _separate(fn):
 def _fused(fn):
     """Runs fn() with backends that use the fused form, untimed."""
     return _with_env("MPPI_B200_FUSED_COMBINE", fn)
+
+
+def _ws(fn):
+    """Runs fn() with backends that use the warp-specialised rollout."""
+    return _with_env("MPPI_B200_WS", fn)
 
 
 def _uniform_loop(w):
@@ -93,4 +100,30 @@ def test_fused_combine_matches_separate_single_step():
         return out
 
     (u1, d1), (u2, d2) = _fused(step), _separate(step)
+    assert np.array_equal(u1, u2) and np.array_equal(d1, d2)
+
+
+@pytest.mark.parametrize("N,K,H", [(24, 1000, 20), (3, 20000, 20), (8, 256, 64)])
+def test_warp_specialised_rollout_matches_plain(N, K, H):
+    w = models.unicycle_batch(seed=22, N=N, K=K, H=H, T=8)
+    plain, _ = _separate(lambda: _uniform_loop(w))
+    ws_sep, _ = _ws(lambda: _separate(lambda: _uniform_loop(w)))
+    ws_fused, kf = _ws(lambda: _fused(lambda: _uniform_loop(w)))
+    assert kf == 1
+    _assert_same(ws_sep, plain)
+    _assert_same(ws_fused, plain)
+
+
+def test_warp_specialised_single_step_matches_plain():
+    w = models.unicycle_single(seed=3, K=1024, H=30)
+    x0 = np.array([0.5, -1.0, 0.2, 0.0], np.float32)
+    u_nom = np.linspace(-0.2, 0.3, w.horizon * w.control_dim).astype(np.float32)
+
+    def step():
+        b = backend_for(w)
+        out = b.dispatch_rollout(4, x0, u_nom)
+        b.close()
+        return out
+
+    (u1, d1), (u2, d2) = _ws(lambda: _fused(step)), _separate(step)
     assert np.array_equal(u1, u2) and np.array_equal(d1, d2)
