@@ -14,11 +14,11 @@
 //               with the loss (Gaussian NLL of u*) and three more GEMMs for
 //               the activation gradients dH = dZ W, saving for the weight
 //               gradients dZ^T and H^T (batch-contiguous images).
-//   mlp_forward_cluster   inference: a cluster of 4 CTAs per 128 rows, each
-//               computing a quarter of every layer's output columns and
+//   mlp_forward_cluster   inference: a cluster of 8 CTAs per 128 rows, each
+//               computing an eighth of every layer's output columns and
 //               broadcasting its slice of the activations into the other
-//               CTAs' shared memory (DSMEM), so the epilogues and weight
-//               loads of one tile are spread over 4 SMs.
+//               CTAs' shared memory (DSMEM), so the MMAs, epilogues and
+//               weight loads of one tile are spread over 8 SMs.
 //   mlp_wgrad   dW_l = dZ_l^T H_{l-1} summed over the batch: split over
 //               batch chunks, a 4-stage bulk-copy ring feeding the MMAs,
 //               FP32 atomics into the gradient.
@@ -406,14 +406,14 @@ __global__ void __launch_bounds__(kFusedThreads, 1) mlp_fused_kernel(const Fused
 }
 
 // ---------------------------------------------------------------------------
-// mlp_forward_cluster: inference, 4 CTAs (one cluster) per 128-row tile
+// mlp_forward_cluster: inference, 8 CTAs (one cluster) per 128-row tile
 // ---------------------------------------------------------------------------
-constexpr uint32_t kCluster = 4;
+constexpr uint32_t kCluster = 8;
 constexpr uint32_t kCThreads = kTile * kGroups;        // 512
-constexpr uint32_t kCSmemW = 64 * kHid * 2;            // this CTA's weight rows (<= 64)
+constexpr uint32_t kCSmemW = 32 * kHid * 2;            // this CTA's weight rows (<= 32)
 constexpr uint32_t kBiasFloats = 3 * kHid + kHid;       // b0..b2 and b3 (<= 256)
 constexpr uint32_t kClusterSmem = 2 * kSmemA + kCSmemW + kSmemBar + kBiasFloats * 4;
-constexpr uint32_t kCTmemCols = 64;
+constexpr uint32_t kCTmemCols = 32;
 static_assert(kClusterSmem <= 232448, "cluster kernel exceeds the shared-memory limit");
 
 __device__ __forceinline__ uint32_t cluster_rank() {
@@ -432,7 +432,8 @@ __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
-// 16-column chunks of an N-wide layer dealt to the cluster's CTAs.
+// 16-column chunks of an N-wide layer dealt to the cluster's CTAs (the MMA's
+// N is a multiple of 16): 32 columns each of a 256-wide hidden layer.
 __device__ __forceinline__ void cluster_slice(uint32_t N, uint32_t c, uint32_t& col0,
                                               uint32_t& ncols) {
   const uint32_t chunks = N / 16, q = chunks / kCluster, rem = chunks % kCluster;
@@ -461,7 +462,7 @@ __device__ __forceinline__ void st_async_v4(uint32_t addr, uint4 v, uint32_t mba
 // Activations ping-pong between two A tiles, each with its own "full"
 // mbarrier: layer g reads A[g % 2]; its epilogue stores the CTA's column
 // slice of the next activations into its own A[(g + 1) % 2] with plain
-// stores and into the three peers' with st.async, completing 48 KB per layer
+// stores and into the seven peers' with st.async, completing 56 KB per layer
 // on each receiver's full barrier, which the receiver arms (arrive.expect_tx)
 // and waits on before its next MMA.  Reuse is safe by causality: a CTA writes A[(g + 1) % 2] of a peer
 // only after its own MMA g, which needed that peer's slice of layer g's
@@ -613,39 +614,36 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kCThreads, 1)
       const uint32_t nbuf = (g + 1) & 1u;
       const uint32_t off = a_s0 + nbuf * kSmemA;
       const uint32_t full = bar_full0 + 8 * nbuf;
-      for (uint32_t j = grp; j < nc / 16; j += kGroups) {
-        float v[16];
-        tc::tmem_ld16(t_row + 16 * j, v);
+      // 8-column pieces: a warp's 32 rows x 8 columns, one 16-byte core-matrix
+      // row (8 BF16) per thread, so all four warps of a lane quarter work
+      for (uint32_t j = grp; j < nc / 8; j += kGroups) {
+        float v[8];
+        tc::tmem_ld8(t_row + 8 * j, v);
 #pragma unroll
-        for (int i = 0; i < 16; ++i) v[i] = gelu(v[i] + bias[16 * j + i]);
-        const uint4 lo = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]),
+        for (int i = 0; i < 8; ++i) v[i] = gelu(v[i] + bias[8 * j + i]);
+        const uint4 h8 = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]),
                                     pack2(v[6], v[7]));
-        const uint4 hi = make_uint4(pack2(v[8], v[9]), pack2(v[10], v[11]), pack2(v[12], v[13]),
-                                    pack2(v[14], v[15]));
-        const uint32_t dst = off + 2 * canon(r, col0 + 16 * j, kHid);
+        const uint32_t dst = off + 2 * canon(r, col0 + 8 * j, kHid);
         // this CTA's own slice by plain local stores (made visible to the
         // tensor core by the proxy fence and barrier at the next layer's
         // start), the peers' copies by remote asynchronous stores
-        st_shared_v4(dst, lo);
-        st_shared_v4(dst + 128, hi);
+        st_shared_v4(dst, h8);
 #pragma unroll
         for (uint32_t q = 1; q < kCluster; ++q) {
           const uint32_t peer = (crank + q) % kCluster;
-          const uint32_t rd = map_to_rank(dst, peer), rb = map_to_rank(full, peer);
-          st_async_v4(rd, lo, rb);
-          st_async_v4(rd + 128, hi, rb);
+          st_async_v4(map_to_rank(dst, peer), h8, map_to_rank(full, peer));
         }
       }
     } else if (ok) {
       // output layer: this CTA's columns straight to global memory
       const float* bias = bias_s + 3 * kHid + col0;
-      for (uint32_t j = grp; j < nc / 16; j += kGroups) {
-        float v[16];
-        tc::tmem_ld16(t_row + 16 * j, v);
+      for (uint32_t j = grp; j < nc / 8; j += kGroups) {
+        float v[8];
+        tc::tmem_ld8(t_row + 8 * j, v);
         if (valid) {
-          float* o = a.out + (size_t)row * a.out_stride + col0 + 16 * j;
+          float* o = a.out + (size_t)row * a.out_stride + col0 + 8 * j;
 #pragma unroll
-          for (int i = 0; i < 16; ++i) o[i] = v[i] + bias[16 * j + i];
+          for (int i = 0; i < 8; ++i) o[i] = v[i] + bias[8 * j + i];
         }
       }
     }
