@@ -51,10 +51,10 @@ L2_FLUSH_BYTES = 256 << 20
 # issue-rate roofline.
 ROLLOUT_COUNTERS = {
     # workload: (warp-inst per rollout-step, DRAM bytes per launch)
-    "batch": (509501440 / 52428800, 238336),          # 9.72
-    "uneven": (186096022 / 16410677, 123136),         # 11.34
-    "single": (255224 / 30720, 40960),                # 8.31
-    "quadrotor/fp32": (7108453214 / 209715200, 487168),   # 33.90
+    "batch": (496386048 / 52428800, 237568),          # 9.47
+    "uneven": (178922783 / 16410677, 122880),         # 10.90
+    "single": (247536 / 30720, 39680),                # 8.06
+    "quadrotor/fp32": (6911910084 / 209715200, 153088),   # 32.96
     "quadrotor/mixed": (6401390457 / 209715200, 124416),  # 30.52
 }
 

@@ -201,6 +201,11 @@ int mppi_device_philox(uint64_t n, const uint32_t* ctr0, const uint32_t* ctr1,
 int mppi_device_sincos(uint64_t n, const float* x, int quarter, float* sin_out,
                        float* cos_out, char* err, size_t err_len);
 
+/* The library's own natural logarithm (mppi_log, used by Box-Muller) on the
+ * device, for accuracy tests; no counterpart in the reference.  Arguments are
+ * normal positive floats. */
+int mppi_device_log(uint64_t n, const float* x, float* out, char* err, size_t err_len);
+
 /* ---- allocation-free control step --------------------------------------
  * No counterpart in the reference.  For callers that must not allocate
  * device memory once running (a fixed-rate control loop, where cudaMalloc /

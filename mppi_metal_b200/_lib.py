@@ -125,6 +125,7 @@ SIGNATURES = {
                                  + [ctypes.POINTER(c_f32)]),
     "mppi_device_philox": (ctypes.c_int, [c_u64, c_ptr, c_ptr, c_ptr, c_ptr] + _ERR),
     "mppi_device_sincos": (ctypes.c_int, [c_u64, c_ptr, ctypes.c_int, c_ptr, c_ptr] + _ERR),
+    "mppi_device_log": (ctypes.c_int, [c_u64, c_ptr, c_ptr] + _ERR),
     "mppi_backend_dispatch_rollout_noalloc": (ctypes.c_int, [c_ptr, c_u64, c_ptr, c_ptr, c_ptr,
                                                              c_ptr, c_ptr, c_ptr] + _ERR),
     "mppi_backend_set_features": (ctypes.c_int, [c_ptr, ctypes.c_char_p, c_u32] + _ERR),

@@ -316,6 +316,16 @@ def device_sincos(x, quarter: bool = False):
     return s, c
 
 
+def device_log(x):
+    """ln x by the library's own device function (mppi_log)."""
+    lib = _lib.load()
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.zeros_like(x)
+    eb = _lib.err_buf()
+    _check(lib.mppi_device_log(x.size, _p(x), _p(out), eb, len(eb)), eb)
+    return out
+
+
 def compile_check(plugin: str, state_dim: int, control_dim: int, cov_full: bool = False,
                   control_cost: bool = False, stage_cost: str = "mppi_stage_cost",
                   terminal_cost: str = "mppi_terminal_cost", dynamics: str = "mppi_dynamics",

@@ -1,6 +1,6 @@
 """Derives the polynomial coefficients of the library's own sine / cosine
-(mppi_prelude.cuh: mppi_sincos_quarter, mppi_sincosf) and checks the error of
-the float32 evaluation the device performs.
+and natural logarithm (mppi_prelude.cuh: mppi_sincos_quarter, mppi_sincosf,
+mppi_log) and checks the error of the float32 evaluation the device performs.
 
     python mppi_metal_b200/csrc/device/derive_poly.py
 
@@ -12,7 +12,9 @@ The printed errors come from evaluating the rounded coefficients the way the
 device does (float32 FMA Horner steps, emulated exactly through float64
 products) against numpy's float64 sin / cos.
 
-Two families:
+Three families:
+  logarithm:     ln x = e ln 2 + f + f^2 * P(f), x = 2^e (1 + f), f in [-1/3, 1/3)
+                 (the exponent is split off around 2/3 so that f is exact)
   quarter-turn:  s(f) = sin(pi/2 f) = f * S(f^2),  c(f) = cos(pi/2 f) = C(f^2)
                  for f in [-1/2, 1/2] (Box-Muller's angle 2 pi u = pi/2 (q + f))
   radians:       sin(r) = r + r^3 * S(r^2),  cos(r) = 1 + r^2 * C(r^2)
@@ -94,6 +96,46 @@ def fit_radians():
     return [f32(x) for x in cs], [f32(x) for x in cc]
 
 
+def fit_log(deg: int = 7):
+    """(ln(1 + f) - f) / f^2 = P(f) on [-1/3, 1/3]; weighted to the relative
+    error of ln(1 + f)."""
+    f = np.concatenate([np.linspace(-1.0 / 3.0, -1e-5, 200001), np.linspace(1e-5, 1.0 / 3.0, 200001)])
+    B = np.stack([f ** i for i in range(deg + 1)], axis=1)
+    t = (np.log1p(f) - f) / (f * f)
+    w = (f * f) / np.abs(np.log1p(f))
+    return [f32(x) for x in lawson(B, t, w)]
+
+
+LN2_HI = f32(0.693145751953125)          # 0x1.62e4p-1: 11 significant bits, e * LN2_HI exact
+LN2_LO = f32(np.log(2.0) - 0.693145751953125)
+
+
+def log32(x, c):
+    """The device's float32 evaluation of ln x for normal x > 0."""
+    i = x.view(np.int32).astype(np.int64)
+    e = (i - 0x3F2AAAAB) >> 23
+    m = (i - (e << 23)).astype(np.int32).view(np.float32)
+    f = (m - np.float32(1.0)).astype(np.float32)
+    z = (f * f).astype(np.float32)
+    p = horner32(c, f)
+    r = fma32(p, z, f)
+    ef = e.astype(np.float32)
+    return fma32(ef, LN2_HI, fma32(ef, LN2_LO, r))
+
+
+def check_log(c):
+    rng = np.random.default_rng(0)
+    u = np.concatenate([
+        ((rng.integers(0, 2 ** 32, 2000000, dtype=np.uint64).astype(np.float32) + np.float32(0.5))
+         * np.float32(2.0 ** -32)).astype(np.float32),
+        np.float32(1.0) - np.arange(1, 20000, dtype=np.float32) * np.float32(2.0 ** -24),
+        np.float32(2.0) ** -np.arange(1, 33, dtype=np.float32)])
+    got = log32(u, c).astype(np.float64)
+    ref = np.log(u.astype(np.float64))
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30)
+    return rel.max(), np.abs(got - ref).max()
+
+
 def check_quarter(cs, cc):
     f = np.linspace(-0.5, 0.5, 2000001).astype(np.float32)
     z = (f * f).astype(np.float32)
@@ -126,6 +168,11 @@ def main():
     print("radians cos C(z):", ", ".join(hexf(x) for x in rc))
     print("  max abs error on [-pi/4, pi/4] (float32 evaluation): sin %.3g  cos %.3g"
           % check_radians(rs, rc))
+    lc = fit_log()
+    print("log P(f):", ", ".join(hexf(x) for x in lc))
+    print("  max error of ln u on u = (x + 0.5) 2^-32 (float32 evaluation): rel %.3g  abs %.3g"
+          % check_log(lc))
+    print("ln2 split:", hexf(LN2_HI), hexf(LN2_LO))
     # Cody-Waite split of pi/2 for the FMA reduction r = x - q (C1 + C2 + C3)
     c1 = f32(np.pi / 2)
     c2 = f32(np.pi / 2 - np.float64(c1))

@@ -14,8 +14,8 @@
 //   - Philox-2x32-10, the uint -> (0,1) map and Box-Muller, the CUDA form of
 //     shaders/philox.h:19-50.  Words are bit-exact with the reference.  The
 //     normals use correctly-rounded float ops for the uniform map (identical
-//     bits to the reference), CUDA's logf, the SM's square root and the
-//     library's own quarter-turn sine / cosine (errors of order 1e-7);
+//     bits to the reference), the library's own logarithm and quarter-turn
+//     sine / cosine and the SM's square root (errors of order 1e-7);
 //   - mppi_sincosf, the library's own sin / cos for plugins.
 #pragma once
 
@@ -180,15 +180,38 @@ __device__ __forceinline__ void mppi_sincosf(float x, float* so, float* co) {
   mppi_quadrant(__float_as_uint(t), fmaf(ps, __fmul_rn(r, z), r), fmaf(pc, z, 1.0f), so, co);
 }
 
+// ln x for normal x > 0 (the Box-Muller argument u1 lies in [2^-33, 1]): the
+// exponent is split off around 2/3, x = 2^e (1 + f) with f in [-1/3, 1/3)
+// exact (Sterbenz), and ln(1 + f) = f + f^2 P(f) with a degree-7 polynomial
+// fitted for this library (csrc/device/derive_poly.py); e ln 2 is added in two
+// parts (the first exact).  Relative error at most 8.7e-8 on the Box-Muller
+// arguments (float32 evaluation against float64).  Not for zero, negative,
+// subnormal, infinite or NaN arguments.
+__device__ __forceinline__ float mppi_log(float x) {
+  const uint32_t i = __float_as_uint(x);
+  const int32_t e = (int32_t)(i - 0x3f2aaaabu) >> 23;
+  const float f = __fsub_rn(__uint_as_float(i - ((uint32_t)e << 23)), 1.0f);
+  float p = fmaf(0x1.1f421ap-3f, f, -0x1.3b27cap-3f);
+  p = fmaf(p, f, 0x1.1ea26ap-3f);
+  p = fmaf(p, f, -0x1.5032fep-3f);
+  p = fmaf(p, f, 0x1.99d426p-3f);
+  p = fmaf(p, f, -0x1.00147ep-2f);
+  p = fmaf(p, f, 0x1.5554fap-2f);
+  p = fmaf(p, f, -0x1.ffffd6p-2f);
+  const float r = fmaf(p, __fmul_rn(f, f), f);
+  const float ef = (float)e;
+  return fmaf(ef, 0x1.62e4p-1f, fmaf(ef, 0x1.7f7d1cp-20f, r));
+}
+
 // Box-Muller (shaders/philox.h:44-50): r = sqrt(-2 ln u1), theta = 2 pi u2.
 // The angle is taken as a quarter-turn count, 4 u2 = (x2 + 0.5) * 2^-30 --
 // exactly 4 times the reference's u2 -- so 2 pi u2 is never rounded to a
-// float; CUDA's logf gives ln u1 and the SM's square root the radius (relative
-// error of order 2^-23).
+// float; the library's logarithm gives ln u1 and the SM's square root the
+// radius (relative error of order 2^-23).
 __device__ __forceinline__ float2 mppi_box_muller(uint2 w) {
   const float u1 = mppi_uint_to_01(w.x);
   const float v = __fmul_rn(__fadd_rn(__uint2float_rn(w.y), 0.5f), 0x1p-30f);
-  const float r = mppi_sqrt_approx(-2.0f * logf(u1));
+  const float r = mppi_sqrt_approx(-2.0f * mppi_log(u1));
   float s, c;
   mppi_sincos_quarter(v, &s, &c);
   return make_float2(r * c, r * s);

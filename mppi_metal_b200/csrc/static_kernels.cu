@@ -31,6 +31,11 @@ __global__ void __launch_bounds__(256)
   co[i] = c;
 }
 
+__global__ void __launch_bounds__(256) log_kernel(uint64_t n, const float* x, float* out) {
+  const uint64_t i = (uint64_t)blockIdx.x * 256 + threadIdx.x;
+  if (i < n) out[i] = mppi_log(x[i]);
+}
+
 void set_err(char* err, size_t len, const std::string& msg) {
   if (err && len) {
     const size_t k = msg.size() < len - 1 ? msg.size() : len - 1;
@@ -105,6 +110,39 @@ extern "C" int mppi_device_sincos(uint64_t n, const float* x, int quarter, float
     }
     if (e == cudaSuccess) e = cudaMemcpy(sin_out, dx + n, bytes, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(cos_out, dx + 2 * n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(buf);
+  }
+  if (e != cudaSuccess) {
+    set_err(err, err_len, std::string("CUDA error: ") + cudaGetErrorString(e));
+    return MPPI_ERR_CUDA;
+  }
+  return MPPI_OK;
+}
+
+extern "C" int mppi_device_log(uint64_t n, const float* x, float* out, char* err,
+                               size_t err_len) {
+  if (n == 0) return MPPI_OK;
+  if (!x || !out) {
+    set_err(err, err_len, "null argument to mppi_device_log.");
+    return MPPI_ERR_INVALID;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_err(err, err_len, "No CUDA device available.");
+    return MPPI_ERR_NO_DEVICE;
+  }
+  void* buf = nullptr;
+  const size_t bytes = n * 4;
+  cudaError_t e = cudaMalloc(&buf, 2 * bytes);
+  if (e == cudaSuccess) {
+    float* dx = static_cast<float*>(buf);  // [x n][out n]
+    e = cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+      log_kernel<<<(unsigned)((n + 255) / 256), 256>>>(n, dx, dx + n);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, dx + n, bytes, cudaMemcpyDeviceToHost);
     cudaFree(buf);
   }
   if (e != cudaSuccess) {

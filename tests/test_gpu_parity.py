@@ -21,7 +21,7 @@ import pytest
 
 from helpers import abs_err, backend_for, nonholonomic_example, oracle_problem, rel_err
 from mppi_metal_b200 import models
-from mppi_metal_b200.backend import Backend, device_philox, device_sincos
+from mppi_metal_b200.backend import Backend, device_log, device_philox, device_sincos
 
 pytestmark = pytest.mark.gpu
 
@@ -82,6 +82,22 @@ def test_device_sincos_quarter_turn_accuracy():
     assert np.max(np.abs(s - np.sin(vd))) < TOL_SINCOS
     assert np.max(np.abs(c - np.cos(vd))) < TOL_SINCOS
     assert s[-1] == 0.0 and c[-1] == 1.0  # u2 rounds to 1: a full turn
+
+
+def test_device_log_accuracy():
+    # Box-Muller's argument u1 = (x + 0.5) 2^-32 for every Philox word x, the
+    # floats just below 1, and the powers of two
+    rng = np.random.default_rng(13)
+    w = rng.integers(0, 2 ** 32, 1 << 20, dtype=np.uint64)
+    u = np.concatenate([
+        ((w.astype(np.float32) + np.float32(0.5)) * np.float32(2.0 ** -32)).astype(np.float32),
+        np.float32(1.0) - np.arange(0, 4096, dtype=np.float32) * np.float32(2.0 ** -24),
+        np.float32(2.0) ** -np.arange(0, 33, dtype=np.float32)]).astype(np.float32)
+    got = device_log(u).astype(np.float64)
+    ref = np.log(u.astype(np.float64))
+    assert got[np.flatnonzero(u == 1.0)[0]] == 0.0
+    rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-30)
+    assert rel.max() < 2e-7
 
 
 def test_noise_normals_match_oracle(oracle):
