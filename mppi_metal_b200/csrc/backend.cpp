@@ -2,12 +2,15 @@
 //
 // Host side of the hot path: owns the per-driver kernel module (NVRTC), the
 // CUDA stream, device buffers and pinned staging buffers, chooses the launch
-// geometry, and issues rollout + combine launches (captured into a CUDA graph
-// for closed loops).  Replaces the reference's MetalBackend
+// geometry and the form of a step, and issues the step's launches (captured
+// into a CUDA graph for closed loops).  Replaces the reference's MetalBackend
 // (src/metal_backend.mm): there, one command buffer per call encodes four
 // passes per step with buffer barriers and waits for completion; here each
-// control step is two kernels, a T-step closed loop is one graph launch, and
-// the host waits once per call.
+// control step is one rollout launch whose agents' last CTAs also combine
+// (or a rollout and a combine kernel, whichever form the per-shape timing
+// keeps), a T-step closed loop is one graph launch, and the host waits once
+// per call.
+//   done      [N] u32          finished rollout CTAs per agent (fused combine)
 //
 // Device data layout for a batch of N agents (all FP32, agent-major):
 //   io:       [step_base u32 x4][x N*n][u_nom N*H*m][u_out N*H*m][diag N*3][stats N*4]
@@ -167,8 +170,8 @@ struct mppi_backend {
   LaunchGeom geom;
   DevBuf d_io, d_costs, d_partials;
   DevBuf d_done;  // [N] per-agent count of finished rollout CTAs (fused combine)
-  // Uniform batches run the combine inside the rollout launch (its agent's
-  // last CTA); MPPI_B200_SEPARATE_COMBINE=1 keeps the separate combine kernel.
+  // false: never run the combine inside the rollout launch (its agent's last
+  // CTA) -- MPPI_B200_SEPARATE_COMBINE=1
   bool fuse_combine = true;
   // MPPI_B200_FUSED_COMBINE=1 / MPPI_B200_WS=1 or 0 pin the step form's
   // combine and warp-specialisation choices (0 = timed)
@@ -892,7 +895,7 @@ int check_override_sizes(mppi_backend* b, size_t mp_bytes, const void* mp, size_
   return MPPI_OK;
 }
 
-// Enqueues T closed-loop steps (rollout + combine/propagate each), through a
+// Enqueues T closed-loop steps (rollout with combine/propagate each), through a
 // CUDA graph captured once per (shape, buffers) and replayed afterwards.
 int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
   char keybuf[320];
