@@ -405,7 +405,16 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
     g.nblk = maxblk;  // the largest agent's CTA count (combine shared memory)
     b->geom = g;
   }
-  CK(b->d_io.ensure(b->io_floats() * 4, &grew));
+  {
+    // zeroed when (re)allocated: the step-form timing of a new shape may run
+    // before the first upload, and then reads zeros, not leftover bits
+    bool fresh = false;
+    CK(b->d_io.ensure(b->io_floats() * 4, &fresh));
+    if (fresh) {
+      grew = true;
+      CK(cudaMemsetAsync(b->d_io.p, 0, b->d_io.bytes, b->stream));
+    }
+  }
   CK(b->d_costs.ensure((size_t)N * b->K * 4, &grew));
   const size_t records = b->ragged ? b->total_records : (size_t)N * b->geom.nblk;
   CK(b->d_partials.ensure(records * b->geom.pstride * 4, &grew));
