@@ -7,7 +7,8 @@ diagnostics.  The same holds for the warp-specialised rollout (a second set
 of warps draws the noise ahead), with either combine.  The backend picks the
 form per launch shape by timing; MPPI_B200_FUSED_COMBINE=1 /
 MPPI_B200_SEPARATE_COMBINE=1 and MPPI_B200_WS=1 / 0 (read when a backend is
-created) pin it here."""
+created) pin it here.  Programmatic dependent launch, on by default, is
+checked against plain launches (MPPI_B200_NO_PDL=1) the same way."""
 from __future__ import annotations
 
 import os
@@ -127,3 +128,12 @@ def test_warp_specialised_single_step_matches_plain():
 
     (u1, d1), (u2, d2) = _ws(lambda: _fused(step)), _separate(step)
     assert np.array_equal(u1, u2) and np.array_equal(d1, d2)
+
+
+def test_programmatic_dependent_launch_matches_plain_launches():
+    # the loop-constant prologue runs before griddepcontrol.wait; everything
+    # the previous launch writes is read after it: same bits either way
+    w = models.unicycle_batch(seed=23, N=6, K=1000, H=24, T=10)
+    pdl, _ = _uniform_loop(w)
+    plain, _ = _with_env("MPPI_B200_NO_PDL", lambda: _uniform_loop(w))
+    _assert_same(pdl, plain)
