@@ -176,8 +176,8 @@ struct mppi_backend {
   // MPPI_B200_FUSED_COMBINE=1 / MPPI_B200_WS=1 or 0 pin the step form's
   // combine and warp-specialisation choices (0 = timed)
   int combine_pin = 0, ws_pin = 0;
-  uint32_t form = 0;          // for combine_key's launch shape: kFormFused | kFormWs
-  std::string combine_key;
+  uint32_t form = 0;          // for form_key's launch shape: kFormFused | kFormWs
+  std::string form_key;
   // Uniform rollout launches (and the proposal network's) use programmatic
   // dependent launch; MPPI_B200_NO_PDL=1 launches them plainly.
   bool pdl = true;
@@ -755,13 +755,13 @@ cudaError_t launch_rollout_combine(mppi_backend* b, uint32_t step_local, bool pr
 // cost a model's rollout registers; the warp-specialised rollout shortens
 // each sample's chain where few CTAs leave SMs idle, and only costs
 // instructions where the SMs are full -- so neither choice wins everywhere.
-int decide_combine(mppi_backend* b, char* err, size_t err_len) {
+int decide_step_form(mppi_backend* b, char* err, size_t err_len) {
   char kb[192];
   snprintf(kb, sizeof(kb), "%u/%u/%u/%d/%u/%u/%u/%u/%p/%p/%u/%d/", b->N, b->K, b->H,
            b->geom.variant, b->geom.block, b->geom.stage_rows, b->geom.nblk, b->grid,
            (const void*)b->mod.get(), (const void*)b->proposal, b->prop_samples, (int)b->ragged);
   const std::string key = std::string(kb) + (b->ragged ? b->tuned_key : std::string());
-  if (b->combine_key == key) return MPPI_OK;
+  if (b->form_key == key) return MPPI_OK;
   std::vector<uint32_t> forms;
   for (uint32_t ws : {0u, kFormWs}) {
     if (ws && (b->ws_pin < 0 || !ws_possible(b))) continue;
@@ -796,7 +796,7 @@ int decide_combine(mppi_backend* b, char* err, size_t err_len) {
     }
   }
   b->form = best;
-  b->combine_key = key;
+  b->form_key = key;
   return MPPI_OK;
 }
 
@@ -926,7 +926,7 @@ int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
       CK(set_rollout_smem(b));
     }
   }
-  if (int rc = decide_combine(b, err, err_len)) return rc;
+  if (int rc = decide_step_form(b, err, err_len)) return rc;
   const std::string key = std::string(keybuf) + (b->ragged ? "/r" + std::to_string(b->grid) + "/" +
                                                                  std::to_string(b->geom.stage_rows) +
                                                                  "/" + b->tuned_key
@@ -1182,7 +1182,7 @@ int mppi_backend_dispatch_rollout(mppi_backend* b, uint64_t step_index, const fl
   const bool mo = mp && mp_bytes, co = cp && cp_bytes;
   if (mo) CK(b->d_mp_ovr.ensure(pad16(b->mp_size)));
   if (co) CK(b->d_cp_ovr.ensure(pad16(b->cp_size)));
-  if (int rc = decide_combine(b, err, err_len)) return rc;
+  if (int rc = decide_step_form(b, err, err_len)) return rc;
   stage_upload(b, step_index, x0, u_nominal, mp, mp_bytes, cp, cp_bytes);
   float* down = b->h_down.as<float>();
   const size_t nd = b->off_stats() - b->off_uout();
