@@ -22,9 +22,9 @@ from mppi_metal_b200 import models
 pytestmark = pytest.mark.gpu
 
 
-def _with_env(name, fn):
+def _with_env(name, fn, value="1"):
     old = os.environ.get(name)
-    os.environ[name] = "1"
+    os.environ[name] = value
     try:
         return fn()
     finally:
@@ -137,3 +137,28 @@ def test_programmatic_dependent_launch_matches_plain_launches():
     pdl, _ = _uniform_loop(w)
     plain, _ = _with_env("MPPI_B200_NO_PDL", lambda: _uniform_loop(w))
     _assert_same(pdl, plain)
+
+
+def test_warp_specialised_proposal_loop_matches_plain():
+    # the noise warps also draw the proposal samples (mean shift and scales
+    # from the network's output): same bits as the plain form
+    pytest.importorskip("torch")
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.unicycle_batch(seed=24, N=12, K=256, H=64, T=4)
+    net = ProposalNet(31, 64, 2, max_batch=256, seed=7)
+
+    def run():
+        b = backend_for(w, bind=False)
+        b.set_features("mppi_proposal_features", 31)
+        b.set_proposal(net, 128)
+        b.prepare(w.num_agents, w.num_steps, w.x0, cost_params=w.cost_params_packed,
+                  cost_stride=w.cost_stride, model_params=w.model_params, sigma=w.agent_sigma)
+        b.run(0)
+        r = b.fetch()
+        b.set_proposal(None)
+        b.close()
+        return r
+
+    ws = _ws(lambda: _fused(run))
+    plain = _with_env("MPPI_B200_WS", lambda: _separate(run), value="0")
+    _assert_same(ws, plain)
