@@ -181,6 +181,13 @@ int mppi_backend_time_passes(mppi_backend* b, uint32_t iters, float* rollout_ms,
 int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
                              uint32_t* stage_rows, uint32_t* smem_bytes,
                              uint32_t* kernels_per_step);
+/* Step form of the last launch shape run (chosen by timing on its first
+ * run, or pinned by MPPI_B200_FUSED_COMBINE / _SEPARATE_COMBINE / _WS):
+ * bit 0 = combine run by each agent's last rollout CTA, bit 1 =
+ * warp-specialised rollout; 0 = plain rollout and separate combine kernel.
+ * No counterpart in the reference, whose step is a fixed sequence of
+ * dispatches (src/metal_backend.mm:678-713). */
+int mppi_backend_step_form(mppi_backend* b, uint32_t* form);
 
 /* Autotuner result for the prepared uneven batch: persistent grid size
  * (0 = one CTA per work item), number of work items, noise staging rows and

@@ -121,6 +121,7 @@ SIGNATURES = {
     "mppi_backend_time_passes": (ctypes.c_int, [c_ptr, c_u32, ctypes.POINTER(c_f32),
                                                 ctypes.POINTER(c_f32)] + _ERR),
     "mppi_backend_launch_info": (ctypes.c_int, [c_ptr] + [ctypes.POINTER(c_u32)] * 5),
+    "mppi_backend_step_form": (ctypes.c_int, [c_ptr, ctypes.POINTER(c_u32)]),
     "mppi_backend_tuning_info": (ctypes.c_int, [c_ptr] + [ctypes.POINTER(c_u32)] * 3
                                  + [ctypes.POINTER(c_f32)]),
     "mppi_device_philox": (ctypes.c_int, [c_u64, c_ptr, c_ptr, c_ptr, c_ptr] + _ERR),

@@ -288,7 +288,11 @@ class Backend:
         vals = [ctypes.c_uint32() for _ in range(5)]
         self.lib.mppi_backend_launch_info(self.h, *[ctypes.byref(v) for v in vals])
         keys = ["block", "nblk", "stage_rows", "smem_bytes", "kernels_per_step"]
-        return {k: v.value for k, v in zip(keys, vals)}
+        info = {k: v.value for k, v in zip(keys, vals)}
+        f = ctypes.c_uint32()
+        self.lib.mppi_backend_step_form(self.h, ctypes.byref(f))
+        info["form"] = {"fused_combine": bool(f.value & 1), "warp_specialised": bool(f.value & 2)}
+        return info
 
 
 def device_philox(c0, c1, key) -> np.ndarray:

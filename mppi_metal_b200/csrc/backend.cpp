@@ -1664,6 +1664,12 @@ int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
   return MPPI_OK;
 }
 
+int mppi_backend_step_form(mppi_backend* b, uint32_t* form) {
+  if (!b || !b->initialized) return MPPI_ERR_NOT_INIT;
+  if (form) *form = b->form;
+  return MPPI_OK;
+}
+
 }  // extern "C"
 
 // ---- learned proposal (include/mppi_b200/mppi_backend.h, "proposal") ------

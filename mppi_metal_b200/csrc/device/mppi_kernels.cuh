@@ -561,6 +561,17 @@ __device__ __forceinline__ void rollout_work(const MppiRolloutArgs& a) {
 // --------------------------------------------------------------------------
 constexpr int kCombineBlock = 256;
 
+// The propagate's dynamics step x <- f(x, u*_0), compiled once and called by
+// every kernel that runs a combine (the combine kernel and the rollout
+// kernels' fused tails).  An inlined copy per kernel may contract
+// multiply-adds differently in each, and the propagated state -- the next
+// step's x0 -- would then depend on the step form chosen for the shape.
+__device__ __noinline__ void propagate_dynamics(float* st, const float* u0, const uint8_t* mp,
+                                                uint32_t step, uint32_t agent) {
+  MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u0, mp,
+                   make_uint2(step, 0x80000000u), agent);
+}
+
 template <int CB>
 __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t agent,
                                               float* dsm) {
@@ -655,9 +666,7 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
       for (int d = 0; d < kM; ++d) a.hist_controls[(size_t)row * kM + d] = u0[d];
     if (a.hist_costs) a.hist_costs[row] = M;
     // counter (step, 0x80000000); seed = agent index (0 for a single agent)
-    MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u0,
-                     a.model_params + a.model_stride * agent, make_uint2(step, 0x80000000u),
-                     agent);
+    propagate_dynamics(st, u0, a.model_params + a.model_stride * agent, step, agent);
 #pragma unroll
     for (int d = 0; d < kN; ++d) xg[d] = st[d];
     if (a.terminal)

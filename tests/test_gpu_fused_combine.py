@@ -104,6 +104,13 @@ def test_fused_combine_matches_separate_single_step():
     assert np.array_equal(u1, u2) and np.array_equal(d1, d2)
 
 
+def test_fused_combine_matches_separate_quadrotor():
+    # the propagate's dynamics are one compiled function for both forms; an
+    # inlined copy per kernel had contracted multiply-adds differently
+    w = models.quadrotor_batch(seed=28, N=3, K=700, H=37, T=6)
+    _assert_same(_fused(lambda: _uniform_loop(w))[0], _separate(lambda: _uniform_loop(w))[0])
+
+
 @pytest.mark.parametrize("N,K,H", [(24, 1000, 20), (3, 20000, 20), (8, 256, 64)])
 def test_warp_specialised_rollout_matches_plain(N, K, H):
     w = models.unicycle_batch(seed=22, N=N, K=K, H=H, T=8)
@@ -162,3 +169,20 @@ def test_warp_specialised_proposal_loop_matches_plain():
     ws = _ws(lambda: _fused(run))
     plain = _with_env("MPPI_B200_WS", lambda: _separate(run), value="0")
     _assert_same(ws, plain)
+
+
+
+def test_step_form_reported():
+    w = models.unicycle_batch(seed=27, N=4, K=512, H=30, T=2)
+
+    def run():
+        b = backend_for(w)
+        b.simulate_batch(w.num_agents, w.num_steps, 0, w.x0, cost_params=w.cost_params_packed,
+                         cost_stride=w.cost_stride, sigma=w.agent_sigma)
+        info = b.launch_info()
+        b.close()
+        return info["form"]
+
+    assert _ws(lambda: _fused(run)) == {"fused_combine": True, "warp_specialised": True}
+    assert _with_env("MPPI_B200_WS", lambda: _separate(run), value="0") == \
+        {"fused_combine": False, "warp_specialised": False}
