@@ -16,7 +16,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import backend_for
+from helpers import backend_for, nonholonomic_example
 from mppi_metal_b200 import models
 
 pytestmark = pytest.mark.gpu
@@ -186,3 +186,46 @@ def test_step_form_reported():
     assert _ws(lambda: _fused(run)) == {"fused_combine": True, "warp_specialised": True}
     assert _with_env("MPPI_B200_WS", lambda: _separate(run), value="0") == \
         {"fused_combine": False, "warp_specialised": False}
+
+
+def _quad_mixed():
+    w = models.quadrotor_batch(seed=29, N=2, K=600, H=30, T=5)
+    w.numeric_mode = 2
+    return w
+
+
+# Every shipped plugin, at sizes where all four step forms apply (128-sample
+# CTAs, whole horizon staged): each form is a separately compiled kernel, and
+# the compiler could contract a plugin's multiply-adds differently in each.
+PLUGIN_WORKLOADS = {
+    "unicycle_obstacles": lambda: models.unicycle_batch(seed=29, N=6, K=600, H=24, T=5),
+    "unicycle_control_cost": lambda: models.unicycle_single(seed=29, K=600, H=24, T=5),
+    "quadrotor": lambda: models.quadrotor_batch(seed=29, N=2, K=600, H=30, T=5),
+    "quadrotor_mixed": _quad_mixed,
+    "bicycle_full_cov": lambda: models.bicycle_uneven(seed=29, N=5, T=5, k_range=(600, 600),
+                                                      h_range=(24, 24)),
+    "gust_integrator": lambda: models.gust_batch(seed=29, N=5, K=600, H=24, T=5),
+    "double_integrator": lambda: models.double_integrator_test(K=600, H=24),
+    "nonholonomic_vehicle": lambda: nonholonomic_example(K=600, H=24),
+}
+
+
+@pytest.mark.parametrize("name", sorted(PLUGIN_WORKLOADS))
+def test_every_step_form_same_bits_per_plugin(name):
+    w = PLUGIN_WORKLOADS[name]()
+
+    def run():
+        b = backend_for(w)
+        r = b.simulate_batch(w.num_agents, w.num_steps, 0, w.x0,
+                             cost_params=w.cost_params_packed or None, cost_stride=w.cost_stride,
+                             sigma=w.agent_sigma)
+        form = b.launch_info()["form"]
+        b.close()
+        return r, form
+
+    base, f0 = _with_env("MPPI_B200_WS", lambda: _separate(run), value="0")
+    assert f0 == {"fused_combine": False, "warp_specialised": False}
+    for ws, pin in ((False, _fused), (True, _separate), (True, _fused)):
+        r, f = _with_env("MPPI_B200_WS", lambda: pin(run), value="1" if ws else "0")
+        assert f == {"fused_combine": pin is _fused, "warp_specialised": ws}
+        _assert_same(r, base)
