@@ -607,14 +607,14 @@ cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a, bool ws = f
                             dim3(b->geom.nblk, b->N), dim3(2 * b->geom.block), b->geom.smem,
                             args);
   if (b->ragged) {
-    if (b->grid) {
-      cudaError_t e = cudaMemsetAsync(b->d_queue.p, 0, 4, b->stream);
-      if (e != cudaSuccess) return e;
-    }
-    return cudaLaunchKernel(fused ? (const void*)b->mod->rollout_work_fused
-                                  : (const void*)b->mod->rollout_work,
-                            dim3(b->grid ? b->grid : b->num_work), dim3(128), args,
-                            b->geom.smem, b->stream);
+    const void* f = fused ? (const void*)b->mod->rollout_work_fused
+                          : (const void*)b->mod->rollout_work;
+    // one CTA per work item: a dependent launch like the uniform batch's;
+    // a persistent grid's queue counter is reset first (a plain launch)
+    if (!b->grid) return launch_dependent(b, f, dim3(b->num_work), dim3(128), b->geom.smem, args);
+    cudaError_t e = cudaMemsetAsync(b->d_queue.p, 0, 4, b->stream);
+    if (e != cudaSuccess) return e;
+    return cudaLaunchKernel(f, dim3(b->grid), dim3(128), args, b->geom.smem, b->stream);
   }
   return launch_dependent(b, fused ? (const void*)b->mod->rollout_fused[b->geom.variant]
                                    : (const void*)b->mod->rollout[b->geom.variant],

@@ -536,6 +536,10 @@ __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
 template <int BLOCK, bool FUSED>
 __device__ __forceinline__ void rollout_work(const MppiRolloutArgs& a) {
   __shared__ uint32_t item_s;
+  // the work list, K and H are constant over a closed loop; each item waits
+  // (griddepcontrol.wait in rollout_item) before it reads the previous
+  // launch's results
+  mppi_allow_dependent_launch();
   for (uint32_t pass = 0;; ++pass) {
     __syncthreads();  // the previous item is done with shared memory
     if (threadIdx.x == 0)

@@ -146,6 +146,26 @@ def test_programmatic_dependent_launch_matches_plain_launches():
     _assert_same(pdl, plain)
 
 
+@pytest.mark.parametrize("grid", ["0", "148"])
+def test_programmatic_dependent_launch_matches_plain_launches_uneven(grid):
+    # one CTA per work item (grid 0): dependent launches; a persistent grid
+    # (its queue counter reset before each launch): plain launches either way
+    w = models.bicycle_uneven(seed=6, N=9, T=5, k_range=(100, 1500), h_range=(6, 28))
+
+    def run():
+        b = backend_for(w)
+        r = b.simulate_batch(w.num_agents, w.num_steps, 0, w.x0,
+                             cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+                             sigma=w.agent_sigma, sample_counts=w.agent_K, horizons=w.agent_H)
+        b.close()
+        return r
+
+    pdl = _with_env("MPPI_B200_UNEVEN_GRID", run, value=grid)
+    plain = _with_env("MPPI_B200_UNEVEN_GRID",
+                      lambda: _with_env("MPPI_B200_NO_PDL", run), value=grid)
+    _assert_same(pdl, plain)
+
+
 def test_warp_specialised_proposal_loop_matches_plain():
     # the noise warps also draw the proposal samples (mean shift and scales
     # from the network's output): same bits as the plain form
