@@ -716,7 +716,7 @@ def run_proposal(args):
                      "achieved": mlp_flops / (net_ms / 1e3) / 1e12, "peak": bf16_peak,
                      "unit": "TFLOP/s", "frac": mlp_flops / (net_ms / 1e3) / 1e12 / bf16_peak,
                      "traffic": None,
-                     "note": f"M = {N} rows: one 4-CTA cluster, latency-bound; the dominant "
+                     "note": f"M = {N} rows: one 8-CTA cluster, latency-bound; the dominant "
                              "kernel of the step is the rollout (issue-bound, see the batch "
                              "workload); peak = measured bf16 burst"
                              + ("" if peaks.get("bf16_tflops") else " (fallback)")},

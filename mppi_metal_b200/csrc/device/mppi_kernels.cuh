@@ -576,6 +576,20 @@ __device__ __noinline__ void propagate_dynamics(float* st, const float* u0, cons
                    make_uint2(step, 0x80000000u), agent);
 }
 
+#ifdef MPPI_FEATURES_FN
+// The plugin's proposal features f[0, MPPI_MAX_FEATURES) of one state (zero
+// where the callable sets none), compiled once for the same reason: the
+// features kernel (a loop's first step) and every combine (the steps after
+// it) call this one copy, so the network's input -- and with it the proposal
+// -- cannot depend on the step form.
+__device__ __noinline__ void compute_features(const float* st, const uint8_t* mp,
+                                              const uint8_t* cp, float* f) {
+#pragma unroll
+  for (int i = 0; i < MPPI_MAX_FEATURES; ++i) f[i] = 0.0f;
+  MPPI_FEATURES_FN(st, mp, cp, f);
+}
+#endif
+
 template <int CB>
 __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t agent,
                                               float* dsm) {
@@ -679,9 +693,7 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
     // the next step's proposal features, from the state just propagated
     if (a.features) {
       float f[MPPI_MAX_FEATURES];
-#pragma unroll
-      for (int i = 0; i < MPPI_MAX_FEATURES; ++i) f[i] = 0.0f;
-      MPPI_FEATURES_FN(st, a.model_params + a.model_stride * agent,
+      compute_features(st, a.model_params + a.model_stride * agent,
                        a.cost_params + a.cost_stride * agent, f);
       float* o = a.features + (size_t)agent * a.feature_stride;
 #pragma unroll
@@ -784,10 +796,8 @@ extern "C" __global__ void __launch_bounds__(128) mppi_features(const MppiFeatur
 #pragma unroll
   for (int d = mppi::kN; d < mppi::kNPad; ++d) st[d] = 0.0f;
   float f[MPPI_MAX_FEATURES];
-#pragma unroll
-  for (int i = 0; i < MPPI_MAX_FEATURES; ++i) f[i] = 0.0f;
-  MPPI_FEATURES_FN(st, a.model_params + a.model_stride * agent,
-                   a.cost_params + a.cost_stride * agent, f);
+  mppi::compute_features(st, a.model_params + a.model_stride * agent,
+                         a.cost_params + a.cost_stride * agent, f);
   float* o = a.out + (size_t)r * a.out_stride;
 #pragma unroll
   for (int i = 0; i < MPPI_MAX_FEATURES; ++i)

@@ -249,3 +249,33 @@ def test_every_step_form_same_bits_per_plugin(name):
         r, f = _with_env("MPPI_B200_WS", lambda: pin(run), value="1" if ws else "0")
         assert f == {"fused_combine": pin is _fused, "warp_specialised": ws}
         _assert_same(r, base)
+
+
+def test_every_step_form_same_bits_quadrotor_proposal():
+    # with a network attached the combine also computes the next step's
+    # features (one compiled copy of the feature callable for every kernel);
+    # the network predicts the first 16 of the 24 steps
+    pytest.importorskip("torch")
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.quadrotor_batch(seed=30, N=3, K=512, H=24, T=4)
+    net = ProposalNet(29, 16, 4, max_batch=128, seed=8)
+
+    def run():
+        b = backend_for(w, bind=False)
+        b.set_features("mppi_proposal_features", 29)
+        b.set_proposal(net, 256)
+        b.prepare(w.num_agents, w.num_steps, w.x0, cost_params=w.cost_params_packed,
+                  cost_stride=w.cost_stride, model_params=w.model_params, sigma=w.agent_sigma)
+        b.run(0)
+        r = b.fetch()
+        form = b.launch_info()["form"]
+        b.set_proposal(None)
+        b.close()
+        return r, form
+
+    base, f0 = _with_env("MPPI_B200_WS", lambda: _separate(run), value="0")
+    assert f0 == {"fused_combine": False, "warp_specialised": False}
+    for ws, pin in ((False, _fused), (True, _separate), (True, _fused)):
+        r, f = _with_env("MPPI_B200_WS", lambda: pin(run), value="1" if ws else "0")
+        assert f == {"fused_combine": pin is _fused, "warp_specialised": ws}
+        _assert_same(r, base)
