@@ -25,6 +25,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import select
 import statistics
 import subprocess
 import sys
@@ -133,6 +134,10 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
+    # 20 ms between samples: the shortest timed regions (the proposal
+    # workload's five 300-step loops) last about 0.1 s
+    INTERVAL_MS = 20
+
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.proc = None
@@ -141,16 +146,26 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-i", str(self.idx), "-lms", "100"], stdout=subprocess.PIPE,
+                 "-i", str(self.idx), "-lms", str(self.INTERVAL_MS)], stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        # the sampler's start-up takes longer than a short timed region: wait
+        # for its first sample (taken before the region, not counted)
+        ready, _, _ = select.select([self.proc.stdout], [], [], 10.0)
+        if ready:
+            self.proc.stdout.readline()
         return self
 
     def __exit__(self, *exc):
         self.rows = []
         if self.proc is None:
             return False
+        if not select.select([self.proc.stdout], [], [], 0)[0]:
+            # a region shorter than the interval: the next sample, at most one
+            # interval after its end, stands for it
+            select.select([self.proc.stdout], [], [], 1.0)
         self.proc.terminate()
         try:
             out, _ = self.proc.communicate(timeout=5)

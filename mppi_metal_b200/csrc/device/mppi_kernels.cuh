@@ -570,10 +570,19 @@ constexpr int kCombineBlock = 256;
 // kernels' fused tails).  An inlined copy per kernel may contract
 // multiply-adds differently in each, and the propagated state -- the next
 // step's x0 -- would then depend on the step form chosen for the shape.
-__device__ __noinline__ void propagate_dynamics(float* st, const float* u0, const uint8_t* mp,
-                                                uint32_t step, uint32_t agent) {
-  MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u0, mp,
+// State and control travel by value (registers), not through memory.
+struct PropagateState {
+  __align__(16) float s[kNPad];
+};
+struct PropagateControl {
+  float u[kM];
+};
+__device__ __noinline__ PropagateState propagate_dynamics(PropagateState x, PropagateControl c,
+                                                          const uint8_t* mp, uint32_t step,
+                                                          uint32_t agent) {
+  MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(x.s)), c.u, mp,
                    make_uint2(step, 0x80000000u), agent);
+  return x;
 }
 
 #ifdef MPPI_FEATURES_FN
@@ -684,7 +693,17 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
       for (int d = 0; d < kM; ++d) a.hist_controls[(size_t)row * kM + d] = u0[d];
     if (a.hist_costs) a.hist_costs[row] = M;
     // counter (step, 0x80000000); seed = agent index (0 for a single agent)
-    propagate_dynamics(st, u0, a.model_params + a.model_stride * agent, step, agent);
+    {
+      PropagateState x;
+      PropagateControl c;
+#pragma unroll
+      for (int d = 0; d < kNPad; ++d) x.s[d] = st[d];
+#pragma unroll
+      for (int d = 0; d < kM; ++d) c.u[d] = u0[d];
+      x = propagate_dynamics(x, c, a.model_params + a.model_stride * agent, step, agent);
+#pragma unroll
+      for (int d = 0; d < kNPad; ++d) st[d] = x.s[d];
+    }
 #pragma unroll
     for (int d = 0; d < kN; ++d) xg[d] = st[d];
     if (a.terminal)

@@ -40,7 +40,7 @@ def test_feature_callable_has_one_compiled_copy():
 
 
 def test_propagate_has_one_compiled_copy():
-    prop = _body(r"__device__ __noinline__ void propagate_dynamics\(")
+    prop = _body(r"__device__ __noinline__ PropagateState propagate_dynamics\(")
     rollout = _body(r"__device__ __forceinline__ void rollout_item\(")
     calls = _calls("MPPI_DYNAMICS_FN")
     # the rollout's per-step recurrence and the propagate, nowhere else
