@@ -120,3 +120,21 @@ def test_reference_style_plugin_includes_resolve(tmp_path):
         "  s[1] += 0.1f * control[1];\n}\n")
     rc, err, _ = compile_check(str(src), 2, 2, stage_cost="", terminal_cost="")
     assert rc == 0, err
+
+
+def test_queries_before_initialize_report_not_init(lib):
+    """A created backend answers the measurement queries with
+    MPPI_ERR_NOT_INIT until initialize (no device call is made)."""
+    import ctypes
+    h = ctypes.c_void_p()
+    assert lib.mppi_backend_create(ctypes.byref(h)) == 0
+    try:
+        form = ctypes.c_uint32(99)
+        assert lib.mppi_backend_step_form(h, ctypes.byref(form)) == _lib.MPPI_ERR_NOT_INIT
+        assert form.value == 99
+        vals = [ctypes.c_uint32() for _ in range(5)]
+        assert lib.mppi_backend_launch_info(h, *[ctypes.byref(v) for v in vals]) == \
+            _lib.MPPI_ERR_NOT_INIT
+        assert lib.mppi_backend_step_form(None, ctypes.byref(form)) == _lib.MPPI_ERR_NOT_INIT
+    finally:
+        lib.mppi_backend_destroy(h)
