@@ -440,12 +440,15 @@ def run_b200(args):
             gpu_c = models.unicycle_executed_cost(
                 outs.states_out[:steps, :agents], outs.controls_out[:steps, :agents],
                 outs.states_out[steps, :agents], w.cost_params[:agents])
+            dt1, rs1, _ = reference_sample_run(w, 2, 2, 1)
             cpu = {"value": rs / dt, "unit": "rollout-steps/s", "cores": nthreads,
                    "kind": "reference",
                    "sample": f"{agents} agents x {steps} closed-loop steps at full K={K_SAMPLES}, "
                              f"H={HORIZON} (reference kernels compiled for the CPU)",
                    "closed_loop_cost_sample": c,
-                   "gpu_closed_loop_cost_same_sample": float(gpu_c.mean())}
+                   "gpu_closed_loop_cost_same_sample": float(gpu_c.mean()),
+                   "one_core": {"value": rs1 / dt1, "unit": "rollout-steps/s",
+                                "sample": "2 agents x 2 closed-loop steps, one thread"}}
 
     if rank != 0:
         dist.finish(R)
