@@ -6,19 +6,26 @@
 // application whose device memory is owned by another framework's allocator
 // and budgeted up front.  Such a caller keeps its own device buffers for the
 // inputs and outputs and calls mppi_backend_dispatch_rollout_noalloc each
-// control period; the temporary data of the step (per-sample costs, the
-// rollout blocks' partial sums) lives in the fixed array below instead of in
-// buffers the backend would otherwise allocate for the step.
+// control period; the temporary data of the step (the rollout blocks'
+// partial sums and the combine statistics) lives in the fixed array below
+// instead of in buffers the backend would otherwise allocate for the step.
 //
 // The array is a file-scope __device__ variable: every GPU that loads this
 // library holds MPPI_NOALLOC_SCRATCH_BYTES of it until the process exits.
 // In host code its name is only a host-side stand-in, so the device address
 // is looked up with cudaGetSymbolAddress, once per device, on that device's
 // first call; that first call should therefore come before any stream
-// capture.  All calls share the one array and it keeps the previous call's
-// contents (the entry point clears the part that must start at zero), so
-// calls whose work overlaps on the GPU -- from two threads, or on two
-// streams without ordering -- race on it.
+// capture.  The address is cached for the life of the process: a
+// cudaDeviceReset while this library is in use is not supported (it also
+// invalidates every backend's own buffers).  All calls share the one array
+// and it keeps the previous call's contents (the entry point clears the part
+// that must start at zero), so calls whose work overlaps on the GPU -- from
+// two threads, or on two streams without ordering -- race on it.
+//
+// The step runs on the backend's own stream: the caller's inputs must be
+// complete in device memory before the call (synchronise the stream that
+// wrote them), and the outputs are complete when the call returns.  The
+// caller's current device is restored before returning.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -32,7 +39,7 @@ namespace {
 
 constexpr size_t kScratchFloats = MPPI_NOALLOC_SCRATCH_BYTES / sizeof(float);
 
-// The step's scratch: zero block, per-sample costs, per-CTA partials, stats.
+// The step's scratch: zero block, per-CTA partial records, statistics.
 static __device__ __align__(256) float g_step_scratch[kScratchFloats];
 
 constexpr int kMaxDevices = 64;
@@ -47,6 +54,21 @@ void put_err(char* err, size_t len, const std::string& msg) {
   }
 }
 
+// Makes `dev` current for the lifetime of the object and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+  int prev = -1;
+  cudaError_t status = cudaSuccess;
+  explicit DeviceGuard(int dev) {
+    status = cudaGetDevice(&prev);
+    if (status == cudaSuccess && prev != dev) status = cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
 }  // namespace
 
 extern "C" int mppi_backend_dispatch_rollout_noalloc(
@@ -59,6 +81,13 @@ extern "C" int mppi_backend_dispatch_rollout_noalloc(
   }
   if (!x0 || !u_nominal || !u_out || !diag3) {
     put_err(err, err_len, "x0, u_nominal, u_out and diag3 must be device pointers, not null.");
+    return MPPI_ERR_INVALID;
+  }
+  if (mppi_b200::backend_has_proposal(b)) {
+    put_err(err, err_len,
+            "mppi_backend_dispatch_rollout_noalloc: a learned proposal network is attached; "
+            "this entry point runs plain MPPI only (detach it with mppi_backend_set_proposal("
+            "b, NULL, 0, ...) or use mppi_backend_dispatch_rollout).");
     return MPPI_ERR_INVALID;
   }
   const size_t need = mppi_b200::step_scratch_floats(b);
@@ -76,9 +105,9 @@ extern "C" int mppi_backend_dispatch_rollout_noalloc(
     put_err(err, err_len, "device ordinal out of range.");
     return MPPI_ERR_INVALID;
   }
-  cudaError_t e = cudaSetDevice(dev);
-  if (e != cudaSuccess) {
-    put_err(err, err_len, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  DeviceGuard guard(dev);
+  if (guard.status != cudaSuccess) {
+    put_err(err, err_len, std::string("cudaSetDevice: ") + cudaGetErrorString(guard.status));
     return MPPI_ERR_CUDA;
   }
   float* scratch = nullptr;
@@ -87,7 +116,7 @@ extern "C" int mppi_backend_dispatch_rollout_noalloc(
     std::lock_guard<std::mutex> lock(g_lookup_mutex);
     if (g_scratch_addr[dev] == nullptr) {
       void* p = nullptr;
-      e = cudaGetSymbolAddress(&p, g_step_scratch);
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_step_scratch);
       if (e != cudaSuccess || p == nullptr) {
         put_err(err, err_len, std::string("cudaGetSymbolAddress of the scratch array failed: ") +
                                   cudaGetErrorString(e));
@@ -106,7 +135,7 @@ extern "C" int mppi_backend_dispatch_rollout_noalloc(
     put_err(err, err_len, msg);
     return rc;
   }
-  e = cudaStreamSynchronize(s);
+  const cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     put_err(err, err_len, std::string("step failed: ") + cudaGetErrorString(e));
     return MPPI_ERR_CUDA;

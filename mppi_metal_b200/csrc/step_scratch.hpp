@@ -15,7 +15,7 @@ struct mppi_backend;
 namespace mppi_b200 {
 
 // Floats of scratch one step needs for the backend's configuration
-// (a zero word block, the per-sample costs, the per-CTA partials, stats).
+// (a zero word block, the per-CTA partials, the combine statistics).
 size_t step_scratch_floats(const mppi_backend* b);
 
 // Enqueues rollout + combine for one agent on `stream`.  Reads x0, u_nominal
@@ -32,5 +32,7 @@ int launch_step_with_scratch(mppi_backend* b, uint64_t step_index, const float* 
 int backend_device(const mppi_backend* b);
 cudaStream_t backend_stream(const mppi_backend* b);
 bool backend_initialized(const mppi_backend* b);
+// Whether a learned proposal network is attached (mppi_backend_set_proposal).
+bool backend_has_proposal(const mppi_backend* b);
 
 }  // namespace mppi_b200
