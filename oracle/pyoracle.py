@@ -32,6 +32,7 @@ MODEL_IDS = {
     "bicycle_lane": 3,
     "quadrotor": 4,
     "gust_integrator": 5,
+    "wez_environment": 6,
 }
 
 # Which oracle/_ref library runs the reference kernels for each model.
@@ -46,11 +47,15 @@ _u32 = ctypes.c_uint32
 _u64 = ctypes.c_uint64
 
 
-def build_oracle() -> None:
-    """Compile the FP64 oracle (and, where the reference tree exists, the
-    reference CPU libraries) with oracle/Makefile."""
+def build_oracle(ref_root: str | os.PathLike | None = None) -> None:
+    """Compile the FP64 oracle and, when the reference source tree is given
+    (``ref_root``, else the MPPI_REF_ROOT environment variable) and holds the
+    reference's shaders, the reference CPU libraries, with oracle/Makefile."""
     subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
-    ref_root = Path(os.environ.get("MPPI_REF_ROOT", "/root/reference"))
+    root = ref_root if ref_root is not None else os.environ.get("MPPI_REF_ROOT", "")
+    if not root:
+        return
+    ref_root = Path(root)
     if (ref_root / "shaders" / "mppi_rollout.metal").exists():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={ref_root}"], check=True)
         product = HERE.parent / "mppi_metal_b200" / "lib" / "libmppi_b200.so"
@@ -205,6 +210,17 @@ class Oracle:
         out = np.zeros(p.horizon * p.control_dim)
         self.lib.oracle_update_eps(ctypes.byref(s), _ptr(w), _ptr(u_nom), _ptr(eps), _ptr(out))
         return out
+
+    def dynamics(self, p: Problem, x, u, step: int = 0, key: int = 0) -> np.ndarray:
+        """One step x <- f(x, u) of the problem's model in double, with the
+        propagate's counter (step, 0x80000000) and the given key."""
+        s = self._prob(p)
+        xo = _f64(x).copy()
+        u = _f64(u)
+        mp = ctypes.create_string_buffer(p.model_params or b"\0", max(1, len(p.model_params)))
+        self.lib.oracle_dynamics(ctypes.byref(s), _ptr(xo), _ptr(u), mp, _u32(step),
+                                 _u32(0x80000000), _u32(key))
+        return xo
 
     def weights(self, costs, lam: float):
         costs = _f64(costs)
