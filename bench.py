@@ -9,11 +9,19 @@ control steps.  One benchmark step = one such closed loop
 rollout -> weights -> update -> propagate & shift.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--workload NAME] [--workloads all|none]
 
 value : rollout-steps/s over all ranks, inputs resident in HBM (device
         time, CUDA events on the library's stream, max over ranks)
 e2e   : the same metric through the public C ABI call with host buffers
         (host->device inputs and device->host histories inside the timing)
+workloads : on one GPU the default line also carries every other
+        configuration, each measured the same way (at most 5 timed loops):
+        the single agent, the uneven bicycle batch, the quadrotor batch in
+        FP32 and mixed mode, and the learned proposal against plain MPPI
+        (unicycle K 256 / 1024 vs K 4096; quadrotor K 4096 vs K 65536) with
+        its speed-up and closed-loop cost ratio.  --workload NAME measures
+        one of them alone as the line.
 --impl reference : the reference's own kernels (its Metal shader sources
         compiled for the CPU, oracle/_ref) on the host cores, on a bounded
         sample of the same workload.
@@ -76,6 +84,9 @@ def parse():
                          "quadrotor, proposal, quadrotor_proposal")
     ap.add_argument("--numeric", choices=["fp32", "mixed"], default="fp32",
                     help="numeric mode of the quadrotor workload")
+    ap.add_argument("--workloads", choices=["all", "none"], default="all",
+                    help="with the default (batch) workload on one GPU: also measure every "
+                         "other configuration and report them under `workloads`")
     ap.add_argument("--proposal-weights", default="",
                     help="proposal workload: load the network from this .npz instead of "
                          "training it on the GPU first (python -m mppi_metal_b200.proposal)")
@@ -327,66 +338,52 @@ def config_block(name: str = "batch", w=None):
 # ---------------------------------------------------------------------------
 # the B200 path
 # ---------------------------------------------------------------------------
-def run_b200(args):
-    import torch
-    from mppi_metal_b200 import dist
-    R = dist.env()
-    rank, world, local_rank = R.rank, R.world, R.local_rank
-    torch.cuda.set_device(local_rank if world > 1 else 0)
-    dist.init(R, "nccl", timeout_s=300)
+class Ctx:
+    """Rank plumbing shared by every measured workload of one run."""
+
+    def __init__(self):
+        import torch
+        from mppi_metal_b200 import dist
+        self.dist = dist
+        self.R = dist.env()
+        self.rank, self.world, self.local_rank = self.R.rank, self.R.world, self.R.local_rank
+        torch.cuda.set_device(self.local_rank if self.world > 1 else 0)
+        dist.init(self.R, "nccl", timeout_s=900)
+        self.flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+        self.gpu = physical_gpu_index(self.local_rank)
+
+    def barrier(self):
+        self.dist.barrier(self.R, "cuda")
+
+    def max_over_ranks(self, x: float) -> float:
+        return self.dist.max_over_ranks(self.R, x, "cuda")
+
+    def flush_l2(self):
+        import torch
+        self.flush.zero_()
+        torch.cuda.synchronize()
+
+    def finish(self):
+        self.dist.finish(self.R)
+
+
+def load_peaks() -> dict:
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+def make_driver(w, K=None, options=None):
+    """MPPIDriver for a workload through the public API (host buffers)."""
     from mppi_metal_b200 import driver as D
-    from mppi_metal_b200 import models
     from mppi_metal_b200._lib import plugin_path
-    from mppi_metal_b200.backend import Backend
-
-    w = workload_for_rank(rank, args.workload, args.numeric)  # per-rank seed: disjoint agents
-    N, T = w.num_agents, w.num_steps
-    ks, hs = agent_shapes(w)
-    rs_per_step = rollout_steps_per_control_step(w) * T  # per bench step (this rank)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-
-    def barrier():
-        dist.barrier(R, "cuda")
-
-    def max_over_ranks(x: float) -> float:
-        return dist.max_over_ranks(R, x, "cuda")
-
-    # ---- value: device-resident closed loop ---------------------------------
-    b = Backend(w.plugin, w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam, w.sigma,
-                w.u_min, w.u_max, sigma_inv=w.sigma_inv, cov_full=w.cov_full,
-                control_cost=w.control_cost, model_params_size=len(w.model_params),
-                cost_params_size=w.cost_stride, seed=w.seed, numeric_mode=w.numeric_mode)
-    b.bind_params(w.model_params, w.cost_params[0])
-    b.prepare(N, T, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
-              sigma=w.agent_sigma, sample_counts=ks, horizons=hs)
-    for _ in range(args.warmup):
-        b.run(0)
-        b.last_run_ms()
-    times = []
-    barrier()
-    with ClockSampler(physical_gpu_index(local_rank)) as clocks:
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            b.run(0)
-            times.append(b.last_run_ms())
-    barrier()
-    total_ms = max_over_ranks(sum(times))
-    value = world * rs_per_step * args.steps / (total_ms / 1e3)
-
-    # ---- kernel-level timing for the roofline --------------------------------
-    rollout_ms, combine_ms = b.time_passes(20)
-    geom = b.launch_info()
-    tuning = b.tuning_info()
-    b.close()
-
-    # ---- e2e: public API, host buffers ---------------------------------------
     form = D.CovarianceForm.kFull if w.cov_full else D.CovarianceForm.kDiagonal
-    cfg = D.DriverConfig(w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam,
+    cfg = D.DriverConfig(w.state_dim, w.control_dim, w.horizon, K or w.sample_count, w.lam,
                          D.ControlNoiseConfig(form, w.sigma, w.sigma_inv, w.control_dim),
                          D.ControlBounds(w.u_min, w.u_max, w.control_dim),
                          D.NumericMode(w.numeric_mode))
-    drv = D.MPPIDriver(cfg, D.DriverOptions(control_cost=w.control_cost))
+    drv = D.MPPIDriver(cfg, options or D.DriverOptions(control_cost=w.control_cost))
     err = D.ErrorRef()
     spec = D.ModelPluginSpec(plugin_path(w.plugin),
                              D.CallableNames("mppi_dynamics", "mppi_stage_cost",
@@ -396,67 +393,129 @@ def run_b200(args):
     assert drv.initialize(spec, err), err.value
     assert drv.set_problem_params(D.ProblemParams(D.ByteView.of(w.model_params),
                                                   D.ByteView.of(w.cost_params[0])), err), err.value
-    agent_params = D.BatchAgentParams(cost_params=w.cost_params_packed,
-                                      cost_params_stride=w.cost_stride, sigma=w.agent_sigma,
-                                      sample_counts=ks, horizons=hs)
+    return drv
+
+
+def timed_e2e(ctx, drv, w, agent_params, steps, warmup):
+    """`steps` calls of MPPIDriver::simulate_batch with host buffers (x0, the
+    per-agent blobs and sigma go up, the histories come down), after
+    `warmup` untimed calls; returns (seconds, outputs of the last call)."""
+    from mppi_metal_b200 import driver as D
+    N, T = w.num_agents, w.num_steps
+    err = D.ErrorRef()
     outs = D.BatchSimulationResults(np.zeros((T, N, w.state_dim), np.float32),
                                     np.zeros((T, N, w.control_dim), np.float32),
                                     np.zeros((T, N), np.float32),
                                     np.zeros((N, w.state_dim), np.float32), N, T)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         assert drv.reset(None, err)
         assert drv.simulate_batch(N, T, w.x0, outs, agent_params, err), err.value
-    e2e_times = []
-    barrier()
-    for _ in range(args.steps):
+    times = []
+    ctx.barrier()
+    for _ in range(steps):
         assert drv.reset(None, err)
         t0 = time.perf_counter()
         assert drv.simulate_batch(N, T, w.x0, outs, agent_params, err), err.value
-        e2e_times.append(time.perf_counter() - t0)
-    barrier()
-    e2e_total = max_over_ranks(sum(e2e_times))
-    # executed closed-loop cost of the last API call (from x0, step index 0)
-    cost = models.executed_cost(w, outs.states_out, outs.controls_out,
-                                outs.terminal_states_out)
-    e2e_value = world * rs_per_step * args.steps / e2e_total
-    HM = w.horizon * w.control_dim
-    sig_len = w.control_dim * w.control_dim if w.cov_full else w.control_dim
+        times.append(time.perf_counter() - t0)
+    ctx.barrier()
+    return ctx.max_over_ranks(sum(times)), outs
+
+
+def e2e_bytes(w, ks=None):
+    """Host<->device bytes of one simulate_batch call: x0, zero nominals,
+    per-agent blobs and sigma up; state, control and cost histories and the
+    terminal states down."""
+    N, T, HM = w.num_agents, w.num_steps, w.horizon * w.control_dim
+    sig_len = (w.control_dim * w.control_dim if w.cov_full else w.control_dim) \
+        if w.agent_sigma is not None else 0
     h2d = (N * w.state_dim + N * HM + 4) * 4 + N * ((w.cost_stride + 15) // 16 * 16) \
         + N * sig_len * 4
     if ks is not None:
         work_items = int(sum((int(k) + 127) // 128 for k in ks))
         h2d += 12 * N + 8 * work_items  # per-agent K / H / offsets and the work list
     d2h = (T * N * (w.state_dim + w.control_dim + 1) + N * w.state_dim) * 4
+    return h2d, d2h
+
+
+def measure_workload(ctx, args, name: str, numeric: str, steps: int, warmup: int,
+                     with_cpu: bool) -> dict:
+    """One plain-MPPI workload: device-resident closed loops (value), the
+    same through MPPIDriver::simulate_batch with host buffers (e2e), the
+    rollout kernel's live launch time against the issue roofline, and (rank
+    0, one GPU, the batched configuration) the reference's CPU kernels."""
+    from mppi_metal_b200 import driver as D
+    from mppi_metal_b200 import models
+    from mppi_metal_b200.backend import Backend
+
+    w = workload_for_rank(ctx.rank, name, numeric)  # per-rank seed: disjoint agents
+    N, T = w.num_agents, w.num_steps
+    ks, hs = agent_shapes(w)
+    rs_per_step = rollout_steps_per_control_step(w) * T  # per bench step (this rank)
+
+    # ---- value: device-resident closed loop ---------------------------------
+    b = Backend(w.plugin, w.state_dim, w.control_dim, w.horizon, w.sample_count, w.lam, w.sigma,
+                w.u_min, w.u_max, sigma_inv=w.sigma_inv, cov_full=w.cov_full,
+                control_cost=w.control_cost, model_params_size=len(w.model_params),
+                cost_params_size=w.cost_stride, seed=w.seed, numeric_mode=w.numeric_mode)
+    b.bind_params(w.model_params, w.cost_params[0])
+    b.prepare(N, T, w.x0, cost_params=w.cost_params_packed, cost_stride=w.cost_stride,
+              sigma=w.agent_sigma, sample_counts=ks, horizons=hs)
+    for _ in range(warmup):
+        b.run(0)
+        b.last_run_ms()
+    times = []
+    ctx.barrier()
+    with ClockSampler(ctx.gpu) as clocks:
+        for _ in range(steps):
+            ctx.flush_l2()
+            b.run(0)
+            times.append(b.last_run_ms())
+    ctx.barrier()
+    total_ms = ctx.max_over_ranks(sum(times))
+    value = ctx.world * rs_per_step * steps / (total_ms / 1e3)
+
+    # ---- kernel-level timing for the roofline --------------------------------
+    rollout_ms, combine_ms = b.time_passes(20)
+    geom = b.launch_info()
+    tuning = b.tuning_info()
+    b.close()
+
+    # ---- e2e: public API, host buffers ---------------------------------------
+    drv = make_driver(w)
+    agent_params = D.BatchAgentParams(cost_params=w.cost_params_packed,
+                                      cost_params_stride=w.cost_stride, sigma=w.agent_sigma,
+                                      sample_counts=ks, horizons=hs)
+    e2e_total, outs = timed_e2e(ctx, drv, w, agent_params, steps, warmup)
+    # executed closed-loop cost of the last API call (from x0, step index 0)
+    cost = models.executed_cost(w, outs.states_out, outs.controls_out, outs.terminal_states_out)
+    e2e_value = ctx.world * rs_per_step * steps / e2e_total
+    h2d, d2h = e2e_bytes(w, ks)
 
     # ---- CPU baseline (rank 0, N = 1 only) ------------------------------------
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload == "batch":
+    if with_cpu and ctx.rank == 0 and ctx.world == 1 and not args.no_cpu_baseline:
         lib = ROOT / "oracle" / "_ref" / "libmppi_ref_unicycle_obstacles.so"
         if lib.exists():
             nthreads = os.cpu_count() or 1
-            agents, steps = choose_reference_sample(w, nthreads, target_s=5.0)
-            dt, rs, c = reference_sample_run(w, agents, steps, nthreads)
+            agents, csteps = choose_reference_sample(w, nthreads, target_s=5.0)
+            dt, rs, c = reference_sample_run(w, agents, csteps, nthreads)
             # the GPU's executed cost on the same agents over the same steps
             gpu_c = models.unicycle_executed_cost(
-                outs.states_out[:steps, :agents], outs.controls_out[:steps, :agents],
-                outs.states_out[steps, :agents], w.cost_params[:agents])
+                outs.states_out[:csteps, :agents], outs.controls_out[:csteps, :agents],
+                outs.states_out[csteps, :agents], w.cost_params[:agents])
             dt1, rs1, _ = reference_sample_run(w, 2, 2, 1)
             cpu = {"value": rs / dt, "unit": "rollout-steps/s", "cores": nthreads,
                    "kind": "reference",
-                   "sample": f"{agents} agents x {steps} closed-loop steps at full K={K_SAMPLES}, "
-                             f"H={HORIZON} (reference kernels compiled for the CPU)",
+                   "sample": f"{agents} agents x {csteps} closed-loop steps at full "
+                             f"K={K_SAMPLES}, H={HORIZON} (reference kernels compiled for the CPU)",
                    "closed_loop_cost_sample": c,
                    "gpu_closed_loop_cost_same_sample": float(gpu_c.mean()),
                    "one_core": {"value": rs1 / dt1, "unit": "rollout-steps/s",
                                 "sample": "2 agents x 2 closed-loop steps, one thread"}}
 
-    if rank != 0:
-        dist.finish(R)
-        return 0
-
     rollout_units = rollout_steps_per_control_step(w)  # rollout-steps per rollout launch
     kname = "mppi_rollout_work_b128" if ks is not None else "mppi_rollout_b%d" % geom["block"]
-    key = args.workload + ("/" + args.numeric if args.workload == "quadrotor" else "")
+    key = name + ("/" + numeric if name == "quadrotor" else "")
     inst, dram = ROLLOUT_COUNTERS.get(key, (None, None))
     roof = {"kernel": kname, "bound": "issue",
             "launch_ms": rollout_ms, "combine_launch_ms": combine_ms,
@@ -473,29 +532,79 @@ def run_b200(args):
         roof.update({"achieved": achieved, "peak": peak, "frac": achieved / peak,
                      "warp_inst_per_rollout_step": inst,
                      "peak_basis": f"148 SMs x 4 warp-inst/clk x {mhz:.0f} MHz (sampled)"})
-    line = {
-        "metric": METRIC, "value": value, "unit": "rollout-steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+    return {
+        "metric": METRIC, "value": value, "unit": "rollout-steps/s", "n_gpus": ctx.world,
+        "steps": steps, "warmup": warmup, "ms_per_step": total_ms / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32" if w.numeric_mode == 0 else "fp32 (fp16 noise)",
         "data": "synthetic (seeded PCG64 workload generator, mppi_metal_b200/models.py)",
-        "config": config_block(args.workload, w),
+        "config": config_block(name, w),
         "control_steps_per_s": value * N / rollout_steps_per_control_step(w),
         "closed_loop_cost": {"mean": float(cost.mean()), "agents": N,
                              "mean_first_agents": float(cost[:8].mean())},
         "e2e": {"value": e2e_value, "unit": "rollout-steps/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e2e_total / args.steps},
-        "gpu_launches": geom["kernels_per_step"] * T * args.steps,
+                "d2h_bytes_per_step": d2h, "ms_per_step": 1e3 * e2e_total / steps,
+                "control_steps_per_s": e2e_value * N / rollout_steps_per_control_step(w)},
+        "gpu_launches": geom["kernels_per_step"] * T * steps,
         "launch_geometry": geom,
         "autotuner": tuning or None,
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clk,
     }
-    print(json.dumps(line))
-    dist.finish(R)
+
+
+def run_b200(args):
+    ctx = Ctx()
+    try:
+        if args.workload in ("proposal", "quadrotor_proposal"):
+            line = measure_proposal(ctx, args, args.workload, args.steps, args.warmup)
+        else:
+            line = measure_workload(ctx, args, args.workload, args.numeric, args.steps,
+                                    args.warmup, with_cpu=args.workload == "batch")
+            if args.workload == "batch" and args.workloads == "all" and ctx.world == 1:
+                line["workloads"] = other_workloads(ctx, args)
+        if ctx.rank == 0:
+            print(json.dumps(line))
+    finally:
+        ctx.finish()
     return 0
 
+
+# Keys of a workload's line kept in the headline line's `workloads` block.
+SUMMARY_KEYS = ("value", "unit", "control_steps_per_s", "steps", "warmup", "ms_per_step",
+                "dtype", "closed_loop_cost", "e2e", "gpu_launches", "roofline", "clocks",
+                "launch_geometry", "autotuner", "plain", "speedup_vs_plain", "arms", "training",
+                "kernel_ms_per_pass", "rollout_steps_per_s")
+
+
+def summarise(line: dict) -> dict:
+    out = {k: line[k] for k in SUMMARY_KEYS if k in line and line[k] is not None}
+    out["workload"] = line["config"]["workload"]
+    return out
+
+
+def other_workloads(ctx, args) -> dict:
+    """Every other configuration, each measured as its own `--workload` line
+    would be (device-resident closed loops + the public API with host
+    buffers), with at most 5 timed and 3 warm-up loops each, so the default
+    run stays within a few minutes.  Runs on one GPU (the scaling runs
+    measure the headline configuration)."""
+    steps = max(1, min(args.steps, 5))
+    warmup = 3
+    out = {}
+    for key, name, numeric in (("single", "single", "fp32"), ("uneven", "uneven", "fp32"),
+                               ("quadrotor_fp32", "quadrotor", "fp32"),
+                               ("quadrotor_mixed", "quadrotor", "mixed")):
+        out[key] = summarise(measure_workload(ctx, args, name, numeric, steps, warmup,
+                                              with_cpu=False))
+    qf, qm = out["quadrotor_fp32"], out["quadrotor_mixed"]
+    qm["vs_fp32"] = {"value": qm["value"] / qf["value"],
+                     "closed_loop_cost": qm["closed_loop_cost"]["mean"]
+                     / qf["closed_loop_cost"]["mean"]}
+    for key in ("proposal", "quadrotor_proposal"):
+        out[key] = summarise(measure_proposal(ctx, args, key, steps, warmup))
+    return out
 
 def run_kernels_only(args):
     """Prepares the workload and launches the rollout and combine kernels
@@ -548,21 +657,22 @@ PROPOSAL_H = 64
 
 def proposal_spec(name: str) -> dict:
     """proposal          : 128 unicycle agents x 300 steps, H 64; proposal-MPPI
-                          K 256 (128 around the prediction) vs plain K 4096
+                          K 256 (128 around the prediction) and K 1024 (512
+                          around it) vs plain K 4096
     quadrotor_proposal : 32 quadrotors x 100 steps, H 100; proposal-MPPI K 4096
                           (1024 around the prediction, the network predicts 60
                           steps) vs plain K 65536"""
     from mppi_metal_b200 import models
     from mppi_metal_b200 import proposal as P
     if name == "quadrotor_proposal":
-        return dict(agents=32, K=4096, samples=1024, plain_K=65536, H=100, T=100, net_H=60,
+        return dict(agents=32, arms=[(4096, 1024)], plain_K=65536, H=100, T=100, net_H=60,
                     features=P.QUADROTOR_FEATURES, label="quadrotor",
                     make=lambda rank: models.quadrotor_batch(seed=4100 + rank, N=32, K=65536,
                                                              H=100, T=100),
                     train=P.train_quadrotor_proposal,
                     data="plain MPPI K=65536, H=100, 4 seeds x 256 agents x 100 steps",
                     desc="32 quadrotors per GPU (n=12, m=4, dt=0.01, 32 spherical obstacles)")
-    return dict(agents=PROPOSAL_AGENTS, K=PROPOSAL_K, samples=PROPOSAL_SAMPLES,
+    return dict(agents=PROPOSAL_AGENTS, arms=[(PROPOSAL_K, PROPOSAL_SAMPLES), (1024, 512)],
                 plain_K=PROPOSAL_PLAIN_K, H=PROPOSAL_H, T=CLOSED_LOOP_STEPS, net_H=PROPOSAL_H,
                 features=P.UNICYCLE_FEATURES, label="unicycle",
                 make=lambda rank: models.unicycle_batch(seed=4000 + rank, N=PROPOSAL_AGENTS,
@@ -573,29 +683,17 @@ def proposal_spec(name: str) -> dict:
                 desc="128 unicycle agents per GPU (16 moving obstacles, sigma U[0.2,0.8])")
 
 
-def run_proposal(args):
-    """Proposal-MPPI against plain MPPI with 16x the samples, on the same
-    agents (proposal_spec).  value = control steps/s of the proposal arm;
-    the plain arm's rate and both closed-loop costs ride along.  Setup (not
-    timed): the network is trained on this GPU by the library's kernels on
-    (features, u*) pairs from plain MPPI."""
-    import torch
-    from mppi_metal_b200 import dist
-    R = dist.env()
-    rank, world, local_rank = R.rank, R.world, R.local_rank
-    torch.cuda.set_device(local_rank if world > 1 else 0)
-    dist.init(R, "nccl", timeout_s=900)
+def measure_proposal(ctx, args, name: str, steps: int, warmup: int) -> dict:
+    """Proposal-MPPI against plain MPPI with more samples, on the same agents
+    (proposal_spec).  value = control steps/s of the first proposal arm;
+    every arm carries its rate, e2e, closed-loop cost and the ratios to the
+    plain arm.  Setup (not timed): the network is trained on this GPU by the
+    library's kernels on (features, u*) pairs from plain MPPI."""
+    import torch  # noqa: F401  (CUDA context for the network's buffers)
     from mppi_metal_b200 import driver as D
     from mppi_metal_b200 import models
     from mppi_metal_b200 import proposal as P
-    from mppi_metal_b200._lib import plugin_path
-    spec = proposal_spec(args.workload)
-
-    def barrier():
-        dist.barrier(R, "cuda")
-
-    def max_over_ranks(x: float) -> float:
-        return dist.max_over_ranks(R, x, "cuda")
+    spec = proposal_spec(name)
 
     t_setup = time.time()
     if args.proposal_weights and Path(args.proposal_weights).exists():
@@ -608,141 +706,125 @@ def run_proposal(args):
                     "data": spec["data"]}
     training["setup_s"] = round(time.time() - t_setup, 1)
 
-    w = spec["make"](rank)
-    N, T, K, KS = w.num_agents, w.num_steps, spec["K"], spec["samples"]
+    w = spec["make"](ctx.rank)
+    N, T = w.num_agents, w.num_steps
     n, m, H = w.state_dim, w.control_dim, w.horizon
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def timed_arm(b):
         P._prepare(b, w)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             b.run(0)
             b.last_run_ms()
         times = []
-        barrier()
-        with ClockSampler(physical_gpu_index(local_rank)) as clocks:
-            for _ in range(args.steps):
-                flush.zero_()
-                torch.cuda.synchronize()
+        ctx.barrier()
+        with ClockSampler(ctx.gpu) as clocks:
+            for _ in range(steps):
+                ctx.flush_l2()
                 P._prepare(b, w)  # every timed loop starts from x0 and a zero nominal
                 b.run(0)
                 times.append(b.last_run_ms())
-        barrier()
+        ctx.barrier()
         r = b.fetch()
         cost = models.executed_cost(w, r["states"], r["controls"], r["terminal"])
-        return max_over_ranks(sum(times)), cost, clocks.summary()
+        return ctx.max_over_ranks(sum(times)), cost, clocks.summary()
 
     plain = P.make_backend(w, spec["plain_K"])
-    plain_ms, plain_cost, _ = timed_arm(plain)
+    plain_ms, plain_cost, plain_clk = timed_arm(plain)
+    plain_form = plain.launch_info()
     plain.close()
-    prop = P.make_backend(w, K)
-    prop.set_features(P.FEATURES_CALLABLE, spec["features"])
-    prop.set_proposal(net, KS)
-    prop_ms, prop_cost, clk = timed_arm(prop)
-    kernels_per_step = prop.launch_info()["kernels_per_step"]  # network + rollout(+combine)
-    rollout_ms, combine_ms = prop.time_passes(20)
-    feat_ms, net_ms = prop.time_proposal(20)
-    prop.set_proposal(None)
-    prop.close()
-    value = world * N * T * args.steps / (prop_ms / 1e3)
-    plain_value = world * N * T * args.steps / (plain_ms / 1e3)
+    plain_value = ctx.world * N * T * steps / (plain_ms / 1e3)
 
-    # ---- e2e: public API (DriverOptions.proposal), host buffers --------------
-    cfg = D.DriverConfig(n, m, H, K, w.lam,
-                         D.ControlNoiseConfig(D.CovarianceForm.kDiagonal, w.sigma, w.sigma_inv, m),
-                         D.ControlBounds(w.u_min, w.u_max, m))
-    drv = D.MPPIDriver(cfg, D.DriverOptions(proposal=net, proposal_samples=KS))
-    err = D.ErrorRef()
-    dspec = D.ModelPluginSpec(plugin_path(w.plugin),
-                              D.CallableNames("mppi_dynamics", "mppi_stage_cost",
-                                              "mppi_terminal_cost"),
-                              D.ParamLayout(len(w.model_params), 4, w.cost_stride, 4),
-                              D.RngConfig(w.seed))
-    assert drv.initialize(dspec, err), err.value
-    assert drv.set_problem_params(D.ProblemParams(D.ByteView.of(w.model_params),
-                                                  D.ByteView.of(w.cost_params[0])), err), err.value
-    ap = D.BatchAgentParams(cost_params=w.cost_params_packed, cost_params_stride=w.cost_stride,
-                            sigma=w.agent_sigma)
-    outs = D.BatchSimulationResults(np.zeros((T, N, n), np.float32),
-                                    np.zeros((T, N, m), np.float32), np.zeros((T, N), np.float32),
-                                    np.zeros((N, n), np.float32), N, T)
-    for _ in range(args.warmup):
-        assert drv.reset(None, err)
-        assert drv.simulate_batch(N, T, w.x0, outs, ap, err), err.value
-    e2e_times = []
-    barrier()
-    for _ in range(args.steps):
-        assert drv.reset(None, err)
-        t0 = time.perf_counter()
-        assert drv.simulate_batch(N, T, w.x0, outs, ap, err), err.value
-        e2e_times.append(time.perf_counter() - t0)
-    barrier()
-    e2e_total = max_over_ranks(sum(e2e_times))
-    e2e_cost = models.executed_cost(w, outs.states_out, outs.controls_out,
-                                    outs.terminal_states_out)
-    sig_len = m if w.agent_sigma is not None else 0
-    h2d = (N * n + N * H * m + 4) * 4 + N * ((w.cost_stride + 15) // 16 * 16) + N * sig_len * 4
-    d2h = (T * N * (n + m + 1) + N * n) * 4
-
-    if rank != 0:
-        dist.finish(R)
-        return 0
     # network forward: 2 * rows * (32*256 + 2*256*256 + 256*P) FLOPs
     out_pad = (spec["net_H"] * m + m + 15) // 16 * 16
     mlp_flops = 2 * N * (32 * 256 + 2 * 256 * 256 + 256 * out_pad)
-    peaks = {}
-    try:
-        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
-    except Exception:
-        pass
+    peaks = load_peaks()
     bf16_peak = peaks.get("bf16_tflops") or 1590.0
-    line = {
-        "metric": METRIC, "value": value, "unit": "control-steps/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": prop_ms / args.steps,
+    h2d, d2h = e2e_bytes(w)
+    arms = []
+    for K, KS in spec["arms"]:
+        prop = P.make_backend(w, K)
+        prop.set_features(P.FEATURES_CALLABLE, spec["features"])
+        prop.set_proposal(net, KS)
+        prop_ms, prop_cost, clk = timed_arm(prop)
+        kernels_per_step = prop.launch_info()["kernels_per_step"]  # network + rollout(+combine)
+        form = prop.launch_info()
+        rollout_ms, combine_ms = prop.time_passes(20)
+        feat_ms, net_ms = prop.time_proposal(20)
+        prop.set_proposal(None)
+        prop.close()
+        value = ctx.world * N * T * steps / (prop_ms / 1e3)
+
+        # ---- e2e: public API (DriverOptions.proposal), host buffers ----------
+        drv = make_driver(w, K, D.DriverOptions(proposal=net, proposal_samples=KS))
+        ap = D.BatchAgentParams(cost_params=w.cost_params_packed,
+                                cost_params_stride=w.cost_stride, sigma=w.agent_sigma)
+        e2e_total, outs = timed_e2e(ctx, drv, w, ap, steps, warmup)
+        e2e_cost = models.executed_cost(w, outs.states_out, outs.controls_out,
+                                        outs.terminal_states_out)
+        del drv
+        arms.append({
+            "samples": K, "proposal_samples": KS,
+            "value": value, "unit": "control-steps/s", "ms_per_step": prop_ms / steps,
+            "rollout_steps_per_s": value * K * H,
+            "closed_loop_cost": {"mean": float(prop_cost.mean()), "agents": N,
+                                 "vs_plain": float(prop_cost.mean() / plain_cost.mean())},
+            "speedup_vs_plain": value / plain_value,
+            "e2e": {"value": ctx.world * N * T * steps / e2e_total, "unit": "control-steps/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": 1e3 * e2e_total / steps,
+                    "closed_loop_cost_mean": float(e2e_cost.mean())},
+            "gpu_launches": (kernels_per_step * T + 1) * steps,
+            "launch_geometry": form,
+            "kernel_ms_per_pass": {"rollout": rollout_ms, "combine": combine_ms,
+                                   "features_kernel": feat_ms, "network": net_ms},
+            "roofline": {"kernel": "mlp_forward_cluster_kernel (proposal network forward)",
+                         "bound": "tensor",
+                         "achieved": mlp_flops / (net_ms / 1e3) / 1e12, "peak": bf16_peak,
+                         "unit": "TFLOP/s",
+                         "frac": mlp_flops / (net_ms / 1e3) / 1e12 / bf16_peak,
+                         "traffic": None,
+                         "note": f"M = {N} rows: one 8-CTA cluster, latency-bound; the "
+                                 "dominant kernel of the step is the rollout (issue-bound, "
+                                 "see the batch workload); peak = measured bf16 burst"
+                                 + ("" if peaks.get("bf16_tflops") else " (fallback)")},
+            "clocks": clk,
+        })
+    first = arms[0]
+    arm_txt = " and ".join(f"K={a['samples']} ({a['proposal_samples']} around the prediction)"
+                           for a in arms)
+    return {
+        "metric": METRIC, "value": first["value"], "unit": "control-steps/s",
+        "n_gpus": ctx.world, "steps": steps, "warmup": warmup,
+        "ms_per_step": first["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32 rollout, bf16 network (fp32 accumulate)",
         "data": "synthetic (seeded PCG64 workload generator, mppi_metal_b200/models.py)",
         "config": {
-            "workload": (f"{args.workload}: {spec['desc']}, H={H}, {T} closed-loop steps; "
-                         f"proposal-MPPI K={K} ({KS} samples around the network's prediction) "
-                         f"against plain MPPI K={spec['plain_K']}"),
-            "agents_per_gpu": N, "samples": K, "proposal_samples": KS,
+            "workload": (f"{name}: {spec['desc']}, H={H}, {T} closed-loop steps; "
+                         f"proposal-MPPI {arm_txt} against plain MPPI K={spec['plain_K']}"),
+            "agents_per_gpu": N, "samples": first["samples"],
+            "proposal_samples": first["proposal_samples"],
             "plain_samples": spec["plain_K"], "horizon": H, "closed_loop_steps": T,
-            "network": (f"MLP {spec['features']}->256->256->256->{spec['net_H'] * m + m}, GELU, "
-                        f"bf16 weights, fp32 accumulate; predicts {spec['net_H']} steps"),
+            "network": (f"MLP {spec['features']}->256->256->256->{spec['net_H'] * m + m}, "
+                        f"GELU, bf16 weights, fp32 accumulate; predicts {spec['net_H']} steps"),
             "step": f"one simulate_batch closed loop ({T} control steps for every agent)",
             "l2": "flushed between timed iterations (256 MiB device write)",
             "parallelism": "agent-sharded replicas, no data-path collective",
         },
-        "rollout_steps_per_s": value * K * H,
+        "rollout_steps_per_s": first["rollout_steps_per_s"],
         "plain": {"control_steps_per_s": plain_value, "samples": spec["plain_K"],
-                  "ms_per_step": plain_ms / args.steps,
-                  "closed_loop_cost_mean": float(plain_cost.mean())},
-        "closed_loop_cost": {"mean": float(prop_cost.mean()), "agents": N,
-                             "vs_plain": float(prop_cost.mean() / plain_cost.mean())},
-        "speedup_vs_plain": value / plain_value,
+                  "ms_per_step": plain_ms / steps, "launch_geometry": plain_form,
+                  "closed_loop_cost_mean": float(plain_cost.mean()), "clocks": plain_clk},
+        "closed_loop_cost": first["closed_loop_cost"],
+        "speedup_vs_plain": first["speedup_vs_plain"],
+        "arms": arms,
         "training": training,
-        "e2e": {"value": world * N * T * args.steps / e2e_total, "unit": "control-steps/s",
-                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "ms_per_step": 1e3 * e2e_total / args.steps,
-                "closed_loop_cost_mean": float(e2e_cost.mean())},
-        "gpu_launches": (kernels_per_step * T + 1) * args.steps,
-        "kernel_ms_per_pass": {"rollout": rollout_ms, "combine": combine_ms,
-                               "features_kernel": feat_ms, "network": net_ms},
-        "roofline": {"kernel": "mlp_forward_cluster_kernel (proposal network forward)",
-                     "bound": "tensor",
-                     "achieved": mlp_flops / (net_ms / 1e3) / 1e12, "peak": bf16_peak,
-                     "unit": "TFLOP/s", "frac": mlp_flops / (net_ms / 1e3) / 1e12 / bf16_peak,
-                     "traffic": None,
-                     "note": f"M = {N} rows: one 8-CTA cluster, latency-bound; the dominant "
-                             "kernel of the step is the rollout (issue-bound, see the batch "
-                             "workload); peak = measured bf16 burst"
-                             + ("" if peaks.get("bf16_tflops") else " (fallback)")},
-        "clocks": clk,
+        "e2e": first["e2e"],
+        "gpu_launches": sum(a["gpu_launches"] for a in arms),
+        "kernel_ms_per_pass": first["kernel_ms_per_pass"],
+        "roofline": first["roofline"],
+        "clocks": first["clocks"],
     }
-    print(json.dumps(line))
-    dist.finish(R)
-    return 0
 
 
 def main():
@@ -751,8 +833,6 @@ def main():
         return run_reference(args)
     if args.mode == "kernels":
         return run_kernels_only(args)
-    if args.workload in ("proposal", "quadrotor_proposal"):
-        return run_proposal(args)
     return run_b200(args)
 
 

@@ -36,6 +36,13 @@ extern "C" {
 
 typedef struct mppi_backend mppi_backend;
 
+/* Largest state (floats).  The reference keeps the state in a 128-byte
+ * thread-local buffer and silently truncates larger ones
+ * (shaders/mppi_core.h:32); each module here sizes that buffer from
+ * state_dim instead -- at least 128 bytes, the reference's value, so its
+ * plugins see the same MPPI_MAX_STATE_BYTES -- up to this limit. */
+#define MPPI_MAX_STATE_DIM 128
+
 /* DriverConfig as the backend needs it (reference mppi_types.hpp:46-62). */
 typedef struct mppi_backend_config {
   uint32_t state_dim;
@@ -65,6 +72,15 @@ typedef struct mppi_backend_plugin {
   uint64_t model_params_size; /* ParamLayout sizes: every blob bound or */
   uint64_t cost_params_size;  /* overridden later has exactly this size */
   uint64_t seed;              /* RngConfig::seed; the device key is its low 32 bits */
+  /* ParamLayout alignments (0 or 1: unspecified) and schema_hash (NULL or
+   * "": none).  A plugin that declares its layout with MPPI_PARAM_LAYOUT
+   * (mppi_core.h) compiles only when the sizes are equal, each alignment is
+   * unspecified or a multiple of the declared one, and the schema is empty or
+   * equal to the declared string; otherwise initialize fails with
+   * MPPI_ERR_INVALID naming the field. */
+  uint64_t model_params_alignment;
+  uint64_t cost_params_alignment;
+  const char* schema_hash;
 } mppi_backend_plugin;
 
 /* Per-agent inputs of a batch (project extension; NULL = shared). */
@@ -157,10 +173,14 @@ int mppi_backend_batch_fetch(mppi_backend* b, float* states_out, float* controls
                              float* u_nominal_out, char* err, size_t err_len);
 
 /* ---- inspection (parity tests; no reference counterpart) ------------------ */
-/* Per-sample costs of the last pass for agents [a0, a0 + n): [n][K]. */
+/* Per-sample costs and weights are kept by single control steps
+ * (mppi_backend_dispatch_rollout) only: the closed loops do not write them
+ * (an unread store per sample and step), and after one these calls return
+ * MPPI_ERR_INVALID.
+ * Per-sample costs of the last control step for agents [a0, a0 + n): [n][K]. */
 int mppi_backend_last_costs(mppi_backend* b, uint32_t a0, uint32_t n, float* out, char* err,
                             size_t err_len);
-/* Normalised weights of the last pass for agents [a0, a0 + n): [n][K]. */
+/* Normalised weights of the last control step for agents [a0, a0 + n): [n][K]. */
 int mppi_backend_last_weights(mppi_backend* b, uint32_t a0, uint32_t n, float* out,
                               char* err, size_t err_len);
 /* Standard normals and shaped noise of samples [k0, k0 + count) of one agent
@@ -174,7 +194,8 @@ int mppi_backend_sample_noise(mppi_backend* b, uint64_t step_index, uint32_t age
  * the backend's stream. */
 int mppi_backend_time_passes(mppi_backend* b, uint32_t iters, float* rollout_ms,
                              float* combine_ms, char* err, size_t err_len);
-/* Launch geometry chosen for the prepared batch shape; kernels_per_step =
+/* Launch geometry chosen for the prepared batch shape (block = samples per
+ * rollout CTA); kernels_per_step =
  * kernel launches of one closed-loop control step (the rollout, which runs
  * the combine in each agent's last CTA for uniform batches, or rollout and
  * combine kernels; plus the network when a proposal is attached). */
@@ -185,6 +206,11 @@ int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
  * run, or pinned by MPPI_B200_FUSED_COMBINE / _SEPARATE_COMBINE / _WS):
  * bit 0 = combine run by each agent's last rollout CTA, bit 1 =
  * warp-specialised rollout; 0 = plain rollout and separate combine kernel.
+ * Bit 2 = cooperative rollout: the plugin splits its stage cost
+ * (MPPI_STAGE_COST_SPLIT) and the launch would have at most two plain CTAs
+ * per SM, so several lanes share each sample, one part of the cost each;
+ * chosen by that rule (MPPI_B200_COOP=0 / 1 pins it), not by timing, as its
+ * sums run in their own order.
  * No counterpart in the reference, whose step is a fixed sequence of
  * dispatches (src/metal_backend.mm:678-713). */
 int mppi_backend_step_form(mppi_backend* b, uint32_t* form);
@@ -223,11 +249,22 @@ int mppi_device_log(uint64_t n, const float* x, float* out, char* err, size_t er
  * u_out [horizon * control_dim] and diag3 [3] are DEVICE pointers the caller
  * owns, and the step's temporary data lives in one static device array of
  * MPPI_NOALLOC_SCRATCH_BYTES that every GPU loading this library keeps
- * until exit.  The call allocates nothing, blocks until the step is done,
- * and rejects problems whose scratch (about 4 * (sample_count + blocks *
- * (4 + horizon * control_dim)) bytes) exceeds the array.  The first call on
- * a device looks the array's device address up (make it before any stream
- * capture).  Calls share the array: calls that overlap on the GPU race. */
+ * until exit.  The call allocates nothing and rejects (MPPI_ERR_INVALID)
+ * problems whose scratch (about 4 * (24 + blocks * (8 + horizon *
+ * control_dim)) bytes, blocks = ceil(sample_count / 128)) exceeds the
+ * array, and backends with a learned proposal attached (this step is plain
+ * MPPI only).
+ * It computes the same bits as mppi_backend_dispatch_rollout for the same
+ * inputs, and keeps no per-sample costs (mppi_backend_last_costs does not
+ * see it).
+ * Streams: the step runs on the backend's own stream.  The inputs must be
+ * complete in device memory before the call (synchronise the stream that
+ * wrote them); the call blocks until the step is done, so the outputs are
+ * complete on return.  The caller's current device is restored.
+ * The first call on a device looks the array's device address up (make it
+ * before any stream capture); the address is kept for the process, so a
+ * cudaDeviceReset while the library is in use is not supported.  Calls
+ * share the array: calls that overlap on the GPU race. */
 #define MPPI_NOALLOC_SCRATCH_BYTES (2u << 20)
 int mppi_backend_dispatch_rollout_noalloc(mppi_backend* b, uint64_t step_index, const float* x0,
                                           const float* u_nominal, const void* model_params,
@@ -273,6 +310,15 @@ int mppi_backend_set_proposal(mppi_backend* b, struct mppi_proposal* proposal,
                               uint32_t proposal_samples, char* err, size_t err_len);
 int mppi_backend_set_record_ustar(mppi_backend* b, uint32_t enable, char* err, size_t err_len);
 int mppi_backend_batch_fetch_ustar(mppi_backend* b, float* ustar_out, char* err, size_t err_len);
+/* The proposal stage alone on the prepared batch's current states (no
+ * counterpart in the reference): features [num_agents][32] and network
+ * outputs [num_agents][network output stride] (either may be NULL), and
+ * whether the network ran per agent (1: on the CUDA cores, batches of at most
+ * 512 agents or MPPI_B200_NET_PER_AGENT=1) or as the tensor-core batch
+ * kernel (0).  In closed loops the per-agent form runs inside each agent's
+ * combine, for the next step's state. */
+int mppi_backend_proposal_stage(mppi_backend* b, float* features_out, float* outputs_out,
+                                uint32_t* per_agent, char* err, size_t err_len);
 /* Device time (CUDA events) of the proposal stage of one pass on the
  * prepared batch: the feature kernel and the network's forward pass. */
 int mppi_backend_time_proposal(mppi_backend* b, uint32_t iters, float* features_ms,

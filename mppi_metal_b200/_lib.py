@@ -46,6 +46,8 @@ class BackendPlugin(ctypes.Structure):
         ("source_path", c_char_p), ("dynamics", c_char_p), ("stage_cost", c_char_p),
         ("terminal_cost", c_char_p), ("model_params_size", c_u64),
         ("cost_params_size", c_u64), ("seed", c_u64),
+        ("model_params_alignment", c_u64), ("cost_params_alignment", c_u64),
+        ("schema_hash", c_char_p),
     ]
 
 
@@ -134,6 +136,7 @@ SIGNATURES = {
     "mppi_backend_set_proposal": (ctypes.c_int, [c_ptr, c_ptr, c_u32] + _ERR),
     "mppi_backend_set_record_ustar": (ctypes.c_int, [c_ptr, c_u32] + _ERR),
     "mppi_backend_batch_fetch_ustar": (ctypes.c_int, [c_ptr, c_ptr] + _ERR),
+    "mppi_backend_proposal_stage": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr] + _ERR),
     "mppi_backend_time_proposal": (ctypes.c_int, [c_ptr, c_u32, ctypes.POINTER(c_f32),
                                                   ctypes.POINTER(c_f32)] + _ERR),
     "mppi_compile_check": (ctypes.c_int, [ctypes.POINTER(BackendPlugin),

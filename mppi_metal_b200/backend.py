@@ -51,7 +51,9 @@ class Backend:
                  cov_full: bool = False, control_cost: bool = False,
                  stage_cost: str = "mppi_stage_cost", terminal_cost: str = "mppi_terminal_cost",
                  dynamics: str = "mppi_dynamics", model_params_size: int = 0,
-                 cost_params_size: int = 0, seed: int = 0, numeric_mode: int = 0):
+                 cost_params_size: int = 0, seed: int = 0, numeric_mode: int = 0,
+                 model_params_alignment: int = 1, cost_params_alignment: int = 1,
+                 schema_hash: str = ""):
         self.lib = _lib.load()
         h = ctypes.c_void_p()
         if self.lib.mppi_backend_create(ctypes.byref(h)) != _lib.MPPI_OK:
@@ -69,7 +71,8 @@ class Backend:
         path = plugin if plugin.endswith(".cu") or "/" in plugin else _lib.plugin_path(plugin)
         plug = _lib.BackendPlugin(path.encode(), dynamics.encode(), stage_cost.encode(),
                                   terminal_cost.encode(), model_params_size, cost_params_size,
-                                  seed & 0xFFFFFFFFFFFFFFFF)
+                                  seed & 0xFFFFFFFFFFFFFFFF, model_params_alignment,
+                                  cost_params_alignment, schema_hash.encode())
         eb = _lib.err_buf()
         _check(self.lib.mppi_backend_initialize(self.h, ctypes.byref(plug), ctypes.byref(cfg),
                                                 eb, len(eb)), eb)
@@ -233,6 +236,18 @@ class Backend:
         _check(self.lib.mppi_backend_batch_fetch_ustar(self.h, _p(out), eb, len(eb)), eb)
         return out
 
+    def proposal_stage(self):
+        """Runs the proposal stage on the prepared batch's current states:
+        (features [N][32], network outputs [N][stride], per_agent flag)."""
+        feat = np.zeros((self.N, 32), np.float32)
+        stride = self._proposal.out_stride
+        out = np.zeros((self.N, stride), np.float32)
+        flag = ctypes.c_uint32()
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_proposal_stage(self.h, _p(feat), _p(out), ctypes.byref(flag),
+                                                    eb, len(eb)), eb)
+        return feat, out, bool(flag.value)
+
     # -- inspection ------------------------------------------------------------
     def last_costs(self, a0: int = 0, n: Optional[int] = None) -> np.ndarray:
         n = self.N - a0 if n is None else n
@@ -291,7 +306,8 @@ class Backend:
         info = {k: v.value for k, v in zip(keys, vals)}
         f = ctypes.c_uint32()
         self.lib.mppi_backend_step_form(self.h, ctypes.byref(f))
-        info["form"] = {"fused_combine": bool(f.value & 1), "warp_specialised": bool(f.value & 2)}
+        info["form"] = {"fused_combine": bool(f.value & 1), "warp_specialised": bool(f.value & 2),
+                        "cooperative": bool(f.value & 4)}
         return info
 
 
@@ -335,13 +351,16 @@ def compile_check(plugin: str, state_dim: int, control_dim: int, cov_full: bool 
                   terminal_cost: str = "mppi_terminal_cost", dynamics: str = "mppi_dynamics",
                   model_params_size: int = 0, cost_params_size: int = 0,
                   proposal: bool = False, features: Optional[str] = None,
-                  numeric_mode: int = 0):
+                  numeric_mode: int = 0, model_params_alignment: int = 1,
+                  cost_params_alignment: int = 1, schema_hash: str = ""):
     """NVRTC-compile a plugin with the library kernels for sm_100a (no GPU).
     Returns (status, error, log)."""
     lib = _lib.load()
     path = plugin if plugin.endswith(".cu") or "/" in plugin else _lib.plugin_path(plugin)
     plug = _lib.BackendPlugin(path.encode(), dynamics.encode(), stage_cost.encode(),
-                              terminal_cost.encode(), model_params_size, cost_params_size, 0)
+                              terminal_cost.encode(), model_params_size, cost_params_size, 0,
+                              model_params_alignment, cost_params_alignment,
+                              schema_hash.encode())
     cfg = _lib.BackendConfig(state_dim, control_dim, 8, 64, 1.0, 1 if cov_full else 0, None, None,
                              None, None, numeric_mode, 1 if control_cost else 0)
     log = ctypes.create_string_buffer(1 << 18)

@@ -32,7 +32,7 @@ CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-EMBED = ["mppi_prelude.cuh", "mppi_launch.h", "mppi_kernels.cuh"]
+EMBED = ["mppi_prelude.cuh", "mppi_launch.h", "mppi_gelu.cuh", "mppi_kernels.cuh"]
 HOST_SOURCES = ["backend.cpp", "nvrtc_module.cpp", "driver.cpp", "driver_c.cpp"]
 CUDA_SOURCES = ["static_kernels.cu", "noalloc.cu", "proposal_mlp.cu"]
 DELIM = "mppi_b200_src"

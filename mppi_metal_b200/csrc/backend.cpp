@@ -13,9 +13,12 @@
 //   done      [N] u32          finished rollout CTAs per agent (fused combine)
 //
 // Device data layout for a batch of N agents (all FP32, agent-major):
-//   io:       [step_base u32 x4][x N*n][u_nom N*H*m][u_out N*H*m][diag N*3][stats N*4]
+//   io:       [step_base u32 x4][x N*n][u_nom N*H*m][u_out N*H*m][diag N*3]
+//             [stats N*MPPI_STATS_STRIDE]
 //             (step_base..u_nom is one upload, u_out..diag one download)
-//   costs     [N][K]            per-sample costs of the last pass
+//   costs     [N][K] hi, [N][K] lo  per-sample cost pairs of the last single
+//                               control step (dispatch_rollout); the closed
+//                               loops do not write them
 //   partials  [N][nblk][ps]     per-CTA softmax / weighted-noise partials
 //   history   [T][N][n], [T][N][m], [T][N]; terminal [N][n]
 //   per-agent blobs [N][pad16(size)], per-agent sigma [N][m or m*m]
@@ -52,6 +55,11 @@ size_t pad4(size_t n) { return (n + 3) & ~size_t(3); }
 size_t pad16(size_t n) { return (n + 15) & ~size_t(15); }
 
 constexpr uint32_t kFeatureStride = 32;  // floats per feature row (network input)
+// Batches of at most this many agents evaluate the proposal network per agent
+// inside their combines (CUDA cores, weights streamed from L2); larger ones
+// run the tensor-core batch kernel, which reads the weights once per 128
+// agents (MPPI_B200_NET_PER_AGENT=0 / 1 pins the choice).
+constexpr uint32_t kNetPerAgentMax = 512;
 
 struct DevBuf {
   void* p = nullptr;
@@ -127,11 +135,14 @@ bool cholesky(uint32_t m, const float* a, std::vector<float>* l) {
 
 struct LaunchGeom {
   int variant = 1;  // index into kRolloutBlocks
-  uint32_t block = 128;
+  uint32_t block = 128;  // samples per CTA
   uint32_t nblk = 0;
   uint32_t stage_rows = 0;
   uint32_t pstride = 0;
   size_t smem = 0;
+  // cooperative form: lanes per sample (0: one thread per sample); its CTAs
+  // have 128 threads, block = 128 / coop samples
+  uint32_t coop = 0;
 };
 
 }  // namespace
@@ -176,6 +187,12 @@ struct mppi_backend {
   // MPPI_B200_FUSED_COMBINE=1 / MPPI_B200_WS=1 or 0 pin the step form's
   // combine and warp-specialisation choices (0 = timed)
   int combine_pin = 0, ws_pin = 0;
+  // MPPI_B200_COOP=1 / 0 pins the cooperative form on / off (0 = the shape
+  // rule of choose_geometry)
+  int coop_pin = 0;
+  // MPPI_B200_NET_PER_AGENT=1 / 0 pins the proposal network's form (0 = by
+  // the batch size, kNetPerAgentMax)
+  int net_pin = 0;
   uint32_t form = 0;          // for form_key's launch shape: kFormFused | kFormWs
   std::string form_key;
   // Uniform rollout launches (and the proposal network's) use programmatic
@@ -243,7 +260,7 @@ struct mppi_backend {
   size_t off_uout() const { return off_unom() + pad4((size_t)N * HM()); }
   size_t off_diag() const { return off_uout() + pad4((size_t)N * HM()); }
   size_t off_stats() const { return off_diag() + pad4((size_t)N * 3); }
-  size_t io_floats() const { return off_stats() + pad4((size_t)N * 4); }
+  size_t io_floats() const { return off_stats() + (size_t)N * MPPI_STATS_STRIDE; }
 
   float* io() const { return d_io.as<float>(); }
   const float* c_sigma() const { return d_consts.as<float>(); }
@@ -296,10 +313,48 @@ bool valid_identifier(const char* s) {
 // is used while that keeps four CTAs per SM, or when every CTA of the launch
 // is resident at once with it; otherwise the noise is regenerated in chunks
 // after the costs are known.
-LaunchGeom choose_geometry(const mppi_backend* b) {
+// The cooperative form (the plugin's stage cost split over lanes, module
+// coop_lanes > 0) serves launches whose plain form would have at most two
+// CTAs per SM: there each sample's serial chain sets the time, and splitting
+// its cost terms over lanes shortens it; with more CTAs the SMs' issue slots
+// are full and the lanes' repeated dynamics would only add work.  A fixed
+// rule of the launch shape, never a timing, so one problem always runs the
+// same arithmetic (the cooperative form sums a sample's cost terms in its
+// own order).
+bool use_coop(const mppi_backend* b, uint32_t N) {
+  if (b->ragged || !b->mod || b->mod->coop_lanes == 0 || b->coop_pin < 0) return false;
+  if (b->coop_pin > 0) return true;
+  const size_t plain_ctas = (size_t)N * ((b->K + 127) / 128);
+  return N > 0 && plain_ctas <= 2 * (size_t)b->num_sms;
+}
+
+LaunchGeom choose_geometry(const mppi_backend* b, uint32_t N) {
   LaunchGeom g;
   const size_t HM = b->HM();
   const size_t budget = std::min<size_t>(b->max_smem_optin ? b->max_smem_optin : 232448, 232448);
+  if (use_coop(b, N)) {
+    // 128 threads, 128 / lanes samples per CTA; the whole horizon staged when
+    // it fits the per-CTA share of four CTAs per SM, else in chunks
+    g.coop = b->mod->coop_lanes;
+    g.block = 128 / g.coop;
+    g.variant = 1;
+    const size_t el = b->stage_elem;
+    const size_t per_cta = rollout_dynamic_share(b, b->mod->coop_static_smem, budget);
+    const size_t fixed = nominal_bytes(b) + (size_t)g.block * 4;
+    const size_t full = fixed + HM * g.block * el;
+    if (full <= per_cta) {
+      g.stage_rows = (uint32_t)HM;
+      g.smem = full;
+    } else {
+      uint32_t rows = (uint32_t)((per_cta > fixed ? per_cta - fixed : 0) / ((size_t)g.block * el));
+      rows = std::min<uint32_t>(std::max<uint32_t>(b->m, rows / b->m * b->m), (uint32_t)HM);
+      g.stage_rows = rows;
+      g.smem = fixed + (size_t)rows * g.block * el;
+    }
+    g.nblk = (b->K + g.block - 1) / g.block;
+    g.pstride = (uint32_t)pad4(MPPI_PARTIAL_HEAD + HM);
+    return g;
+  }
   // Prefer 128 threads; fall back to 64 for very long horizons.
   const int order[2] = {1, 0};
   const size_t el = b->stage_elem;
@@ -324,10 +379,10 @@ LaunchGeom choose_geometry(const mppi_backend* b) {
     // staged (few agents x few samples: one partial wave) gains nothing from
     // the fourth CTA per SM, and chunked staging would regenerate every
     // noise value after the costs are known: stage the whole horizon.
-    if (full <= budget && b->N > 0) {
+    if (full <= budget && N > 0) {
       const size_t per_sm = b->smem_reserved + b->mod->rollout_static_smem[vi] + full;
       const size_t fit = std::min<size_t>(512 / block, b->smem_per_sm / per_sm);
-      const size_t ctas = (size_t)b->N * ((b->K + block - 1) / block);
+      const size_t ctas = (size_t)N * ((b->K + block - 1) / block);
       if (fit >= 1 && ctas <= fit * (size_t)b->num_sms) {
         g.stage_rows = (uint32_t)HM;
         g.smem = full;
@@ -348,6 +403,9 @@ LaunchGeom choose_geometry(const mppi_backend* b) {
   return g;
 }
 
+// The geometry of the prepared batch (b->N agents).
+LaunchGeom choose_geometry(const mppi_backend* b) { return choose_geometry(b, b->N); }
+
 size_t combine_smem(const mppi_backend* b);
 
 // Dynamic shared memory limit of the current rollout kernels (plain and
@@ -362,6 +420,14 @@ cudaError_t set_rollout_smem(const mppi_backend* b) {
     cudaError_t e =
         cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem);
     if (e != cudaSuccess) return e;
+  }
+  if (b->geom.coop) {
+    for (const void* f :
+         {(const void*)b->mod->rollout_coop, (const void*)b->mod->rollout_coop_fused}) {
+      cudaError_t e =
+          cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem);
+      if (e != cudaSuccess) return e;
+    }
   }
   if (!b->ragged) {
     for (const void* f : {(const void*)b->mod->rollout_ws, (const void*)b->mod->rollout_ws_fused}) {
@@ -415,7 +481,8 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
       CK(cudaMemsetAsync(b->d_io.p, 0, b->d_io.bytes, b->stream));
     }
   }
-  CK(b->d_costs.ensure((size_t)N * b->K * 4, &grew));
+  // per-sample cost pairs, kept by single control steps for inspection
+  if (T == 0) CK(b->d_costs.ensure((size_t)2 * N * b->K * 4, &grew));
   const size_t records = b->ragged ? b->total_records : (size_t)N * b->geom.nblk;
   CK(b->d_partials.ensure(records * b->geom.pstride * 4, &grew));
   {
@@ -450,6 +517,30 @@ int ensure_shape(mppi_backend* b, uint32_t N, uint32_t T, bool ws, bool wc, bool
   return MPPI_OK;
 }
 
+// Whether the attached proposal network runs per agent (inside the combines,
+// and for a loop's first step in the rows kernel) rather than as the
+// tensor-core batch kernel.  A rule of the batch size, not a timing.
+bool net_per_agent(const mppi_backend* b) {
+  if (!b->proposal || !b->spec.proposal || b->net_pin < 0 || !b->mod->proposal_rows)
+    return false;
+  return b->net_pin > 0 || b->N <= kNetPerAgentMax;
+}
+
+MppiNetRows net_rows(const mppi_backend* b) {
+  MppiNetRows r{};
+  const mppi_b200::ProposalWeights w = mppi_b200::proposal_weights(b->proposal);
+  for (int l = 0; l < 4; ++l) {
+    r.w[l] = w.w[l];
+    r.b[l] = w.b[l];
+  }
+  r.in = w.in;
+  r.hidden = w.hidden;
+  r.out = w.out;
+  r.out_stride = mppi_b200::proposal_shape(b->proposal).out_stride;
+  r.out_buf = b->d_prop.as<float>();
+  return r;
+}
+
 MppiRolloutArgs rollout_args(const mppi_backend* b, uint32_t step_local) {
   MppiRolloutArgs a{};
   a.num_agents = b->N;
@@ -474,7 +565,10 @@ MppiRolloutArgs rollout_args(const mppi_backend* b, uint32_t step_local) {
   a.cost_params = b->run_cp;
   a.model_stride = b->run_mp_stride;
   a.cost_stride = b->run_cp_stride;
-  a.costs = b->d_costs.as<float>();
+  if (b->T == 0) {  // a single control step: keep its costs for inspection
+    a.costs = b->d_costs.as<float>();
+    a.costs_lo = a.costs + (size_t)b->N * b->K;
+  }
   a.partials = b->d_partials.as<float>();
   if (b->ragged) {
     const uint32_t* info = b->d_agent_info.as<uint32_t>();
@@ -529,6 +623,8 @@ MppiCombineArgs combine_args(const mppi_backend* b, uint32_t step_local, bool pr
     c.cost_stride = b->run_cp_stride;
     c.features = b->d_feat.as<float>();
     c.feature_stride = kFeatureStride;
+    // the next step's network output by the combine's threads
+    if (net_per_agent(b)) c.net = net_rows(b);
   }
   if (b->ragged) {
     const uint32_t* info = b->d_agent_info.as<uint32_t>();
@@ -570,8 +666,29 @@ cudaError_t launch_network(mppi_backend* b) {
                                              b->pdl);
 }
 
-// Features, then the network (both on the backend stream).
+// Features and the network per agent, one CTA per agent (the rows kernel).
+cudaError_t launch_proposal_rows(mppi_backend* b) {
+  MppiProposalRowsArgs a{};
+  a.f.rows = b->N;
+  a.f.agents_mod = b->N;
+  a.f.x_stride = b->n;
+  a.f.out_stride = kFeatureStride;
+  a.f.x = b->io() + b->off_x();
+  a.f.model_params = b->run_mp;
+  a.f.cost_params = b->run_cp;
+  a.f.model_stride = b->run_mp_stride;
+  a.f.cost_stride = b->run_cp_stride;
+  a.f.out = b->d_feat.as<float>();
+  a.net = net_rows(b);
+  void* args[] = {&a};
+  return cudaLaunchKernel((const void*)b->mod->proposal_rows, dim3(b->N), dim3(128), args, 0,
+                          b->stream);
+}
+
+// Features, then the network (both on the backend stream): per agent in one
+// kernel, or the features kernel and the tensor-core batch kernel.
 cudaError_t launch_proposal(mppi_backend* b) {
+  if (net_per_agent(b)) return launch_proposal_rows(b);
   cudaError_t e = launch_features(b);
   return e == cudaSuccess ? launch_network(b) : e;
 }
@@ -616,6 +733,10 @@ cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a, bool ws = f
     if (e != cudaSuccess) return e;
     return cudaLaunchKernel(f, dim3(b->grid), dim3(128), args, b->geom.smem, b->stream);
   }
+  if (b->geom.coop)
+    return launch_dependent(b, fused ? (const void*)b->mod->rollout_coop_fused
+                                     : (const void*)b->mod->rollout_coop,
+                            dim3(b->geom.nblk, b->N), dim3(128), b->geom.smem, args);
   return launch_dependent(b, fused ? (const void*)b->mod->rollout_fused[b->geom.variant]
                                    : (const void*)b->mod->rollout[b->geom.variant],
                           dim3(b->geom.nblk, b->N), dim3(b->geom.block), b->geom.smem, args);
@@ -724,7 +845,7 @@ bool fused_combine(const mppi_backend* b) { return (b->form & kFormFused) != 0; 
 // The warp-specialised rollout needs 128-sample CTAs with the whole horizon
 // staged, in a uniform batch.
 bool ws_possible(const mppi_backend* b) {
-  return !b->ragged && b->geom.block == 128 && b->geom.stage_rows >= b->HM();
+  return !b->ragged && !b->geom.coop && b->geom.block == 128 && b->geom.stage_rows >= b->HM();
 }
 
 // One step's kernels after the proposal stage in the given form: the rollout
@@ -942,10 +1063,13 @@ int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
     cudaError_t le = cudaSuccess;
     const bool prop = b->proposal && b->spec.proposal;
     // with a proposal: features of x0 once, then per step network -> rollout
-    // -> combine (which leaves the next step's features behind)
-    if (prop) le = launch_features(b);
+    // -> combine (which leaves the next step's features behind); with the
+    // per-agent network the first step's kernel evaluates it for x0 and each
+    // combine evaluates it for the next step
+    const bool per_agent = prop && net_per_agent(b);
+    if (prop) le = per_agent ? launch_proposal_rows(b) : launch_features(b);
     for (uint32_t s = 0; s < b->T && le == cudaSuccess; ++s) {
-      if (prop) le = launch_network(b);
+      if (prop && !per_agent) le = launch_network(b);
       if (le == cudaSuccess) le = launch_rollout_combine(b, s, true);
     }
     cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
@@ -962,6 +1086,23 @@ int enqueue_closed_loop(mppi_backend* b, char* err, size_t err_len) {
     b->graph_key = key;
   }
   CK(cudaGraphLaunch(b->graph, b->stream));
+  return MPPI_OK;
+}
+
+// Per-sample costs and weights exist for the last single control step only
+// (dispatch_rollout): the closed loops do not write them.
+int check_step_costs(mppi_backend* b, uint32_t a0, uint32_t n, const float* out, char* err,
+                     size_t err_len) {
+  if (b->T != 0 || b->d_costs.p == nullptr) {
+    set_err(err, err_len,
+            "per-sample costs are kept by dispatch_rollout only (closed loops do not write "
+            "them); run a single control step first.");
+    return MPPI_ERR_INVALID;
+  }
+  if (!out || a0 + n > b->N) {
+    set_err(err, err_len, "agent range out of bounds.");
+    return MPPI_ERR_INVALID;
+  }
   return MPPI_OK;
 }
 
@@ -983,6 +1124,10 @@ int mppi_backend_create(mppi_backend** out) {
     if (fc && *fc && *fc != '0') (*out)->combine_pin = 1;
     if (!(*out)->fuse_combine) (*out)->combine_pin = -1;
     if (const char* ws = getenv("MPPI_B200_WS"); ws && *ws) (*out)->ws_pin = *ws == '0' ? -1 : 1;
+    if (const char* co = getenv("MPPI_B200_COOP"); co && *co)
+      (*out)->coop_pin = *co == '0' ? -1 : 1;
+    if (const char* np = getenv("MPPI_B200_NET_PER_AGENT"); np && *np)
+      (*out)->net_pin = *np == '0' ? -1 : 1;
   }
   return *out ? MPPI_OK : MPPI_ERR_INVALID;
 }
@@ -1005,9 +1150,10 @@ int mppi_backend_initialize(mppi_backend* b, const mppi_backend_plugin* plugin,
     set_err(err, err_len, "state_dim, control_dim, horizon and sample_count must be > 0.");
     return MPPI_ERR_INVALID;
   }
-  if (cfg->state_dim * 4 > 128) {
+  if (cfg->state_dim > MPPI_MAX_STATE_DIM) {
     set_err(err, err_len, "DriverConfig::state_dim (" + std::to_string(cfg->state_dim) +
-                              ") exceeds MPPI_MAX_STATE_BYTES / 4 = 32.");
+                              ") exceeds the state limit of " +
+                              std::to_string(MPPI_MAX_STATE_DIM) + " floats.");
     return MPPI_ERR_INVALID;
   }
   if (cfg->control_dim > 16) {
@@ -1100,6 +1246,9 @@ int mppi_backend_initialize(mppi_backend* b, const mppi_backend_plugin* plugin,
   spec.noise_half = b->noise_half;
   spec.model_params_bytes = b->mp_size;
   spec.cost_params_bytes = b->cp_size;
+  spec.model_params_alignment = plugin->model_params_alignment ? plugin->model_params_alignment : 1;
+  spec.cost_params_alignment = plugin->cost_params_alignment ? plugin->cost_params_alignment : 1;
+  spec.schema_hash = plugin->schema_hash ? plugin->schema_hash : "";
   std::string merr;
   const int rc = mppi_b200::load_module(spec, &b->mod, &merr);
   if (rc != MPPI_OK) {
@@ -1473,10 +1622,7 @@ int mppi_backend_reset(mppi_backend* b, char* err, size_t err_len) {
 int mppi_backend_last_costs(mppi_backend* b, uint32_t a0, uint32_t n, float* out, char* err,
                             size_t err_len) {
   if (int rc = check_init(b, err, err_len)) return rc;
-  if (!out || a0 + n > b->N) {
-    set_err(err, err_len, "agent range out of bounds.");
-    return MPPI_ERR_INVALID;
-  }
+  if (int rc = check_step_costs(b, a0, n, out, err, err_len)) return rc;
   CK(cudaMemcpyAsync(out, b->d_costs.as<float>() + (size_t)a0 * b->K, (size_t)n * b->K * 4,
                      cudaMemcpyDeviceToHost, b->stream));
   CK(cudaStreamSynchronize(b->stream));
@@ -1486,10 +1632,7 @@ int mppi_backend_last_costs(mppi_backend* b, uint32_t a0, uint32_t n, float* out
 int mppi_backend_last_weights(mppi_backend* b, uint32_t a0, uint32_t n, float* out, char* err,
                               size_t err_len) {
   if (int rc = check_init(b, err, err_len)) return rc;
-  if (!out || a0 + n > b->N) {
-    set_err(err, err_len, "agent range out of bounds.");
-    return MPPI_ERR_INVALID;
-  }
+  if (int rc = check_step_costs(b, a0, n, out, err, err_len)) return rc;
   DevBuf w;
   CK(w.ensure((size_t)b->N * b->K * 4));
   MppiWeightsArgs a{};
@@ -1497,6 +1640,7 @@ int mppi_backend_last_weights(mppi_backend* b, uint32_t a0, uint32_t n, float* o
   a.K = b->K;
   a.lambda = b->lambda;
   a.costs = b->d_costs.as<float>();
+  a.costs_lo = a.costs + (size_t)b->N * b->K;
   a.stats = b->io() + b->off_stats();
   a.weights = w.as<float>();
   void* args[] = {&a};
@@ -1581,6 +1725,22 @@ int mppi_backend_time_proposal(mppi_backend* b, uint32_t iters, float* features_
     return MPPI_ERR_INVALID;
   }
   float ms = 0.0f;
+  if (net_per_agent(b)) {
+    // features kernel alone, then the rows kernel (features and network)
+    CK(cudaEventRecord(b->ev0, b->stream));
+    for (uint32_t i = 0; i < iters; ++i) CK(launch_features(b));
+    CK(cudaEventRecord(b->ev1, b->stream));
+    CK(cudaEventSynchronize(b->ev1));
+    CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    if (features_ms) *features_ms = ms / iters;
+    CK(cudaEventRecord(b->ev0, b->stream));
+    for (uint32_t i = 0; i < iters; ++i) CK(launch_proposal_rows(b));
+    CK(cudaEventRecord(b->ev1, b->stream));
+    CK(cudaEventSynchronize(b->ev1));
+    CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+    if (network_ms) *network_ms = ms / iters;
+    return MPPI_OK;
+  }
   CK(cudaEventRecord(b->ev0, b->stream));
   for (uint32_t i = 0; i < iters; ++i) CK(launch_proposal(b));
   CK(cudaEventRecord(b->ev1, b->stream));
@@ -1623,6 +1783,9 @@ int mppi_compile_check_proposal(const mppi_backend_plugin* plugin, const mppi_ba
   spec.noise_half = cfg->numeric_mode != 0;
   spec.model_params_bytes = plugin->model_params_size;
   spec.cost_params_bytes = plugin->cost_params_size;
+  spec.model_params_alignment = plugin->model_params_alignment ? plugin->model_params_alignment : 1;
+  spec.cost_params_alignment = plugin->cost_params_alignment ? plugin->cost_params_alignment : 1;
+  spec.schema_hash = plugin->schema_hash ? plugin->schema_hash : "";
   spec.proposal = proposal != 0;
   spec.features = features ? features : "";
   if (!spec.features.empty() && !valid_identifier(features)) {
@@ -1660,13 +1823,14 @@ int mppi_backend_launch_info(mppi_backend* b, uint32_t* block, uint32_t* nblk,
   if (stage_rows) *stage_rows = b->geom.stage_rows;
   if (smem_bytes) *smem_bytes = (uint32_t)b->geom.smem;
   if (kernels_per_step)
-    *kernels_per_step = (fused_combine(b) ? 1u : 2u) + (b->proposal && b->spec.proposal ? 1u : 0u);
+    *kernels_per_step = (fused_combine(b) ? 1u : 2u) +
+                        (b->proposal && b->spec.proposal && !net_per_agent(b) ? 1u : 0u);
   return MPPI_OK;
 }
 
 int mppi_backend_step_form(mppi_backend* b, uint32_t* form) {
   if (!b || !b->initialized) return MPPI_ERR_NOT_INIT;
-  if (form) *form = b->form;
+  if (form) *form = b->form | (b->geom.coop ? 4u : 0u);
   return MPPI_OK;
 }
 
@@ -1839,6 +2003,26 @@ int mppi_backend_batch_fetch_ustar(mppi_backend* b, float* out, char* err, size_
   return MPPI_OK;
 }
 
+int mppi_backend_proposal_stage(mppi_backend* b, float* features_out, float* outputs_out,
+                                uint32_t* per_agent, char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (b->N == 0 || !b->proposal || !b->spec.proposal) {
+    set_err(err, err_len, "no proposal attached / no batch prepared.");
+    return MPPI_ERR_INVALID;
+  }
+  CK(launch_proposal(b));
+  if (features_out)
+    CK(cudaMemcpyAsync(features_out, b->d_feat.p, (size_t)b->N * kFeatureStride * 4,
+                       cudaMemcpyDeviceToHost, b->stream));
+  if (outputs_out)
+    CK(cudaMemcpyAsync(outputs_out, b->d_prop.p,
+                       (size_t)b->N * mppi_b200::proposal_shape(b->proposal).out_stride * 4,
+                       cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  if (per_agent) *per_agent = net_per_agent(b) ? 1u : 0u;
+  return MPPI_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -1848,22 +2032,25 @@ int mppi_backend_batch_fetch_ustar(mppi_backend* b, float* out, char* err, size_
 // allocation-free entry point in csrc/noalloc.cu).  Scratch layout (floats):
 //   [0, 16)              zero block: the step_base word reads 0, the step index
 //                        travels in step_local
-//   [16, 16 + K)         per-sample costs
-//   [.., + nblk * ps)    per-CTA partial records
-//   [.., + 4)            combine statistics
+//   [16, .. + nblk * ps) per-CTA partial records
+//   [.., + 8)            combine statistics
+// The geometry is the one a single-agent dispatch_rollout uses (one agent,
+// whatever batch the backend prepared last), so both calls compute the same
+// bits.  Per-sample costs are not kept (no inspection on this path).
 // ---------------------------------------------------------------------------
 #include "step_scratch.hpp"
 
 namespace mppi_b200 {
 
 size_t step_scratch_floats(const mppi_backend* b) {
-  const LaunchGeom g = choose_geometry(b);
-  return 16 + pad4(b->K) + (size_t)g.nblk * g.pstride + 4;
+  const LaunchGeom g = choose_geometry(b, 1);
+  return 16 + (size_t)g.nblk * g.pstride + MPPI_STATS_STRIDE;
 }
 
 int backend_device(const mppi_backend* b) { return b->device; }
 cudaStream_t backend_stream(const mppi_backend* b) { return b->stream; }
 bool backend_initialized(const mppi_backend* b) { return b != nullptr && b->initialized; }
+bool backend_has_proposal(const mppi_backend* b) { return b->proposal != nullptr; }
 
 int launch_step_with_scratch(mppi_backend* b, uint64_t step_index, const float* x0,
                              const float* u_nominal, const void* model_params,
@@ -1877,22 +2064,27 @@ int launch_step_with_scratch(mppi_backend* b, uint64_t step_index, const float* 
     *error = ebuf;
     return rc;
   };
-  const LaunchGeom g = choose_geometry(b);
+  const LaunchGeom g = choose_geometry(b, 1);
   const size_t need = step_scratch_floats(b);
   if (scratch_floats < need) {
     *error = "scratch too small";
     return MPPI_ERR_INVALID;
   }
   float* zero = scratch;
-  float* costs = scratch + 16;
-  float* partials = costs + pad4(b->K);
+  float* partials = scratch + 16;
   float* stats = partials + (size_t)g.nblk * g.pstride;
-  const void* rk = (const void*)b->mod->rollout[g.variant];
+  const void* rk = g.coop ? (const void*)b->mod->rollout_coop
+                          : (const void*)b->mod->rollout[g.variant];
+  const uint32_t threads = g.coop ? 128u : g.block;
   if (g.smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(rk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)g.smem);
+    // raise the kernel's dynamic shared memory limit if it is below this
+    // launch's need; never lower it (a prepared batch may need more)
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, rk);
+    if (e == cudaSuccess && (size_t)fa.maxDynamicSharedSizeBytes < g.smem)
+      e = cudaFuncSetAttribute(rk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g.smem);
     if (e != cudaSuccess) {
-      set_err(err, err_len, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+      set_err(err, err_len, std::string("rollout shared memory limit: ") + cudaGetErrorString(e));
       return fail(MPPI_ERR_CUDA);
     }
   }
@@ -1922,10 +2114,9 @@ int launch_step_with_scratch(mppi_backend* b, uint64_t step_index, const float* 
                                 : b->d_zero.as<uint8_t>();
   a.cost_params = cost_params ? static_cast<const uint8_t*>(cost_params)
                               : b->d_zero.as<uint8_t>();
-  a.costs = costs;
   a.partials = partials;
   void* ra[] = {&a};
-  e = cudaLaunchKernel(rk, dim3(g.nblk, 1), dim3(g.block), ra, g.smem, stream);
+  e = cudaLaunchKernel(rk, dim3(g.nblk, 1), dim3(threads), ra, g.smem, stream);
   if (e != cudaSuccess) {
     set_err(err, err_len, std::string("rollout launch: ") + cudaGetErrorString(e));
     return fail(MPPI_ERR_CUDA);

@@ -48,6 +48,7 @@
 #pragma once
 
 #include "mppi_launch.h"
+#include "mppi_gelu.cuh"
 
 #ifndef MPPI_STATE_DIM
 #error "MPPI_STATE_DIM must be defined"
@@ -75,6 +76,17 @@
 #ifndef MPPI_CP_BYTES
 #define MPPI_CP_BYTES 0
 #endif
+// ParamLayout alignments and schema_hash (checked against a plugin's
+// MPPI_PARAM_LAYOUT declaration)
+#ifndef MPPI_MP_ALIGN
+#define MPPI_MP_ALIGN 1
+#endif
+#ifndef MPPI_CP_ALIGN
+#define MPPI_CP_ALIGN 1
+#endif
+#ifndef MPPI_SCHEMA_HASH
+#define MPPI_SCHEMA_HASH ""
+#endif
 #ifndef MPPI_STAGE_COST_FN
 #define MPPI_STAGE_COST_FN mppi_default_stage_cost
 #endif
@@ -99,6 +111,35 @@ constexpr unsigned kFull = 0xffffffffu;
 
 static_assert(kN >= 1 && kN * 4 <= MPPI_MAX_STATE_BYTES, "state_dim out of range");
 static_assert(kM >= 1 && kM <= MPPI_MAX_CONTROL_DIM, "control_dim out of range");
+
+// ---- ParamLayout against the plugin's declared layout (MPPI_PARAM_LAYOUT) ----
+// The messages carry a marker the host looks for in the compile log.
+__host__ __device__ constexpr bool str_eq(const char* a, const char* b) {
+  while (*a != '\0' && *a == *b) {
+    ++a;
+    ++b;
+  }
+  return *a == *b;
+}
+typedef mppi_declared_param_layout<0> DeclaredLayout;
+static_assert(!DeclaredLayout::declared || DeclaredLayout::model_size == MPPI_MP_BYTES,
+              "MPPI_PARAM_LAYOUT_MISMATCH: ParamLayout::model_params_size differs from the "
+              "model parameter size the plugin declares");
+static_assert(!DeclaredLayout::declared || DeclaredLayout::cost_size == MPPI_CP_BYTES,
+              "MPPI_PARAM_LAYOUT_MISMATCH: ParamLayout::cost_params_size differs from the "
+              "cost parameter size the plugin declares");
+static_assert(!DeclaredLayout::declared || MPPI_MP_ALIGN == 1 ||
+                  MPPI_MP_ALIGN % DeclaredLayout::model_align == 0,
+              "MPPI_PARAM_LAYOUT_MISMATCH: ParamLayout::model_params_alignment is not a multiple "
+              "of the model parameter alignment the plugin declares");
+static_assert(!DeclaredLayout::declared || MPPI_CP_ALIGN == 1 ||
+                  MPPI_CP_ALIGN % DeclaredLayout::cost_align == 0,
+              "MPPI_PARAM_LAYOUT_MISMATCH: ParamLayout::cost_params_alignment is not a multiple "
+              "of the cost parameter alignment the plugin declares");
+static_assert(!DeclaredLayout::declared || str_eq(MPPI_SCHEMA_HASH, "") ||
+                  str_eq(MPPI_SCHEMA_HASH, DeclaredLayout::schema),
+              "MPPI_PARAM_LAYOUT_MISMATCH: ParamLayout::schema_hash differs from the schema "
+              "the plugin declares");
 
 typedef typename mppi_first_arg<decltype(&MPPI_DYNAMICS_FN)>::type DynStateT;
 typedef typename mppi_first_arg<decltype(&MPPI_STAGE_COST_FN)>::type StageStateT;
@@ -140,17 +181,46 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
+__device__ __forceinline__ double warp_min_d(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(kFull, v, o));
+  return v;
+}
+
+// Sample costs are accumulated as an unevaluated pair hi + lo of floats:
+// Knuth's TwoSum gives the exact rounding error of every addition to hi,
+// and lo collects those errors.  With lambda = 1 and costs of order 1e3-1e4
+// the softmax turns the plain float sum's rounding (an ulp of the running
+// total per step, about 5e-4 at 8e3) into weight errors of the same size;
+// the pair keeps the accumulated total to the rounding of the cost terms
+// themselves.  Additions only (no multiply to contract into an FMA).
+__device__ __forceinline__ void acc_cost(float& hi, float& lo, float x) {
+  const float s = hi + x;
+  const float bp = s - hi;
+  const float err = (hi - (s - bp)) + (x - bp);
+  hi = s;
+  lo += err;
+}
+
+// The pair as one double (exact: |lo| is far below hi's last bit times 2^29).
+__device__ __forceinline__ double cost_pair(float hi, float lo) {
+  return (double)hi + (double)lo;
+}
+__device__ __forceinline__ float pair_hi(double v) { return (float)v; }
+__device__ __forceinline__ float pair_lo(double v) { return (float)(v - (double)(float)v); }
+
 // Block reductions with a fixed combination order (bit-reproducible).
+// scratch must hold NW doubles (8-byte aligned).
 template <int NW>
-__device__ __forceinline__ float block_min(float v, float* scratch) {
-  v = warp_min(v);
+__device__ __forceinline__ double block_min_d(double v, double* scratch) {
+  v = warp_min_d(v);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   __syncthreads();
   if (lane == 0) scratch[w] = v;
   __syncthreads();
-  float r = scratch[0];
+  double r = scratch[0];
 #pragma unroll
-  for (int i = 1; i < NW; ++i) r = fminf(r, scratch[i]);
+  for (int i = 1; i < NW; ++i) r = fmin(r, scratch[i]);
   return r;
 }
 template <int NW>
@@ -261,17 +331,35 @@ __device__ __forceinline__ void copy_words(uint32_t* dst, const uint8_t* src, in
 // extra warps add exact zeros (and +inf to the minimum) to the CTA
 // statistics, so the results are the same bits as the plain form.
 // --------------------------------------------------------------------------
+//
+// LANES > 1 (cooperative form; the plugin's stage cost split into LANES parts
+// by MPPI_STAGE_COST_SPLIT, BLOCK * LANES threads): the LANES consecutive
+// threads of a sample share its staged noise (each draws every LANES-th
+// step), all step the dynamics, and each accumulates one part of the stage
+// cost (part 0 also the control and terminal costs); the parts are summed as
+// doubles by a butterfly of shuffles at the end, ((p0 + p1) + (p2 + p3)) for
+// four.  A sample's cost then sums its terms in another order than the other
+// forms, so its bits differ from theirs in the last places.
+// --------------------------------------------------------------------------
 constexpr uint32_t kWsChunk = 4;
 
-template <int BLOCK, bool WS = false>
+typedef mppi_stage_cost_split<&MPPI_STAGE_COST_FN> StageSplit;
+// Lanes per sample of the cooperative form (0: the plugin declares no split).
+constexpr int kCoopLanes = StageSplit::parts;
+static_assert(kCoopLanes == 0 || kCoopLanes == 2 || kCoopLanes == 4,
+              "MPPI_STAGE_COST_SPLIT: the part count must be 2 or 4");
+
+template <int BLOCK, bool WS = false, int LANES = 1>
 __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t agent,
                                              uint32_t blk, uint32_t K, uint32_t H,
                                              const float* un_g, float* part) {
-  constexpr int NT = WS ? 2 * BLOCK : BLOCK;  // threads of the CTA
+  static_assert(!(WS && LANES > 1), "the cooperative form is not warp-specialised");
+  constexpr int NT = WS ? 2 * BLOCK : BLOCK * LANES;  // threads of the CTA
   constexpr int NW = NT / 32;
   constexpr int PER_LANE = BLOCK / 32;
+  static_assert(BLOCK % 32 == 0, "sample columns come in warps");
   extern __shared__ __align__(16) float dsm[];
-  __shared__ float red_s[3 * NW];
+  __shared__ __align__(8) float red_s[3 * NW];  // block sums; NW doubles for the minimum
 #if MPPI_MP_SMEM
   __shared__ __align__(16) uint32_t mp_s[(MPPI_MP_BYTES + 3) / 4];
 #endif
@@ -282,7 +370,9 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   const uint32_t tid = threadIdx.x;
   const uint32_t lane = tid & 31, warp = tid >> 5;
   const bool producer = WS && tid >= (uint32_t)BLOCK;  // noise-drawing warp (WS form)
-  const uint32_t col = WS ? tid % BLOCK : tid;         // this thread's sample column
+  // this thread's sample column, and its part of the sample (cooperative form)
+  const uint32_t col = WS ? tid % BLOCK : tid / LANES;
+  const uint32_t sub = tid % LANES;
   const uint32_t HM = H * kM;
   const uint32_t k = blk * BLOCK + col;
   const bool active = k < K;
@@ -352,7 +442,7 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   // independent, so they overlap.  Phase B runs the state recurrence, reading
   // the noise back.  No thread touches another's column until the weighted
   // sums, so neither phase needs a barrier.
-  float J = 0.0f;
+  float J = 0.0f, Jlo = 0.0f;  // the sample's cost as the pair J + Jlo (acc_cost)
   __align__(16) float st[kNPad];
   const bool runs = active && !producer;  // this thread runs a sample's recurrence
   if (runs) {
@@ -399,13 +489,19 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
 #pragma unroll
       for (int i = 0; i < kM; ++i) cc = fmaf(un_s[t * kM + i], sinv[i] * eps[i], cc);
 #endif
-      J = fmaf(a.lambda, cc, J);
+      acc_cost(J, Jlo, (LANES == 1 || sub == 0) ? a.lambda * cc : 0.0f);
     }
 #endif
     MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u, mp,
                      make_uint2(step, mppi_dyn_ctr(k, H, kP, t)), key);
-    J += MPPI_STAGE_COST_FN(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u, mp,
-                            cp);
+    if constexpr (LANES > 1)
+      acc_cost(J, Jlo,
+               StageSplit::part(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u, mp,
+                                cp, (int)sub));
+    else
+      acc_cost(J, Jlo,
+               MPPI_STAGE_COST_FN(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u,
+                                  mp, cp));
   };
   if constexpr (WS) {
     if (staged) {
@@ -431,36 +527,63 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   } else {
     // Time is processed in chunks of TC steps (the whole horizon when the
     // staging buffer holds it).  Phase A draws the chunk's noise into this
-    // thread's own staging column: Philox chains of different steps are
+    // sample's staging column: Philox chains of different steps are
     // independent, so they overlap.  Phase B runs the state recurrence,
-    // reading the noise back.  No thread touches another's column until the
-    // weighted sums, so neither phase needs a barrier.
+    // reading the noise back.  No thread touches another sample's column
+    // until the weighted sums, so neither phase needs a CTA barrier; the
+    // lanes of a cooperative sample (one warp) share a column and meet at a
+    // warp barrier between the phases.
     const uint32_t TC = staged ? H : a.stage_rows / kM;
     for (uint32_t t0 = 0; t0 < H; t0 += TC) {
       const uint32_t t1 = min(H, t0 + TC);
       const uint32_t row0 = staged ? 0u : t0;
 #pragma unroll 4
-      for (uint32_t t = t0; t < t1; ++t) draw(t, row0);
+      for (uint32_t t = t0 + sub; t < t1; t += LANES) draw(t, row0);
+      if constexpr (LANES > 1) __syncwarp();
       if (runs)
         for (uint32_t t = t0; t < t1; ++t) advance(t, row0);
+      if constexpr (LANES > 1) __syncwarp();
     }
   }
-  if (runs) {
-    J += MPPI_TERMINAL_COST_FN(reinterpret_cast<TermStateT>(reinterpret_cast<void*>(st)), mp, cp);
-    if (a.costs) a.costs[(size_t)agent * a.K + k] = J;  // agent stride: the largest K
+  double Jd = __longlong_as_double(0x7ff0000000000000ll);  // +inf: no sample here
+  if constexpr (LANES > 1) {
+    // part 0 carries the terminal cost; the parts meet in a butterfly
+    if (runs && sub == 0)
+      acc_cost(J, Jlo,
+               MPPI_TERMINAL_COST_FN(reinterpret_cast<TermStateT>(reinterpret_cast<void*>(st)),
+                                     mp, cp));
+    double Jp = cost_pair(J, Jlo);
+#pragma unroll
+    for (int o = 1; o < LANES; o <<= 1) Jp += __shfl_xor_sync(kFull, Jp, o);
+    if (runs) Jd = Jp;
+  } else if (runs) {
+    acc_cost(J, Jlo,
+             MPPI_TERMINAL_COST_FN(reinterpret_cast<TermStateT>(reinterpret_cast<void*>(st)), mp,
+                                   cp));
+    Jd = cost_pair(J, Jlo);
   }
+  // one thread per sample counts below (part 0 of a cooperative sample)
+  const bool counts = runs && sub == 0;
+  if (counts && a.costs) {  // inspection calls only; agent stride: the largest K
+    a.costs[(size_t)agent * a.K + k] = pair_hi(Jd);
+    a.costs_lo[(size_t)agent * a.K + k] = pair_lo(Jd);
+  }
+  if (!counts) Jd = __longlong_as_double(0x7ff0000000000000ll);
 
   // ---- CTA softmax statistics against the CTA minimum ----
-  const float bmin = block_min<NW>(runs ? J : pos_inf(), red_s);
-  const float e = runs ? expf(-(J - bmin) / a.lambda) : 0.0f;
-  float s_e = e, s_e2 = e * e, s_c = runs ? J : 0.0f;
+  // The minimum and the differences c_k - m_b are taken on the cost pairs
+  // (as doubles), so exp(-(c_k - m_b) / lambda) sees no rounding of c_k.
+  const double bmin = block_min_d<NW>(Jd, reinterpret_cast<double*>(red_s));
+  const float e = counts ? expf(-(float)(Jd - bmin) / a.lambda) : 0.0f;
+  float s_e = e, s_e2 = e * e, s_c = counts ? pair_hi(Jd) : 0.0f;
   block_sum3<NW>(s_e, s_e2, s_c, red_s);
-  if (!producer) e_s[col] = e;
+  if (!producer && sub == 0) e_s[col] = e;
   if (tid == 0) {
-    part[0] = bmin;
+    part[0] = pair_hi(bmin);
     part[1] = s_e;
     part[2] = s_e2;
     part[3] = s_c;
+    part[4] = pair_lo(bmin);
   }
   __syncthreads();
   float e_r[PER_LANE];
@@ -477,7 +600,7 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
       __syncthreads();
       const uint32_t t0 = r0 / kM, t1 = (r0 + rows) / kM;
       if (!producer)
-        for (uint32_t t = t0; t < t1; ++t) draw(t, t0);
+        for (uint32_t t = t0 + sub; t < t1; t += LANES) draw(t, t0);
       __syncthreads();
     } else {
       base = stage_s + (size_t)r0 * BLOCK;
@@ -521,13 +644,14 @@ __device__ __forceinline__ void fused_combine_tail(const MppiRolloutArgs& a, uin
 // Uniform batch: grid (nblk, num_agents), every agent K samples, horizon H.
 // FUSED: the kernel form with the combine tail (a separate entry point, so
 // the plain form keeps its register allocation).
-template <int BLOCK, bool FUSED, bool WS = false>
+template <int BLOCK, bool FUSED, bool WS = false, int LANES = 1>
 __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   mppi_allow_dependent_launch();
   const uint32_t agent = blockIdx.y, blk = blockIdx.x;
-  rollout_item<BLOCK, WS>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
-                          a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
-  if (FUSED && a.agent_done) fused_combine_tail<WS ? 2 * BLOCK : BLOCK>(a, agent, a.nblk);
+  rollout_item<BLOCK, WS, LANES>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
+                                 a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
+  if (FUSED && a.agent_done)
+    fused_combine_tail<WS ? 2 * BLOCK : BLOCK * LANES>(a, agent, a.nblk);
 }
 
 // Uneven batch: work items (agent, CTA-of-agent), longest horizons first.
@@ -597,12 +721,71 @@ __device__ __noinline__ void compute_features(const float* st, const uint8_t* mp
   for (int i = 0; i < MPPI_MAX_FEATURES; ++i) f[i] = 0.0f;
   MPPI_FEATURES_FN(st, mp, cp, f);
 }
+
+// The proposal network for one row, by the calling CTA's threads (all of
+// them call it): in -> hidden -> hidden -> hidden -> out with GELU between,
+// the features, weights and hidden activations rounded to BF16 and FP32
+// accumulation, like the tensor-core kernels.  Output n of a layer belongs
+// to threads n, n + blockDim.x, ...; its dot product runs over k in a fixed
+// order (four partial sums over k-blocks of 8, blocks b = 0, 1, 2, 3 mod 4,
+// added as (s0 + s1) + (s2 + s3)), so the result does not depend on the
+// CTA size -- one compiled copy serves the combine kernel, the rollout
+// kernels' fused combines and the first step's kernel.  The weights stream
+// from L2 in 16-byte pieces of their K-major core-matrix image.
+__device__ __forceinline__ float bf16_lo(uint32_t w) { return __uint_as_float(w << 16); }
+__device__ __forceinline__ float bf16_hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
+
+__device__ __noinline__ void network_row(const float* f, const MppiNetRows& net, float* out) {
+  constexpr int kMaxHidden = 256;
+  __shared__ __align__(16) float h_s[2][kMaxHidden];
+  const uint32_t tid = threadIdx.x, nt = blockDim.x;
+  for (uint32_t k = tid; k < net.in; k += nt)
+    h_s[1][k] = mppi_round_bf16(k < (uint32_t)MPPI_MAX_FEATURES ? f[k] : 0.0f);
+  __syncthreads();
+  for (int l = 0; l < 4; ++l) {
+    const uint32_t K = l == 0 ? net.in : net.hidden;
+    const uint32_t N = l == 3 ? net.out : net.hidden;
+    const float* hin = h_s[(l + 1) & 1];
+    float* hout = h_s[l & 1];
+    const uint4* W = reinterpret_cast<const uint4*>(net.w[l]);
+    for (uint32_t n = tid; n < N; n += nt) {
+      // row n, k-block b (8 inputs) at element (n / 8) 8K + 64 b + (n % 8) 8
+      const uint4* wr = W + (size_t)(n >> 3) * K + (n & 7u);
+      float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 4
+      for (uint32_t b = 0; b < K / 8; ++b) {
+        const uint4 w8 = __ldg(wr + 8 * b);
+        const float4 h0 = *reinterpret_cast<const float4*>(hin + 8 * b);
+        const float4 h1 = *reinterpret_cast<const float4*>(hin + 8 * b + 4);
+        float& s = acc[b & 3u];
+        s = fmaf(bf16_lo(w8.x), h0.x, s);
+        s = fmaf(bf16_hi(w8.x), h0.y, s);
+        s = fmaf(bf16_lo(w8.y), h0.z, s);
+        s = fmaf(bf16_hi(w8.y), h0.w, s);
+        s = fmaf(bf16_lo(w8.z), h1.x, s);
+        s = fmaf(bf16_hi(w8.z), h1.y, s);
+        s = fmaf(bf16_lo(w8.w), h1.z, s);
+        s = fmaf(bf16_hi(w8.w), h1.w, s);
+      }
+      const float z = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + net.b[l][n];
+      if (l < 3)
+        hout[n] = mppi_round_bf16(mppi_gelu(z));
+      else
+        out[n] = z;
+    }
+    __syncthreads();
+  }
+}
 #endif
 
 template <int CB>
 __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t agent,
                                               float* dsm) {
   __shared__ float stat_s[4];
+  __shared__ double min_s;
+#ifdef MPPI_FEATURES_FN
+  __shared__ float feat_s[MPPI_MAX_FEATURES];  // the next step's network input
+#endif
   const uint32_t tid = threadIdx.x;
   const bool ragged = a.agent_K != nullptr;
   const uint32_t K = ragged ? a.agent_K[agent] : a.K;
@@ -617,14 +800,19 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   // Statistics over the CTA records by warp 0 alone (lane l takes records
   // l, l + 32, ...), so the summation order -- and every bit of the result --
   // is the same whichever CTA size runs the combine.
+  // The records' minima are cost pairs (hi at 0, lo at 4), compared and
+  // subtracted as doubles like the rollout's per-sample costs.
   if (tid < 32) {
-    float lm = pos_inf();
-    for (uint32_t b = tid; b < nblk; b += 32) lm = fminf(lm, __ldcg(P + (size_t)b * ps));
-    const float Mw = warp_min(lm);
+    double lm = __longlong_as_double(0x7ff0000000000000ll);
+    for (uint32_t b = tid; b < nblk; b += 32) {
+      const float* pb = P + (size_t)b * ps;
+      lm = fmin(lm, cost_pair(__ldcg(pb), __ldcg(pb + 4)));
+    }
+    const double Mw = warp_min_d(lm);
     float S = 0.0f, Q = 0.0f, C = 0.0f;
     for (uint32_t b = tid; b < nblk; b += 32) {
       const float* pb = P + (size_t)b * ps;
-      const float sc = expf(-(__ldcg(pb) - Mw) / a.lambda);
+      const float sc = expf(-(float)(cost_pair(__ldcg(pb), __ldcg(pb + 4)) - Mw) / a.lambda);
       scale_s[b] = sc;
       S = fmaf(sc, __ldcg(pb + 1), S);
       Q = fmaf(sc * sc, __ldcg(pb + 2), Q);
@@ -634,7 +822,8 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
     Q = warp_sum(Q);
     C = warp_sum(C);
     if (tid == 0) {
-      stat_s[0] = Mw;
+      min_s = Mw;
+      stat_s[0] = pair_hi(Mw);
       stat_s[1] = S;
       stat_s[2] = Q;
       stat_s[3] = C;
@@ -665,10 +854,12 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
     a.diag[agent * 3 + 1] = C / (float)K;
     a.diag[agent * 3 + 2] = S * S / Q;  // 1 / sum w^2 with w = e / S
     if (a.stats) {
-      a.stats[agent * 4 + 0] = M;
-      a.stats[agent * 4 + 1] = S;
-      a.stats[agent * 4 + 2] = Q;
-      a.stats[agent * 4 + 3] = C;
+      float* st = a.stats + (size_t)agent * MPPI_STATS_STRIDE;
+      st[0] = M;
+      st[1] = S;
+      st[2] = Q;
+      st[3] = C;
+      st[4] = pair_lo(min_s);
     }
   }
   if (!a.propagate) return;
@@ -716,11 +907,20 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
                        a.cost_params + a.cost_stride * agent, f);
       float* o = a.features + (size_t)agent * a.feature_stride;
 #pragma unroll
-      for (int i = 0; i < MPPI_MAX_FEATURES; ++i)
+      for (int i = 0; i < MPPI_MAX_FEATURES; ++i) {
         if ((uint32_t)i < a.feature_stride) o[i] = f[i];
+        feat_s[i] = f[i];
+      }
     }
 #endif
   }
+#ifdef MPPI_FEATURES_FN
+  // ... and the next step's network output, by this CTA (the per-agent form)
+  if (a.features && a.net.w[0]) {
+    __syncthreads();  // feat_s complete
+    network_row(feat_s, a.net, a.net.out_buf + (size_t)agent * a.net.out_stride);
+  }
+#endif
   for (uint32_t j = tid; j < HM; j += CB) {
     const uint32_t t = j / kM, d = j % kM;
     un[j] = (t + 1 < H) ? u_s[j + kM] : u_s[(H - 1) * kM + d];  // shift left, hold last
@@ -758,6 +958,21 @@ extern "C" __global__ void __launch_bounds__(256, 2)
   mppi::rollout_body<128, true, true>(a);
 }
 
+// Cooperative forms (plugins with MPPI_STAGE_COST_SPLIT): 128 threads, i.e.
+// 128 / kCoopLanes samples per CTA.  Without a split the entries exist but
+// the host never launches them (mppi_coop_lanes reads 0).
+constexpr int kCoopBlock = mppi::kCoopLanes > 0 ? 128 / mppi::kCoopLanes : 128;
+extern "C" __device__ const uint32_t mppi_coop_lanes = mppi::kCoopLanes;
+extern "C" __global__ void __launch_bounds__(128, 4) mppi_rollout_coop(const MppiRolloutArgs a) {
+  if constexpr (mppi::kCoopLanes > 1)
+    mppi::rollout_body<kCoopBlock, false, false, mppi::kCoopLanes>(a);
+}
+extern "C" __global__ void __launch_bounds__(128, 4)
+    mppi_rollout_coop_fused(const MppiRolloutArgs a) {
+  if constexpr (mppi::kCoopLanes > 1)
+    mppi::rollout_body<kCoopBlock, true, false, mppi::kCoopLanes>(a);
+}
+
 // Uneven batches always use 128-thread CTAs, so the partition of samples into
 // CTAs -- and therefore every floating-point sum -- does not depend on the
 // tuned grid size or staging mode.
@@ -779,9 +994,11 @@ extern "C" __global__ void __launch_bounds__(256) mppi_weights(const MppiWeights
   const uint32_t agent = blockIdx.y;
   const uint32_t k = blockIdx.x * 256 + threadIdx.x;
   if (k >= a.K) return;
-  const float M = a.stats[agent * 4 + 0], S = a.stats[agent * 4 + 1];
-  const float c = a.costs[(size_t)agent * a.K + k];
-  a.weights[(size_t)agent * a.K + k] = expf(-(c - M) / a.lambda) / S;
+  const float* st = a.stats + (size_t)agent * MPPI_STATS_STRIDE;
+  const double M = mppi::cost_pair(st[0], st[4]);
+  const size_t i = (size_t)agent * a.K + k;
+  const double c = mppi::cost_pair(a.costs[i], a.costs_lo[i]);
+  a.weights[i] = expf(-(float)(c - M) / a.lambda) / st[1];
 }
 
 extern "C" __global__ void __launch_bounds__(128) mppi_noise(const MppiNoiseArgs a) {
@@ -803,6 +1020,38 @@ extern "C" __global__ void __launch_bounds__(128) mppi_noise(const MppiNoiseArgs
 }
 
 #ifdef MPPI_FEATURES_FN
+// Proposal features and the per-agent network of state rows: one CTA per
+// row (the first step of a loop whose combines evaluate the network).
+extern "C" __global__ void __launch_bounds__(128) mppi_proposal_rows(const MppiProposalRowsArgs a) {
+  __shared__ float feat_s[MPPI_MAX_FEATURES];
+  const uint32_t r = blockIdx.x;
+  const MppiFeaturesArgs& fa = a.f;
+  // the states come from the previous kernel (no-op in plain launches)
+  mppi::mppi_grid_dependency_wait();
+  if (threadIdx.x == 0) {
+    const uint32_t agent = r % fa.agents_mod;
+    __align__(16) float st[mppi::kNPad];
+    const float* xr = fa.x + (size_t)r * fa.x_stride;
+#pragma unroll
+    for (int d = 0; d < mppi::kN; ++d) st[d] = xr[d];
+#pragma unroll
+    for (int d = mppi::kN; d < mppi::kNPad; ++d) st[d] = 0.0f;
+    float f[MPPI_MAX_FEATURES];
+    mppi::compute_features(st, fa.model_params + fa.model_stride * agent,
+                           fa.cost_params + fa.cost_stride * agent, f);
+#pragma unroll
+    for (int i = 0; i < MPPI_MAX_FEATURES; ++i) feat_s[i] = f[i];
+    if (fa.out) {
+      float* o = fa.out + (size_t)r * fa.out_stride;
+#pragma unroll
+      for (int i = 0; i < MPPI_MAX_FEATURES; ++i)
+        if ((uint32_t)i < fa.out_stride) o[i] = f[i];
+    }
+  }
+  __syncthreads();
+  mppi::network_row(feat_s, a.net, a.net.out_buf + (size_t)r * a.net.out_stride);
+}
+
 // Proposal features: one thread per state row.
 extern "C" __global__ void __launch_bounds__(128) mppi_features(const MppiFeaturesArgs a) {
   const uint32_t r = blockIdx.x * 128 + threadIdx.x;

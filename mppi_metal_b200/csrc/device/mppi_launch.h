@@ -9,8 +9,30 @@
 #endif
 
 // Floats in front of the weighted-noise sums of one partial record:
-// [block min cost, sum e, sum e^2, sum cost].
-#define MPPI_PARTIAL_HEAD 4
+// [block min cost (hi), sum e, sum e^2, sum cost, block min cost (lo), 0, 0, 0].
+// Minimum costs travel as pairs hi + lo of floats (the rollout accumulates
+// each sample's cost that way), so the rescaling exp(-(m_b - M) / lambda)
+// sees their difference unrounded.
+#define MPPI_PARTIAL_HEAD 8
+
+// Floats per agent of the combine statistics:
+// [min cost (hi), sum e, sum e^2, sum cost, min cost (lo), 0, 0, 0].
+#define MPPI_STATS_STRIDE 8
+
+// The learned proposal's network evaluated per agent on the CUDA cores (the
+// per-agent form of its forward pass, used where few agents make the
+// tensor-core batch kernel latency-bound): layer l's BF16 weights in the
+// tensor-core kernels' K-major core-matrix image (rows = outputs), its FP32
+// biases, and where the outputs go.  w[0] null = not used.
+struct MppiNetRows {
+  const uint16_t* w[4];
+  const float* b[4];
+  uint32_t in;          // padded input width of layer 0 (32)
+  uint32_t hidden;      // hidden width (256)
+  uint32_t out;         // padded outputs of layer 3 (multiple of 16)
+  uint32_t out_stride;  // floats between agents' output rows
+  float* out_buf;       // [N][out_stride]: predicted u* then raw log-scales
+};
 
 // One launch of the combine (+ optional propagate & shift) kernel.
 // Grid = num_agents, one CTA per agent.
@@ -32,7 +54,7 @@ struct MppiCombineArgs {
   float* u_nom;        // [N][H*m] read; shifted in place when propagating
   float* u_out;        // [N][H*m]
   float* diag;         // [N][3]: best cost, mean cost, effective sample size
-  float* stats;        // [N][4]: min, sum e, sum e^2, sum cost (may be null)
+  float* stats;        // [N][MPPI_STATS_STRIDE] (may be null)
   float* x;            // [N][n] state, propagated in place
   float* hist_states;  // [T][N][n] (may be null)
   float* hist_controls;  // [T][N][m] (may be null)
@@ -53,6 +75,9 @@ struct MppiCombineArgs {
   float* features;          // [N][feature_stride]
   uint32_t feature_stride;  // <= MPPI_MAX_FEATURES
   uint32_t pad1;
+  // The next step's network output from those features, computed here by
+  // the combine's threads (net.w[0] null: by the separate network kernel).
+  MppiNetRows net;
 };
 
 // One launch of the fused rollout kernel: every agent of the batch, every
@@ -83,7 +108,10 @@ struct MppiRolloutArgs {
   const uint8_t* cost_params;
   uint64_t model_stride;
   uint64_t cost_stride;
-  float* costs;     // [N][K] per-sample costs (may be null)
+  // Per-sample costs as pairs costs + costs_lo, [N][K] each; null on the
+  // closed loops (only single-step inspection calls keep them).
+  float* costs;
+  float* costs_lo;
   float* partials;  // [N][nblk][pstride]
   // Uneven batches (all null for a uniform batch).  Agent a has agent_K[a]
   // samples, horizon agent_H[a] <= H (nominals keep the stride H*m) and its
@@ -139,6 +167,13 @@ struct MppiFeaturesArgs {
   float* out;
 };
 
+// Proposal features and the per-agent network of state rows (the first step
+// of a loop whose combines evaluate the network): one CTA per row.
+struct MppiProposalRowsArgs {
+  MppiFeaturesArgs f;
+  MppiNetRows net;
+};
+
 // Normalised weights from the per-sample costs and the combine statistics
 // (inspection path; the control update does not need them materialised).
 struct MppiWeightsArgs {
@@ -146,9 +181,10 @@ struct MppiWeightsArgs {
   uint32_t K;
   float lambda;
   uint32_t pad0;
-  const float* costs;  // [N][K]
-  const float* stats;  // [N][4]
-  float* weights;      // [N][K]
+  const float* costs;     // [N][K] hi parts
+  const float* costs_lo;  // [N][K] lo parts
+  const float* stats;     // [N][MPPI_STATS_STRIDE]
+  float* weights;         // [N][K]
 };
 
 // Noise of samples [k0, k0 + count) of one agent, every time step.

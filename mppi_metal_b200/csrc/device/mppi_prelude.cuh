@@ -32,7 +32,8 @@ typedef long long int64_t;
 #endif
 
 #ifndef MPPI_MAX_STATE_BYTES
-// Thread-local state buffer limit (shaders/mppi_core.h:32).
+// Thread-local state buffer size (shaders/mppi_core.h:32: 128 bytes).  The
+// library compiles each module with the larger of 128 and the state's size.
 #define MPPI_MAX_STATE_BYTES 128
 #endif
 #ifndef MPPI_MAX_CONTROL_DIM
@@ -70,6 +71,69 @@ __device__ __forceinline__ float mppi_default_terminal_cost(const uint8_t*, cons
                                                             const uint8_t*) {
   return 0.0f;
 }
+
+// ---------------------------------------------------------------------------
+// Parameter-layout declaration (the ParamLayout contract of the reference's
+// include/mppi_metal/mppi_types.hpp:88-94, whose README promises that
+// initialize fails when the declared layout does not match the binding).
+// A plugin may state the layout of the blobs its callables read:
+//   MPPI_PARAM_LAYOUT(model_bytes, model_align, cost_bytes, cost_align, "schema")
+//   MPPI_PARAM_LAYOUT_OF(ModelParamsT, CostParamsT, "schema")
+// and the module then compiles only if the driver's ParamLayout agrees:
+// equal blob sizes, an alignment that is 1 (unspecified) or a multiple of the
+// declared one, and a schema_hash that is empty or equal to the declared
+// string.  A plugin without the declaration is bound as the reference binds
+// it (sizes checked against the blobs only).
+// ---------------------------------------------------------------------------
+template <int>
+struct mppi_declared_param_layout {
+  static constexpr bool declared = false;
+  static constexpr unsigned long long model_size = 0, model_align = 1;
+  static constexpr unsigned long long cost_size = 0, cost_align = 1;
+  static constexpr const char* schema = "";
+};
+#define MPPI_PARAM_LAYOUT(MODEL_BYTES, MODEL_ALIGN, COST_BYTES, COST_ALIGN, SCHEMA) \
+  template <>                                                                      \
+  struct mppi_declared_param_layout<0> {                                           \
+    static constexpr bool declared = true;                                         \
+    static constexpr unsigned long long model_size = (MODEL_BYTES);                \
+    static constexpr unsigned long long model_align = (MODEL_ALIGN);               \
+    static constexpr unsigned long long cost_size = (COST_BYTES);                  \
+    static constexpr unsigned long long cost_align = (COST_ALIGN);                 \
+    static constexpr const char* schema = SCHEMA;                                  \
+  };
+#define MPPI_PARAM_LAYOUT_OF(MODEL_T, COST_T, SCHEMA) \
+  MPPI_PARAM_LAYOUT(sizeof(MODEL_T), alignof(MODEL_T), sizeof(COST_T), alignof(COST_T), SCHEMA)
+
+// ---------------------------------------------------------------------------
+// Optional split stage cost (no counterpart in the reference).  A plugin
+// whose stage cost is a sum of independent terms may declare
+//   MPPI_STAGE_COST_SPLIT(stage_fn, part_fn, PARTS)
+// with part_fn(state, control, model_params, cost_params, int part) returning
+// part `part` of stage_fn's value (the parts sum to it).  For launches with
+// few CTAs (latency-bound: each sample's serial chain sets the time), the
+// library then runs a cooperative rollout form: PARTS lanes per sample all
+// step the dynamics and each evaluates one part, so the chain per step
+// carries 1/PARTS of the cost terms.
+// ---------------------------------------------------------------------------
+template <auto F>
+struct mppi_stage_cost_split {
+  static constexpr int parts = 0;
+  template <class S>
+  __device__ static float part(S, const float*, const uint8_t*, const uint8_t*, int) {
+    return 0.0f;
+  }
+};
+#define MPPI_STAGE_COST_SPLIT(STAGE_FN, PART_FN, PARTS)                               \
+  template <>                                                                        \
+  struct mppi_stage_cost_split<&STAGE_FN> {                                          \
+    static constexpr int parts = (PARTS);                                            \
+    template <class S>                                                               \
+    __device__ static float part(S s, const float* u, const uint8_t* mp,             \
+                                 const uint8_t* cp, int j) {                         \
+      return PART_FN(s, u, mp, cp, j);                                               \
+    }                                                                                \
+  };
 
 // First-parameter type of a plain function, so the library can hand a
 // plugin its state in whatever pointer type the plugin declared.

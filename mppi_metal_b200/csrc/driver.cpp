@@ -127,10 +127,12 @@ bool MPPIDriver::initialize(const ModelPluginSpec& model, std::string* error) {
 	}
 
 	// ---- added: the limits the reference's kernels silently truncate at
-	// (shaders/mppi_core.h:32-33), and the ParamLayout alignment contract ----
-	if (cfg.state_dim * 4u > 128u) {
+	// (shaders/mppi_core.h:32-33; the state buffer is sized per module here,
+	// up to MPPI_MAX_STATE_DIM floats), and the ParamLayout alignment
+	// contract ----
+	if (cfg.state_dim > MPPI_MAX_STATE_DIM) {
 		return fail("DriverConfig::state_dim (" + std::to_string(cfg.state_dim) +
-			") exceeds the 128-byte state limit (32 floats).");
+			") exceeds the state limit of " + std::to_string(MPPI_MAX_STATE_DIM) + " floats.");
 	}
 	if (cfg.control_dim > 16u) {
 		return fail("DriverConfig::control_dim (" + std::to_string(cfg.control_dim) +
@@ -160,6 +162,9 @@ bool MPPIDriver::initialize(const ModelPluginSpec& model, std::string* error) {
 	plug.model_params_size = model.param_layout.model_params_size;
 	plug.cost_params_size = model.param_layout.cost_params_size;
 	plug.seed = model.rng.seed;
+	plug.model_params_alignment = model.param_layout.model_params_alignment;
+	plug.cost_params_alignment = model.param_layout.cost_params_alignment;
+	plug.schema_hash = model.param_layout.schema_hash.c_str();
 	mppi_backend_config bc{};
 	bc.state_dim = cfg.state_dim;
 	bc.control_dim = cfg.control_dim;

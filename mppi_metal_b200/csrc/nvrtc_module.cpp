@@ -102,6 +102,13 @@ std::map<uint64_t, std::shared_ptr<const KernelModule>> g_modules;
 
 }  // namespace
 
+bool valid_schema_hash(const std::string& s) {
+  if (s.size() > 256) return false;
+  for (char c : s)
+    if (c < 0x20 || c > 0x7e || c == '"' || c == '\\') return false;
+  return true;
+}
+
 const char* embedded_source(const char* name) {
   for (const auto& f : kEmbeddedFiles)
     if (strcmp(f.name, name) == 0) return f.text;
@@ -141,6 +148,9 @@ int compile_module(const ModuleSpec& spec, bool use_cache, bool ptxas_verbose,
       "-lineinfo",
       "--include-path=" + dir_of(spec.plugin_path),
       "-DMPPI_STATE_DIM=" + std::to_string(spec.state_dim),
+      // the state buffer: the reference's 128 bytes, or the state's size
+      "-DMPPI_MAX_STATE_BYTES=" +
+          std::to_string(std::max<uint64_t>(128, ((uint64_t)spec.state_dim * 4 + 15) / 16 * 16)),
       "-DMPPI_CONTROL_DIM=" + std::to_string(spec.control_dim),
       "-DMPPI_COV_FULL=" + std::to_string(spec.cov_full ? 1 : 0),
       "-DMPPI_CONTROL_COST=" + std::to_string(spec.control_cost ? 1 : 0),
@@ -151,7 +161,15 @@ int compile_module(const ModuleSpec& spec, bool use_cache, bool ptxas_verbose,
       "-DMPPI_STAGE_COST_FN=" + stage,
       "-DMPPI_TERMINAL_COST_FN=" + term,
       "-DMPPI_PROPOSAL=" + std::to_string(spec.proposal ? 1 : 0),
+      "-DMPPI_MP_ALIGN=" + std::to_string(spec.model_params_alignment ? spec.model_params_alignment : 1),
+      "-DMPPI_CP_ALIGN=" + std::to_string(spec.cost_params_alignment ? spec.cost_params_alignment : 1),
+      "-DMPPI_SCHEMA_HASH=\"" + spec.schema_hash + "\"",
   };
+  if (!valid_schema_hash(spec.schema_hash)) {
+    *error = "ParamLayout::schema_hash must be printable ASCII without quotes or backslashes "
+             "(at most 256 characters).";
+    return MPPI_ERR_INVALID;
+  }
   if (!spec.features.empty()) opts.push_back("-DMPPI_FEATURES_FN=" + spec.features);
   if (ptxas_verbose) opts.push_back("--ptxas-options=-v");
 
@@ -214,6 +232,17 @@ int compile_module(const ModuleSpec& spec, bool use_cache, bool ptxas_verbose,
                  "'.";
         return MPPI_ERR_CALLABLE;
       }
+    }
+    // ParamLayout against the plugin's MPPI_PARAM_LAYOUT: name the field
+    const std::string marker = "MPPI_PARAM_LAYOUT_MISMATCH: ";
+    const size_t at = log.find(marker);
+    if (at != std::string::npos) {
+      const size_t from = at + marker.size();
+      const size_t to = log.find('"', from);
+      *error = "Declared parameter layout does not match the plugin '" + spec.plugin_path +
+               "': " + log.substr(from, to == std::string::npos ? std::string::npos : to - from) +
+               " (MPPI_PARAM_LAYOUT).";
+      return MPPI_ERR_INVALID;
     }
     *error = "Failed to compile user plugin '" + spec.plugin_path + "' with the MPPI kernels:\n" +
              log;
@@ -283,11 +312,25 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->rollout_ws, mod->library, "mppi_rollout_ws_b128");
   if (ce == cudaSuccess)
     ce = cudaLibraryGetKernel(&mod->rollout_ws_fused, mod->library, "mppi_rollout_ws_fused_b128");
+  if (ce == cudaSuccess)
+    ce = cudaLibraryGetKernel(&mod->rollout_coop, mod->library, "mppi_rollout_coop");
+  if (ce == cudaSuccess)
+    ce = cudaLibraryGetKernel(&mod->rollout_coop_fused, mod->library, "mppi_rollout_coop_fused");
+  if (ce == cudaSuccess) {
+    // lanes per sample of the cooperative form (0: the plugin declares no split)
+    void* g = nullptr;
+    size_t gs = 0;
+    ce = cudaLibraryGetGlobal(&g, &gs, mod->library, "mppi_coop_lanes");
+    if (ce == cudaSuccess && gs == sizeof(uint32_t))
+      ce = cudaMemcpy(&mod->coop_lanes, g, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+  }
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->combine, mod->library, "mppi_combine");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->weights, mod->library, "mppi_weights");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->noise, mod->library, "mppi_noise");
   if (ce == cudaSuccess && !spec.features.empty())
     ce = cudaLibraryGetKernel(&mod->features, mod->library, "mppi_features");
+  if (ce == cudaSuccess && !spec.features.empty())
+    ce = cudaLibraryGetKernel(&mod->proposal_rows, mod->library, "mppi_proposal_rows");
   for (int i = 0; i < 3 && ce == cudaSuccess; ++i) {
     cudaFuncAttributes fa{}, ff{};
     ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout[i]));
@@ -301,6 +344,13 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
     if (ce == cudaSuccess)
       ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_ws_fused));
     mod->ws_static_smem = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
+  }
+  if (ce == cudaSuccess) {
+    cudaFuncAttributes fa{}, ff{};
+    ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout_coop));
+    if (ce == cudaSuccess)
+      ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_coop_fused));
+    mod->coop_static_smem = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
   }
   if (ce == cudaSuccess) {
     cudaFuncAttributes fa{}, ff{};

@@ -32,7 +32,16 @@ struct ModuleSpec {
   std::string features;     // proposal-feature callable ("" = none)
   uint64_t model_params_bytes = 0;
   uint64_t cost_params_bytes = 0;
+  // ParamLayout alignments and schema_hash, checked at compile time against
+  // a plugin's MPPI_PARAM_LAYOUT declaration (mppi_prelude.cuh)
+  uint64_t model_params_alignment = 1;
+  uint64_t cost_params_alignment = 1;
+  std::string schema_hash;
 };
+
+// Whether `s` can travel as the schema string of the compile (printable
+// ASCII without quotes or backslashes, at most 256 characters).
+bool valid_schema_hash(const std::string& s);
 
 // Rollout block sizes compiled into every module (mppi_rollout_b<N>).
 constexpr int kRolloutBlocks[3] = {64, 128, 256};
@@ -48,10 +57,18 @@ struct KernelModule {
   cudaKernel_t rollout_ws = nullptr;
   cudaKernel_t rollout_ws_fused = nullptr;
   size_t ws_static_smem = 0;
+  // cooperative forms (128 threads, coop_lanes per sample), plain and fused;
+  // coop_lanes = 0 when the plugin declares no split stage cost
+  cudaKernel_t rollout_coop = nullptr;
+  cudaKernel_t rollout_coop_fused = nullptr;
+  uint32_t coop_lanes = 0;
+  size_t coop_static_smem = 0;
   cudaKernel_t combine = nullptr;
   cudaKernel_t weights = nullptr;
   cudaKernel_t noise = nullptr;
   cudaKernel_t features = nullptr;  // only when ModuleSpec::features is set
+  // features + the per-agent network, one CTA per row (same condition)
+  cudaKernel_t proposal_rows = nullptr;
   // static shared memory of the rollout kernels, the larger of the plain and
   // fused forms (their dynamic share is sized so that this plus the dynamic
   // part keeps the target residency)

@@ -23,6 +23,18 @@ struct ProposalShape {
 
 ProposalShape proposal_shape(const mppi_proposal* p);
 
+// The network's parameters as the per-agent form reads them: layer l's BF16
+// weight image (K-major core-matrix layout, rows = outputs) and FP32 biases,
+// the padded input width, the hidden width and the padded output count.
+struct ProposalWeights {
+  const uint16_t* w[4];
+  const float* b[4];
+  uint32_t in;
+  uint32_t hidden;
+  uint32_t out;
+};
+ProposalWeights proposal_weights(const mppi_proposal* p);
+
 // Enqueues the network's forward pass for `rows` feature rows on `stream`
 // (capturable into a CUDA graph): out[r][0..H*m) predicted u*, then m raw
 // log-scales.  programmatic: launched with programmatic stream

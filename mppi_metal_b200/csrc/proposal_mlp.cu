@@ -50,6 +50,7 @@
 
 #include "../../include/mppi_b200/mppi_backend.h"
 #include "../../include/mppi_b200/mppi_proposal.h"
+#include "device/mppi_gelu.cuh"
 #include "device/tc_sm100.cuh"
 #include "proposal.hpp"
 
@@ -94,37 +95,14 @@ __host__ __device__ __forceinline__ size_t timg(uint32_t r, uint32_t col, uint32
          (col & 7);
 }
 
-// GELU(z) = z Phi(z) with Phi(z) = (1 + erf(z / sqrt 2)) / 2, and its
-// derivative Phi(z) + z phi(z).  erf by Abramowitz and Stegun, "Handbook of
-// Mathematical Functions", eq. 7.1.26 (Hastings' approximation): for x >= 0,
-// erf x = 1 - t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-x^2) with
-// t = 1 / (1 + p x), |error| <= 1.5e-7; the reciprocal and the exponential
-// come from the SM's approximate instructions (relative errors of order
-// 2^-22).  The exp(-x^2) = exp(-z^2 / 2) it computes is the Gaussian factor of
-// the derivative as well.  The activations are rounded to BF16 (8 significant
-// bits) before they feed the next GEMM, far above this error.
-__device__ __forceinline__ void gelu_phi(float z, float& cdf, float& gauss) {
-  const float x = fabsf(z) * 0.70710678118654752f;
-  float t;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(t) : "f"(fmaf(0.3275911f, x, 1.0f)));
-  float p = fmaf(1.061405429f, t, -1.453152027f);
-  p = fmaf(p, t, 1.421413741f);
-  p = fmaf(p, t, -0.284496736f);
-  p = fmaf(p, t, 0.254829592f);
-  p *= t;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(gauss) : "f"(-1.44269504088896341f * x * x));
-  cdf = fmaf(0.5f, copysignf(fmaf(-p, gauss, 1.0f), z), 0.5f);
-}
-
-__device__ __forceinline__ float gelu(float z) {
-  float cdf, g;
-  gelu_phi(z, cdf, g);
-  return z * cdf;
-}
+// GELU and its derivative (csrc/device/mppi_gelu.cuh: erf by Abramowitz and
+// Stegun 7.1.26 on the SM's reciprocal and exp2), shared with the per-agent
+// network evaluation of the MPPI module.
+__device__ __forceinline__ float gelu(float z) { return mppi_gelu(z); }
 
 __device__ __forceinline__ float gelu_grad(float z) {
   float cdf, g;
-  gelu_phi(z, cdf, g);
+  mppi_gelu_phi(z, cdf, g);
   return fmaf(z * 0.39894228040143268f, g, cdf);
 }
 
@@ -1084,6 +1062,18 @@ namespace mppi_b200 {
 ProposalShape proposal_shape(const mppi_proposal* p) {
   return ProposalShape{p->cfg.input_dim, p->cfg.horizon, p->cfg.control_dim, p->out_pad,
                        p->cfg.log_scale_min, p->cfg.log_scale_max, p->device};
+}
+
+ProposalWeights proposal_weights(const mppi_proposal* p) {
+  ProposalWeights w{};
+  for (int l = 0; l < 4; ++l) {
+    w.w[l] = reinterpret_cast<const uint16_t*>(p->W[l]);
+    w.b[l] = p->params + p->seg[2 * l + 1];
+  }
+  w.in = kIn;
+  w.hidden = kHid;
+  w.out = p->out_pad;
+  return w;
 }
 
 cudaError_t proposal_enqueue_forward(mppi_proposal* p, cudaStream_t stream, const float* x,

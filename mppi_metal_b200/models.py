@@ -68,6 +68,37 @@ class GustModelParams(ctypes.Structure):
     _fields_ = [("dt", _f), ("noise_std", _f), ("p_event", _f), ("gust_accel", _f)]
 
 
+class WezModelParams(ctypes.Structure):
+    _fields_ = [("v_max", _f), ("dt", _f), ("adv_v_max", _f), ("adv_fire_prob_max", _f),
+                ("adv_max_range", _f), ("adv_min_range", _f), ("adv_k_gain", _f),
+                ("adv_capture_radius", _f), ("adv_max_steps", ctypes.c_int32),
+                ("num_adversaries", ctypes.c_int32)]
+
+
+class WezCostParams(ctypes.Structure):
+    _fields_ = [("x_goal", _f), ("y_goal", _f), ("goal_radius", _f), ("pos_weight", _f),
+                ("heading_weight", _f), ("control_weight", _f), ("adv_collision_weight", _f),
+                ("adv_dist_weight", _f)]
+
+
+class WezAdversary(ctypes.Structure):
+    _fields_ = [("x", _f), ("y", _f), ("theta", _f), ("v", _f),
+                ("steps_since_active", ctypes.c_uint16), ("active", ctypes.c_bool),
+                ("terminal", ctypes.c_bool)]
+
+
+WEZ_ADVERSARIES = 8
+
+
+class WezState(ctypes.Structure):
+    """The WEZ example's AgentState: 180 bytes = 45 float slots."""
+    _fields_ = [("x", _f), ("y", _f), ("theta", _f), ("v", _f), ("captured", ctypes.c_bool),
+                ("adversaries", WezAdversary * WEZ_ADVERSARIES)]
+
+
+WEZ_STATE_DIM = ctypes.sizeof(WezState) // 4  # 45
+
+
 def blob(s: ctypes.Structure) -> bytes:
     return ctypes.string_at(ctypes.addressof(s), ctypes.sizeof(s))
 
@@ -179,6 +210,55 @@ def gust_batch(seed: int = 0, N: int = 16, K: int = 1024, H: int = 30, T: int = 
     return Workload("gust_batch", "gust_integrator", "gust_integrator", 5, 2, H, K, lam,
                     sigma, sigma.copy(), np.full(2, -2.0, np.float32),
                     np.full(2, 2.0, np.float32), N, T, x0, blob(mp), [], None, seed=seed)
+
+
+def wez_state(s: WezState) -> np.ndarray:
+    """The state record as the 45 float slots the driver carries."""
+    return np.frombuffer(blob(s), np.float32).copy()
+
+
+def wez_fields(x: np.ndarray) -> WezState:
+    """The state record behind 45 float slots."""
+    return WezState.from_buffer_copy(np.ascontiguousarray(x, np.float32).tobytes())
+
+
+def wez_batch(seed: int | None = None, N: int = 256, K: int = 128, H: int = 20,
+              T: int = 100) -> Workload:
+    """The reference's WEZ example (examples/wez_environment_batch/main.cpp:
+    54-230): an ego vehicle (state x, y, theta, v, captured) driving to the
+    goal (5, 5) among 8 pursuing adversaries whose engagement zones activate
+    at random; K 128, H 20, lambda 1, sigma [2, 1], |a| <= 3, |omega| <= 1.5,
+    dt 0.05.  Every agent starts at the origin with adversary 1 at (2, 0)
+    heading pi and the others at (0, 2) heading -pi/2, all at speed 2.
+    seed=None keeps the example's identical agents; a seed places each
+    agent's start and goal and the adversaries at random (U[-6, 6]^2)."""
+    mp = WezModelParams(2.0, 0.05, 2.0, 0.1, 8.0, 3.0, 3.0, 0.5, 100, WEZ_ADVERSARIES)
+    rng = np.random.default_rng(seed) if seed is not None else None
+    x0 = np.zeros((N, WEZ_STATE_DIM), np.float32)
+    cps = []
+    for a in range(N):
+        s = WezState()
+        for i in range(WEZ_ADVERSARIES):
+            d = s.adversaries[i]
+            d.x, d.y, d.theta = (2.0, 0.0, 3.14) if i == 0 else (0.0, 2.0, -1.57)
+            d.v = 2.0
+            d.steps_since_active = 0 if i == 0 else 50
+        c = WezCostParams(5.0, 5.0, 0.2, 10.0, 0.0, 0.1, 100.0, 0.0)
+        if rng is not None:
+            s.x, s.y = (float(v) for v in rng.uniform(-6.0, 6.0, 2))
+            s.theta = float(rng.uniform(-np.pi, np.pi))
+            for i in range(WEZ_ADVERSARIES):
+                d = s.adversaries[i]
+                d.x, d.y = (float(v) for v in rng.uniform(-6.0, 6.0, 2))
+                d.theta = float(rng.uniform(-np.pi, np.pi))
+            c.x_goal, c.y_goal = (float(v) for v in rng.uniform(-6.0, 6.0, 2))
+        x0[a] = wez_state(s)
+        cps.append(blob(c))
+    sigma = np.array([2.0, 1.0], np.float32)
+    return Workload("wez_batch", "wez_environment", "wez_environment", WEZ_STATE_DIM, 2, H, K,
+                    1.0, sigma, (1.0 / sigma).astype(np.float32),
+                    np.array([-3.0, -1.5], np.float32), np.array([3.0, 1.5], np.float32), N, T,
+                    x0, blob(mp), cps, None, seed=0 if seed is None else seed)
 
 
 def double_integrator_test(K: int = 64, H: int = 10) -> Workload:

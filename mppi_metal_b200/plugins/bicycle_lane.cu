@@ -4,6 +4,9 @@
 #include "mppi_core.h"
 #include "model_params.h"
 
+// The blobs this plugin reads (checked against the driver's ParamLayout).
+MPPI_PARAM_LAYOUT_OF(BicycleModelParams, BicycleCostParams, "mppi_b200/bicycle_lane/1")
+
 __device__ void mppi_dynamics(uint8_t* state_raw, const float* control,
                               const uint8_t* model_params_raw, uint2 rng_counter,
                               uint32_t rng_seed) {

@@ -7,6 +7,11 @@
 #include "philox.h"
 #include "model_params.h"
 
+// The blob this plugin reads (no cost parameters), checked against the
+// driver's ParamLayout.
+MPPI_PARAM_LAYOUT(sizeof(GustModelParams), alignof(GustModelParams), 0, 1,
+                  "mppi_b200/gust_integrator/1")
+
 __device__ void mppi_dynamics(uint8_t* state_raw, const float* control,
                               const uint8_t* model_params_raw, uint2 rng_counter,
                               uint32_t rng_seed) {

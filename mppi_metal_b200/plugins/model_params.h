@@ -175,4 +175,34 @@ typedef struct {
   float gust_accel;
 } GustModelParams;
 
+/* ------------------------------------------------------------------------ */
+/* wez_environment: the reference's stochastic example                       */
+/* (examples/wez_environment_batch/wez_environment.metal:8-32,               */
+/* examples/wez_environment_batch/main.cpp:11-37).  Field order kept so the  */
+/* example's blobs bind unchanged.  State and formulas: wez_environment.cu.  */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  float v_max;
+  float dt;
+  float adv_v_max;
+  float adv_fire_prob_max;
+  float adv_max_range;
+  float adv_min_range;
+  float adv_k_gain;
+  float adv_capture_radius;
+  int adv_max_steps;
+  int num_adversaries;
+} WezModelParams;
+
+typedef struct {
+  float x_goal;
+  float y_goal;
+  float goal_radius;
+  float pos_weight;
+  float heading_weight;
+  float control_weight;
+  float adv_collision_weight;
+  float adv_dist_weight;
+} WezCostParams;
+
 #endif /* MPPI_B200_MODEL_PARAMS_H */

@@ -14,6 +14,9 @@
 #include "mppi_core.h"
 #include "model_params.h"
 
+// The blobs this plugin reads (checked against the driver's ParamLayout).
+MPPI_PARAM_LAYOUT_OF(UnicycleModelParams, UnicycleCostParams, "mppi_b200/unicycle_obstacles/1")
+
 __device__ void mppi_dynamics(uint8_t* state_raw, const float* control,
                               const uint8_t* model_params_raw, uint2 rng_counter,
                               uint32_t rng_seed) {
@@ -89,6 +92,62 @@ __device__ float mppi_stage_cost(const float* s, const float* control,
     pen = unicycle_penetration<MPPI_UNICYCLE_MAX_OBS, true>(s, c);
   return unicycle_goal(s, c) + c->w_obs * pen;
 }
+
+// Part `part` of 4 of the stage cost, for the library's cooperative rollout
+// (MPPI_STAGE_COST_SPLIT): the obstacle pairs [part * PP, (part + 1) * PP)
+// with PP = num_obs / 8 pairs (1 for 8 obstacles, 2 for 16), and the goal
+// term in part 0.  The four parts sum to mppi_stage_cost up to rounding.
+template <int PP, bool MASK>
+__device__ __forceinline__ float unicycle_penetration_part(const float* s,
+                                                           const UnicycleCostParams* c,
+                                                           int part) {
+  const float t = s[3];
+  const unsigned n = c->num_obs;
+  const float2 tt = make_float2(t, t);
+  const float2 nx = make_float2(-s[0], -s[0]), ny = make_float2(-s[1], -s[1]);
+  const float2* cx2 = reinterpret_cast<const float2*>(c->obs_cx) + part * PP;
+  const float2* cy2 = reinterpret_cast<const float2*>(c->obs_cy) + part * PP;
+  const float2* vx2 = reinterpret_cast<const float2*>(c->obs_vx) + part * PP;
+  const float2* vy2 = reinterpret_cast<const float2*>(c->obs_vy) + part * PP;
+  const float2* r2 = reinterpret_cast<const float2*>(c->obs_r) + part * PP;
+  float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+  for (int j = 0; j < PP; ++j) {
+    const float2 ex = __fadd2_rn(__ffma2_rn(vx2[j], tt, cx2[j]), nx);
+    const float2 ey = __fadd2_rn(__ffma2_rn(vy2[j], tt, cy2[j]), ny);
+    const float2 d2 = __ffma2_rn(ex, ex, __fmul2_rn(ey, ey));
+    float2 r = r2[j];
+    if (MASK) {
+      const unsigned i0 = (unsigned)(2 * (part * PP + j));
+      r.x = i0 < n ? r.x : 0.0f;
+      r.y = i0 + 1u < n ? r.y : 0.0f;
+    }
+    const float2 m = make_float2(fminf(mppi_sqrt_approx(d2.x), r.x),
+                                 fminf(mppi_sqrt_approx(d2.y), r.y));
+    acc = __fadd2_rn(acc, __fadd2_rn(r, make_float2(-m.x, -m.y)));
+  }
+  return acc.x + acc.y;
+}
+
+__device__ float mppi_stage_cost_part(const float* s, const float* control,
+                                      const uint8_t* model_params_raw,
+                                      const uint8_t* cost_params_raw, int part) {
+  const UnicycleCostParams* c = reinterpret_cast<const UnicycleCostParams*>(cost_params_raw);
+  const unsigned n = c->num_obs;
+  float pen;
+  if (n == MPPI_UNICYCLE_MAX_OBS)
+    pen = unicycle_penetration_part<MPPI_UNICYCLE_MAX_OBS / 8, false>(s, c, part);
+  else if (n == 8)
+    pen = unicycle_penetration_part<1, false>(s, c, part);
+  else if (n < 8)
+    pen = unicycle_penetration_part<1, true>(s, c, part);
+  else
+    pen = unicycle_penetration_part<MPPI_UNICYCLE_MAX_OBS / 8, true>(s, c, part);
+  const float goal = part == 0 ? unicycle_goal(s, c) : 0.0f;
+  return fmaf(c->w_obs, pen, goal);
+}
+
+MPPI_STAGE_COST_SPLIT(mppi_stage_cost, mppi_stage_cost_part, 4)
 
 __device__ float mppi_terminal_cost(const float* s, const uint8_t* model_params_raw,
                                     const uint8_t* cost_params_raw) {

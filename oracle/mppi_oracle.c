@@ -216,12 +216,117 @@ static void dyn_gust(double* s, const double* u, const GustModelParams* mp, uint
   s[1] += s[3] * dt;
 }
 
+/* wez_environment (plugins/wez_environment.cu), following the reference's
+ * examples/wez_environment_batch/wez_environment.metal:84-184 (dynamics) and
+ * :186-240 (costs), with the adversaries read where the state holds them
+ * (the reference's cost view starts them 4 bytes early, :59 vs :74).
+ * State slots (the example's AgentState as floats): [0, 4) ego x, y, theta,
+ * v; [4] a packed word (byte 0: captured); adversary i at 5 + 5 i: x, y,
+ * theta, v and a packed word (bytes 0-1 steps_since_active, byte 2 active,
+ * byte 3 terminal).  A packed word travels as the float with its bits; a
+ * float converts to double and back exactly, so the bits survive.  The
+ * activation draw compares the bit-exact float uniform. */
+static uint32_t wez_bits(double v) {
+  const float f = (float)v;
+  uint32_t b;
+  memcpy(&b, &f, 4);
+  return b;
+}
+static double wez_from_bits(uint32_t b) {
+  float f;
+  memcpy(&f, &b, 4);
+  return (double)f;
+}
+static double wez_wrap(double x) {
+  const double pi = (double)3.1415926535f;
+  double e = fmod(x + pi, 2.0 * pi);
+  if (e < 0.0) e += 2.0 * pi;
+  return e - pi;
+}
+static int wez_count(const oracle_problem* p, const WezModelParams* mp) {
+  const int cap = ((int)p->state_dim * 4 - 20) / 20;
+  return mp->num_adversaries < cap ? mp->num_adversaries : cap;
+}
+
+static void dyn_wez(const oracle_problem* p, double* s, const double* u,
+                    const WezModelParams* mp, uint32_t ctr0, uint32_t ctr1, uint32_t key) {
+  const double dt = mp->dt;
+  const double th = s[2], v = s[3];
+  s[0] += v * cos(th) * dt;
+  s[1] += v * sin(th) * dt;
+  s[2] += u[1] * dt;
+  s[3] += u[0] * dt;
+  uint32_t ego = wez_bits(s[4]);
+  const int n = wez_count(p, mp);
+  for (int i = 0; i < n; ++i) {
+    double* a = s + 5 + 5 * i;
+    uint32_t w = wez_bits(a[4]);
+    uint32_t steps = w & 0xffffu;
+    int active = (w >> 16) & 0xffu, terminal = (w >> 24) & 0xffu;
+    const double dx = s[0] - a[0], dy = s[1] - a[1];
+    if (active) {
+      const double target = atan2(dy, dx);
+      const double rc = mp->adv_capture_radius;
+      if (dx * dx + dy * dy < rc * rc) ego = (ego & ~0xffu) | 1u;
+      const double omega = mp->adv_k_gain * wez_wrap(target - a[2]);
+      a[0] += a[3] * cos(a[2]) * dt;
+      a[1] += a[3] * sin(a[2]) * dt;
+      a[2] += omega * dt;
+      steps = (steps + 1u) & 0xffffu;
+      if ((int)steps > mp->adv_max_steps) {
+        active = 0;
+        terminal = 1;
+      }
+    } else if (!terminal) {
+      const double dist = sqrt(dx * dx + dy * dy);
+      if (dist < mp->adv_max_range) {
+        double prob = mp->adv_fire_prob_max;
+        if (dist > mp->adv_min_range) {
+          const double span = (double)mp->adv_max_range - mp->adv_min_range;
+          prob = span > (double)1e-6f ? prob * (mp->adv_max_range - dist) / span : 0.0;
+        }
+        uint32_t r[2];
+        oracle_philox2x32_10(ctr0, ctr1 + 0x1000u + (uint32_t)i, key, r);
+        if ((double)oracle_uint_to_01(r[0]) < prob) {
+          active = 1;
+          steps = 0;
+        }
+      }
+    }
+    a[4] = wez_from_bits(steps | ((uint32_t)active << 16) | ((uint32_t)terminal << 24));
+  }
+  s[4] = wez_from_bits(ego);
+  s[2] = wez_wrap(s[2]);
+  if (s[3] > mp->v_max) s[3] = mp->v_max;
+  if (s[3] < -mp->v_max) s[3] = -mp->v_max;
+}
+
+static double wez_stage_cost(const oracle_problem* p, const double* s, const double* u,
+                             const WezModelParams* mp, const WezCostParams* cp) {
+  const double gx = s[0] - cp->x_goal, gy = s[1] - cp->y_goal;
+  double c = cp->pos_weight * (gx * gx + gy * gy) +
+             cp->control_weight * (u[0] * u[0] + u[1] * u[1]);
+  const double r2 = (double)mp->adv_capture_radius * mp->adv_capture_radius + (double)1e-6f;
+  const int n = wez_count(p, mp);
+  for (int i = 0; i < n; ++i) {
+    const double* a = s + 5 + 5 * i;
+    if ((wez_bits(a[4]) >> 16) & 0xffu) {
+      const double dx = s[0] - a[0], dy = s[1] - a[1];
+      c += cp->adv_collision_weight * exp(-(dx * dx + dy * dy) / r2);
+    }
+  }
+  return c;
+}
+
 void oracle_dynamics(const oracle_problem* p, double* x, const double* u,
                      const void* model_params, uint32_t ctr0, uint32_t ctr1,
                      uint32_t key) {
   switch (p->model) {
     case ORACLE_MODEL_GUST:
       dyn_gust(x, u, (const GustModelParams*)model_params, ctr0, ctr1, key);
+      break;
+    case ORACLE_MODEL_WEZ:
+      dyn_wez(p, x, u, (const WezModelParams*)model_params, ctr0, ctr1, key);
       break;
     case ORACLE_MODEL_DOUBLE_INTEGRATOR: dyn_double_integrator(x, u); break;
     case ORACLE_MODEL_NONHOLONOMIC:
@@ -315,6 +420,9 @@ double oracle_stage_cost(const oracle_problem* p, const double* x, const double*
       return quad_state_cost(x, (const QuadrotorCostParams*)cost_params, 0);
     case ORACLE_MODEL_GUST: /* plugins/gust_integrator.cu */
       return x[0] * x[0] + x[1] * x[1] + (double)0.1f * (x[2] * x[2] + x[3] * x[3]);
+    case ORACLE_MODEL_WEZ:
+      return wez_stage_cost(p, x, u, (const WezModelParams*)model_params,
+                            (const WezCostParams*)cost_params);
     default: return 0.0;
   }
 }
@@ -341,6 +449,11 @@ double oracle_terminal_cost(const oracle_problem* p, const double* x,
       return quad_state_cost(x, (const QuadrotorCostParams*)cost_params, 1);
     case ORACLE_MODEL_GUST:
       return 10.0 * (x[0] * x[0] + x[1] * x[1]);
+    case ORACLE_MODEL_WEZ: { /* wez_environment.metal:222-240 */
+      const WezCostParams* cp = (const WezCostParams*)cost_params;
+      const double gx = x[0] - cp->x_goal, gy = x[1] - cp->y_goal;
+      return cp->pos_weight * (gx * gx + gy * gy) * 10.0;
+    }
     default: return 0.0;
   }
 }

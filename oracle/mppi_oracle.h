@@ -43,6 +43,7 @@ enum {
   ORACLE_MODEL_BICYCLE_LANE = 3,
   ORACLE_MODEL_QUADROTOR = 4,
   ORACLE_MODEL_GUST = 5,
+  ORACLE_MODEL_WEZ = 6,
 };
 
 typedef struct {

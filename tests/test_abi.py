@@ -6,6 +6,7 @@ from __future__ import annotations
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 from mppi_metal_b200 import _lib
@@ -61,6 +62,7 @@ PLUGINS = [
     ("gust_integrator", 5, 2, 16, 0),
     ("bicycle_lane", 5, 2, 16, 544),
     ("quadrotor", 12, 4, 32, 560),
+    ("wez_environment", 45, 2, 40, 32),  # 180-byte state: beyond the reference's 128
 ]
 
 
@@ -138,3 +140,63 @@ def test_queries_before_initialize_report_not_init(lib):
         assert lib.mppi_backend_step_form(None, ctypes.byref(form)) == _lib.MPPI_ERR_NOT_INIT
     finally:
         lib.mppi_backend_destroy(h)
+
+
+# ---- ParamLayout against a plugin's declared layout (MPPI_PARAM_LAYOUT) ----
+# The reference declares ParamLayout::schema_hash and alignments
+# (include/mppi_metal/mppi_types.hpp:88-94) and its README promises that
+# initialize fails when the declared layout does not match the binding; the
+# shipped plugins declare theirs, and the module compile checks them.
+
+def _layout_check(**kw):
+    base = dict(model_params_size=16, cost_params_size=352)
+    base.update(kw)
+    return compile_check("unicycle_obstacles", 4, 2, **base)
+
+
+def test_declared_layout_accepts_matching_param_layout():
+    for kw in ({}, dict(model_params_alignment=4, cost_params_alignment=16),
+               dict(schema_hash="mppi_b200/unicycle_obstacles/1")):
+        rc, err, _ = _layout_check(**kw)
+        assert rc == 0, (kw, err)
+
+
+@pytest.mark.parametrize("kw,field", [
+    (dict(model_params_size=20), "ParamLayout::model_params_size"),
+    (dict(cost_params_size=348), "ParamLayout::cost_params_size"),
+    (dict(model_params_alignment=2), "ParamLayout::model_params_alignment"),
+    (dict(cost_params_alignment=2), "ParamLayout::cost_params_alignment"),
+    (dict(schema_hash="mppi_b200/unicycle_obstacles/2"), "ParamLayout::schema_hash"),
+])
+def test_declared_layout_mismatch_is_named(kw, field):
+    rc, err, _ = _layout_check(**kw)
+    assert rc == _lib.MPPI_ERR_INVALID, err
+    assert field in err and "does not match" in err, err
+
+
+def test_schema_hash_characters_are_checked():
+    rc, err, _ = _layout_check(schema_hash='bad"quote')
+    assert rc == _lib.MPPI_ERR_INVALID
+    assert "schema_hash" in err
+
+
+def test_undeclared_plugin_keeps_reference_binding():
+    # the reference's own test plugin declares no layout: any sizes, any
+    # schema string compile (the reference checks sizes against blobs only)
+    rc, err, _ = compile_check("double_integrator", 4, 2, model_params_size=16,
+                               cost_params_size=8, schema_hash="anything")
+    assert rc == 0, err
+
+
+def test_state_limit_is_named():
+    # the state buffer is sized per module up to MPPI_MAX_STATE_DIM floats;
+    # beyond it initialize fails naming state_dim (validation, no GPU)
+    from mppi_metal_b200 import driver as D
+    s = np.ones(2, np.float32)
+    cfg = D.DriverConfig(state_dim=129, control_dim=2, horizon=10, sample_count=64,
+                         noise=D.ControlNoiseConfig(D.CovarianceForm.kDiagonal, s, s, 2),
+                         bounds=D.ControlBounds(-s, s, 2))
+    drv = D.MPPIDriver(cfg)
+    err = D.ErrorRef()
+    assert not drv.initialize(D.ModelPluginSpec(_lib.plugin_path("double_integrator")), err)
+    assert "state_dim" in err.value and "128 floats" in err.value, err.value

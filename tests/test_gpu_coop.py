@@ -1,0 +1,143 @@
+"""The cooperative rollout form (plugins that split their stage cost with
+MPPI_STAGE_COST_SPLIT; the unicycle splits its obstacle terms in 4 parts).
+
+For launches whose one-thread-per-sample form would have at most two CTAs
+per SM -- latency-bound: each sample's serial chain sets the time -- four
+lanes share a sample: they step the same dynamics on the same staged noise
+and each accumulates one part of the stage cost; the parts are summed at the
+end.  Checked here:
+  * the rule picks it for the single-agent configuration and not for the
+    batched one;
+  * against the FP64 oracle: costs 1e-5 relative, u_next 1e-4, weights 1e-5;
+  * against the one-thread-per-sample form (MPPI_B200_COOP=0): the same
+    values up to the order of the cost sums (1e-6 relative on costs);
+  * its fused and separate combines give the same bits, and the closed loop
+    is reproducible;
+  * with a learned proposal attached (the proposal workload's shape).
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from helpers import abs_err, backend_for, oracle_problem, rel_err
+from mppi_metal_b200 import models
+
+pytestmark = pytest.mark.gpu
+
+
+def _env(pairs, fn):
+    old = {k: os.environ.get(k) for k in pairs}
+    os.environ.update(pairs)
+    try:
+        return fn()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
+
+
+def _step(w, x0, u_nom, step=3):
+    b = backend_for(w)
+    u, d = b.dispatch_rollout(step, x0, u_nom)
+    out = (u, d, b.last_costs()[0], b.last_weights()[0], b.launch_info()["form"])
+    b.close()
+    return out
+
+
+def test_rule_picks_cooperative_form_by_launch_shape():
+    w = models.unicycle_single(seed=0, K=1024, H=30)
+    assert _step(w, w.x0[0], np.zeros(60, np.float32))[4]["cooperative"]
+    wb = models.unicycle_batch(seed=1, N=256, K=4096, H=50, T=1)
+    b = backend_for(wb)
+    b.prepare(wb.num_agents, 1, wb.x0, cost_params=wb.cost_params_packed,
+              cost_stride=wb.cost_stride, sigma=wb.agent_sigma)
+    b.run(0)
+    assert not b.launch_info()["form"]["cooperative"]
+
+
+@pytest.mark.parametrize("K,H", [(1024, 30), (777, 17)])
+def test_cooperative_step_matches_oracle(oracle, K, H):
+    w = models.unicycle_single(seed=4, K=K, H=H)
+    x0 = np.array([1.5, -0.5, 0.4, 0.0], np.float32)
+    u_nom = (np.random.default_rng(K).normal(size=H * 2) * 0.3).astype(np.float32)
+    u, d, costs, wts, form = _step(w, x0, u_nom)
+    assert form["cooperative"]
+    o = oracle.step(oracle_problem(w), 3, w.seed, x0, u_nom)
+    assert rel_err(costs, o["costs"]) <= 1e-5
+    assert abs_err(u, o["u_out"]) <= 1e-4
+    assert abs_err(wts, o["weights"]) <= 1e-5
+    assert rel_err([d[2]], [o["diag"][2]]) <= 1e-5
+
+
+def test_cooperative_matches_one_thread_per_sample():
+    w = models.unicycle_single(seed=6, K=2048, H=30)
+    x0 = np.array([-3.0, 2.0, -0.7, 0.0], np.float32)
+    u_nom = np.linspace(-0.4, 0.4, 60).astype(np.float32)
+    uc, dc, cc, _, fc = _step(w, x0, u_nom)
+    up, dp, cp, _, fp = _env({"MPPI_B200_COOP": "0"}, lambda: _step(w, x0, u_nom))
+    assert fc["cooperative"] and not fp["cooperative"]
+    assert rel_err(cc, cp) <= 1e-6
+    assert abs_err(uc, up) <= 1e-5
+
+
+def _loop(w):
+    b = backend_for(w)
+    r = b.simulate_batch(w.num_agents, w.num_steps, 0, w.x0, cost_params=w.cost_params_packed,
+                         cost_stride=w.cost_stride, sigma=w.agent_sigma)
+    f = b.launch_info()["form"]
+    b.close()
+    return r, f
+
+
+def test_cooperative_fused_and_separate_combine_same_bits():
+    w = models.unicycle_batch(seed=31, N=8, K=1000, H=24, T=10)
+    fused, ff = _env({"MPPI_B200_FUSED_COMBINE": "1"}, lambda: _loop(w))
+    sep, fs = _env({"MPPI_B200_SEPARATE_COMBINE": "1"}, lambda: _loop(w))
+    assert ff["cooperative"] and fs["cooperative"]
+    assert ff["fused_combine"] and not fs["fused_combine"]
+    for k in fused:
+        assert np.array_equal(fused[k], sep[k]), k
+    again, _ = _loop(w)
+    for k in fused:
+        assert np.array_equal(fused[k], again[k]), k
+
+
+def test_cooperative_closed_loop_matches_oracle(oracle):
+    w = models.unicycle_batch(seed=32, N=6, K=1024, H=30, T=6)
+    r, f = _loop(w)
+    assert f["cooperative"]
+    o = oracle.simulate_batch(oracle_problem(w), w.num_agents, w.num_steps, 0, w.seed, w.x0,
+                              cost_params_packed=w.cost_params_packed, cost_stride=w.cost_stride,
+                              sigma_packed=w.agent_sigma.astype(float))
+    assert abs_err(r["controls"], o["controls"]) <= 1e-4
+    assert abs_err(r["states"], o["states"]) <= 1e-4
+
+
+def test_cooperative_with_proposal_matches_one_thread_per_sample():
+    pytest.importorskip("torch")
+    from mppi_metal_b200.proposal import ProposalNet
+    w = models.unicycle_batch(seed=33, N=12, K=256, H=64, T=4)
+    net = ProposalNet(31, 64, 2, max_batch=256, seed=9)
+
+    def run():
+        b = backend_for(w, bind=False)
+        b.set_features("mppi_proposal_features", 31)
+        b.set_proposal(net, 128)
+        b.prepare(w.num_agents, w.num_steps, w.x0, cost_params=w.cost_params_packed,
+                  cost_stride=w.cost_stride, model_params=w.model_params, sigma=w.agent_sigma)
+        b.run(0)
+        r, f = b.fetch(), b.launch_info()["form"]
+        b.set_proposal(None)
+        b.close()
+        return r, f
+
+    rc, fc = run()
+    rp, fp = _env({"MPPI_B200_COOP": "0"}, run)
+    assert fc["cooperative"] and not fp["cooperative"]
+    assert abs_err(rc["controls"], rp["controls"]) <= 1e-4
+    assert abs_err(rc["states"], rp["states"]) <= 1e-4

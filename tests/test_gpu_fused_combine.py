@@ -8,7 +8,10 @@ of warps draws the noise ahead), with either combine.  The backend picks the
 form per launch shape by timing; MPPI_B200_FUSED_COMBINE=1 /
 MPPI_B200_SEPARATE_COMBINE=1 and MPPI_B200_WS=1 / 0 (read when a backend is
 created) pin it here.  Programmatic dependent launch, on by default, is
-checked against plain launches (MPPI_B200_NO_PDL=1) the same way."""
+checked against plain launches (MPPI_B200_NO_PDL=1) the same way.
+These tests compare the forms with one thread per sample; the cooperative
+form, which the backend picks by launch shape for plugins with a split stage
+cost, is pinned off here (MPPI_B200_COOP=0) and tested in test_gpu_coop.py."""
 from __future__ import annotations
 
 import os
@@ -20,6 +23,11 @@ from helpers import backend_for, nonholonomic_example
 from mppi_metal_b200 import models
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _one_thread_per_sample(monkeypatch):
+    monkeypatch.setenv("MPPI_B200_COOP", "0")
 
 
 def _with_env(name, fn, value="1"):
@@ -203,9 +211,10 @@ def test_step_form_reported():
         b.close()
         return info["form"]
 
-    assert _ws(lambda: _fused(run)) == {"fused_combine": True, "warp_specialised": True}
+    assert _ws(lambda: _fused(run)) == {"fused_combine": True, "warp_specialised": True,
+                                        "cooperative": False}
     assert _with_env("MPPI_B200_WS", lambda: _separate(run), value="0") == \
-        {"fused_combine": False, "warp_specialised": False}
+        {"fused_combine": False, "warp_specialised": False, "cooperative": False}
 
 
 def _quad_mixed():
@@ -244,10 +253,11 @@ def test_every_step_form_same_bits_per_plugin(name):
         return r, form
 
     base, f0 = _with_env("MPPI_B200_WS", lambda: _separate(run), value="0")
-    assert f0 == {"fused_combine": False, "warp_specialised": False}
+    assert f0 == {"fused_combine": False, "warp_specialised": False, "cooperative": False}
     for ws, pin in ((False, _fused), (True, _separate), (True, _fused)):
         r, f = _with_env("MPPI_B200_WS", lambda: pin(run), value="1" if ws else "0")
-        assert f == {"fused_combine": pin is _fused, "warp_specialised": ws}
+        assert f == {"fused_combine": pin is _fused, "warp_specialised": ws,
+                     "cooperative": False}
         _assert_same(r, base)
 
 
@@ -274,8 +284,9 @@ def test_every_step_form_same_bits_quadrotor_proposal():
         return r, form
 
     base, f0 = _with_env("MPPI_B200_WS", lambda: _separate(run), value="0")
-    assert f0 == {"fused_combine": False, "warp_specialised": False}
+    assert f0 == {"fused_combine": False, "warp_specialised": False, "cooperative": False}
     for ws, pin in ((False, _fused), (True, _separate), (True, _fused)):
         r, f = _with_env("MPPI_B200_WS", lambda: pin(run), value="1" if ws else "0")
-        assert f == {"fused_combine": pin is _fused, "warp_specialised": ws}
+        assert f == {"fused_combine": pin is _fused, "warp_specialised": ws,
+                     "cooperative": False}
         _assert_same(r, base)

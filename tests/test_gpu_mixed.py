@@ -97,3 +97,28 @@ def test_quadrotor_fp32_matches_oracle(oracle):
     o = oracle.step(p, 2, w.seed, w.x0[0], un)
     r = np.abs(costs - o["costs"]) / np.abs(o["costs"])
     assert np.quantile(r, 0.99) < 1e-5
+
+
+@pytest.mark.parametrize("seed", [3, 8])
+def test_quadrotor_fp32_well_conditioned_every_sample(oracle, seed):
+    """FP32 quadrotor pinned by its maximum: a well-conditioned case (hover
+    nominal, sigma 0.1, H 30, lambda 1 as configured) where no sample
+    tumbles.  End to end against the oracle on the same seed: every
+    sample's cost to 1e-5 relative, u_next to 1e-4, weights to 1e-5 and ESS
+    to 1e-5 relative, for two warm-started steps."""
+    w = quad(0, K=2048, H=30, seed=seed)
+    assert w.lam == 1.0
+    w.sigma = np.full(4, 0.1, np.float32)
+    w.sigma_inv = (1.0 / w.sigma ** 2).astype(np.float32)
+    b = backend_for(w)
+    p = oracle_problem(w)
+    hover = float(w.u_max[0]) / 2.0
+    un = np.full(w.horizon * 4, hover, np.float32)
+    for step in (0, 1):
+        u_out, diag = b.dispatch_rollout(step, w.x0[0], un)
+        o = oracle.step(p, step, w.seed, w.x0[0], un)
+        assert rel_err(b.last_costs()[0], o["costs"]) <= 1e-5
+        assert abs_err(u_out, o["u_out"]) <= 1e-4
+        assert abs_err(b.last_weights()[0], o["weights"]) <= 1e-5
+        assert rel_err([diag[2]], [o["diag"][2]]) <= 1e-5
+        un = np.concatenate([u_out[4:], u_out[-4:]]).astype(np.float32)

@@ -133,3 +133,76 @@ def test_training_reduces_the_loss():
     out = net.forward(xd[:512]).cpu().numpy()
     mse = float(np.mean((out[:, :s.hm] - y[:512]) ** 2))
     assert mse < 0.25 * float(np.mean(y[:512] ** 2)), mse
+
+
+# ---- the per-agent form (CUDA cores, inside the MPPI module) ---------------
+# Batches of at most 512 agents evaluate the network per agent: the first
+# step's kernel and every combine run it for their agent's next state, with
+# the same BF16 roundings as the tensor-core kernels and FP32 sums in a fixed
+# order; the tolerance is the tensor-core kernels'.
+
+def _proposal_backend(w, net, samples=128):
+    from helpers import backend_for
+    b = backend_for(w, bind=False)
+    b.set_features("mppi_proposal_features", 31)
+    b.set_proposal(net, samples)
+    b.prepare(w.num_agents, w.num_steps, w.x0, cost_params=w.cost_params_packed,
+              cost_stride=w.cost_stride, model_params=w.model_params, sigma=w.agent_sigma)
+    return b
+
+
+def _with_env(name, value, fn):
+    import os
+    old = os.environ.get(name)
+    os.environ[name] = value
+    try:
+        return fn()
+    finally:
+        if old is None:
+            del os.environ[name]
+        else:
+            os.environ[name] = old
+
+
+def test_per_agent_forward_matches_tensor_core_and_oracle():
+    from mppi_metal_b200 import models
+    s = mo.Shape(31, 64, 2)
+    net = _net(s, 2, max_batch=128)
+    p = mo.init_params(s, 13)
+    net.set_params(p)
+    w = models.unicycle_batch(seed=40, N=24, K=256, H=64, T=2)
+    feat, out, per_agent = _proposal_backend(w, net).proposal_stage()
+    assert per_agent
+    ref = mo.forward(s, p.astype(np.float64), feat[:, :31])
+    tc = net.forward(torch.from_numpy(np.ascontiguousarray(feat[:, :31])).cuda()).cpu().numpy()
+    tol = 2e-3 * np.abs(ref).max() + 1e-4
+    assert np.abs(out[:, :s.out_dim] - ref[:, :s.out_dim]).max() <= tol
+    assert np.abs(out[:, :s.out_dim] - tc[:, :s.out_dim]).max() <= tol
+    # the tensor-core form of the same stage (pinned): the same features
+    feat2, out2, pa2 = _with_env("MPPI_B200_NET_PER_AGENT", "0",
+                                 lambda: _proposal_backend(w, net).proposal_stage())
+    assert not pa2
+    assert np.array_equal(feat, feat2)
+    assert np.abs(out2[:, :s.out_dim] - out[:, :s.out_dim]).max() <= tol
+
+
+def test_per_agent_network_closed_loop_matches_tensor_core_form():
+    from mppi_metal_b200 import models
+    s = mo.Shape(31, 64, 2)
+    net = _net(s, 3, max_batch=128)
+    net.set_params(mo.init_params(s, 14))
+    w = models.unicycle_batch(seed=41, N=12, K=256, H=64, T=4)
+
+    def run():
+        b = _proposal_backend(w, net)
+        b.run(0)
+        r, kps = b.fetch(), b.launch_info()["kernels_per_step"]
+        b.set_proposal(None)
+        b.close()
+        return r, kps
+
+    per_agent, k1 = run()
+    tensor_core, k2 = _with_env("MPPI_B200_NET_PER_AGENT", "0", run)
+    assert k2 == k1 + 1  # the tensor-core form launches the network every step
+    assert np.abs(per_agent["controls"] - tensor_core["controls"]).max() <= 1e-3
+    assert np.abs(per_agent["states"] - tensor_core["states"]).max() <= 1e-3
