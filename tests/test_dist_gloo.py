@@ -10,6 +10,7 @@ import sys
 from pathlib import Path
 
 import numpy as np
+import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 
@@ -78,3 +79,64 @@ def test_reference_arm_runs_on_rank_zero_only(tmp_path):
                         "--steps", "1", "--warmup", "0"], capture_output=True, text=True,
                        env=env, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def _library_worker(rank: int, world: int, port: int, q) -> None:
+    """A rank of the weak-scaling path on the library: its own agents (seed
+    per rank), one batch closed loop on cuda:0, gloo for the barrier and the
+    max over ranks only."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "tests"))
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from mppi_metal_b200 import dist, models
+    from helpers import backend_for
+    R = dist.env()
+    dist.init(R, "gloo", timeout_s=120)
+    w = models.unicycle_batch(seed=dist.agent_seed(500, R), N=4, K=512, H=16, T=3)
+    b = backend_for(w)
+    b.prepare(w.num_agents, w.num_steps, w.x0, cost_params=w.cost_params_packed,
+              cost_stride=w.cost_stride, sigma=w.agent_sigma)
+    dist.barrier(R)
+    b.run(0)
+    ms = b.last_run_ms()
+    r = b.fetch()
+    dist.barrier(R)
+    q.put({"rank": R.rank, "controls": r["controls"].tolist(), "ms": ms,
+           "max_ms": dist.max_over_ranks(R, ms)})
+    dist.barrier(R)
+    b.close()
+    dist.finish(R)
+
+
+@pytest.mark.gpu
+def test_two_ranks_run_the_library_on_their_own_agents():
+    # both ranks share this run's one GPU: their kernels are independent
+    # replicas (no rank waits on another's kernel); the host-side gloo group
+    # carries only the barrier and the max of the device times
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_library_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in procs:
+        d = q.get(timeout=600)
+        out[d["rank"]] = d
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert out[0]["max_ms"] == out[1]["max_ms"] == max(out[0]["ms"], out[1]["ms"])
+    # each rank's results are the single-process results of the same agents
+    sys.path.insert(0, str(ROOT / "tests"))
+    from helpers import backend_for
+    from mppi_metal_b200 import models
+    for rank in (0, 1):
+        w = models.unicycle_batch(seed=500 + rank, N=4, K=512, H=16, T=3)
+        r = backend_for(w).simulate_batch(w.num_agents, w.num_steps, 0, w.x0,
+                                          cost_params=w.cost_params_packed,
+                                          cost_stride=w.cost_stride, sigma=w.agent_sigma)
+        assert np.array_equal(np.asarray(out[rank]["controls"], np.float32), r["controls"])
+    assert out[0]["controls"] != out[1]["controls"]
