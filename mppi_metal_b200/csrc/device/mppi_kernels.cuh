@@ -748,30 +748,63 @@ __device__ __noinline__ void network_row(const float* f, const MppiNetRows& net,
     const float* hin = h_s[(l + 1) & 1];
     float* hout = h_s[l & 1];
     const uint4* W = reinterpret_cast<const uint4*>(net.w[l]);
-    for (uint32_t n = tid; n < N; n += nt) {
+    // two outputs per pass (n and n + nt), their weight loads issued in
+    // batches of 8 k-blocks each, so 16 loads are in flight per thread
+    for (uint32_t n0 = tid; n0 < N; n0 += 2 * nt) {
+      const uint32_t n1 = n0 + nt;
+      const bool two = n1 < N;
       // row n, k-block b (8 inputs) at element (n / 8) 8K + 64 b + (n % 8) 8
-      const uint4* wr = W + (size_t)(n >> 3) * K + (n & 7u);
-      float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll 4
-      for (uint32_t b = 0; b < K / 8; ++b) {
-        const uint4 w8 = __ldg(wr + 8 * b);
-        const float4 h0 = *reinterpret_cast<const float4*>(hin + 8 * b);
-        const float4 h1 = *reinterpret_cast<const float4*>(hin + 8 * b + 4);
-        float& s = acc[b & 3u];
-        s = fmaf(bf16_lo(w8.x), h0.x, s);
-        s = fmaf(bf16_hi(w8.x), h0.y, s);
-        s = fmaf(bf16_lo(w8.y), h0.z, s);
-        s = fmaf(bf16_hi(w8.y), h0.w, s);
-        s = fmaf(bf16_lo(w8.z), h1.x, s);
-        s = fmaf(bf16_hi(w8.z), h1.y, s);
-        s = fmaf(bf16_lo(w8.w), h1.z, s);
-        s = fmaf(bf16_hi(w8.w), h1.w, s);
+      const uint4* wr0 = W + (size_t)(n0 >> 3) * K + (n0 & 7u);
+      const uint4* wr1 = W + (size_t)(n1 >> 3) * K + (n1 & 7u);
+      float acc0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, acc1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      const uint32_t nb = K / 8;
+      for (uint32_t b0 = 0; b0 < nb; b0 += 8) {
+        uint4 w0[8], w1[8];
+#pragma unroll
+        for (uint32_t i = 0; i < 8; ++i) {
+          const bool in = b0 + i < nb;
+          w0[i] = in ? __ldg(wr0 + 8 * (b0 + i)) : make_uint4(0u, 0u, 0u, 0u);
+          w1[i] = (in && two) ? __ldg(wr1 + 8 * (b0 + i)) : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < 8; ++i) {
+          const uint32_t b = b0 + i;
+          if (b < nb) {
+            const float4 h0 = *reinterpret_cast<const float4*>(hin + 8 * b);
+            const float4 h1 = *reinterpret_cast<const float4*>(hin + 8 * b + 4);
+            float& s0 = acc0[b & 3u];
+            float& s1 = acc1[b & 3u];
+            s0 = fmaf(bf16_lo(w0[i].x), h0.x, s0);
+            s1 = fmaf(bf16_lo(w1[i].x), h0.x, s1);
+            s0 = fmaf(bf16_hi(w0[i].x), h0.y, s0);
+            s1 = fmaf(bf16_hi(w1[i].x), h0.y, s1);
+            s0 = fmaf(bf16_lo(w0[i].y), h0.z, s0);
+            s1 = fmaf(bf16_lo(w1[i].y), h0.z, s1);
+            s0 = fmaf(bf16_hi(w0[i].y), h0.w, s0);
+            s1 = fmaf(bf16_hi(w1[i].y), h0.w, s1);
+            s0 = fmaf(bf16_lo(w0[i].z), h1.x, s0);
+            s1 = fmaf(bf16_lo(w1[i].z), h1.x, s1);
+            s0 = fmaf(bf16_hi(w0[i].z), h1.y, s0);
+            s1 = fmaf(bf16_hi(w1[i].z), h1.y, s1);
+            s0 = fmaf(bf16_lo(w0[i].w), h1.z, s0);
+            s1 = fmaf(bf16_lo(w1[i].w), h1.z, s1);
+            s0 = fmaf(bf16_hi(w0[i].w), h1.w, s0);
+            s1 = fmaf(bf16_hi(w1[i].w), h1.w, s1);
+          }
+        }
       }
-      const float z = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + net.b[l][n];
+      const float z0 = ((acc0[0] + acc0[1]) + (acc0[2] + acc0[3])) + net.b[l][n0];
       if (l < 3)
-        hout[n] = mppi_round_bf16(mppi_gelu(z));
+        hout[n0] = mppi_round_bf16(mppi_gelu(z0));
       else
-        out[n] = z;
+        out[n0] = z0;
+      if (two) {
+        const float z1 = ((acc1[0] + acc1[1]) + (acc1[2] + acc1[3])) + net.b[l][n1];
+        if (l < 3)
+          hout[n1] = mppi_round_bf16(mppi_gelu(z1));
+        else
+          out[n1] = z1;
+      }
     }
     __syncthreads();
   }

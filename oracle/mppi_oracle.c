@@ -10,7 +10,7 @@
 
 #include "../mppi_metal_b200/plugins/model_params.h"
 
-#define MAX_STATE 32
+#define MAX_STATE 128 /* the library's state limit (MPPI_MAX_STATE_DIM floats) */
 #define ORACLE_PI 3.14159265358979323846
 #define MAX_CTRL 16
 

@@ -129,3 +129,23 @@ def test_full_covariance_noise_has_requested_covariance(oracle):
     _, e = oracle.noise(p, 0, 5, 0)
     emp = np.cov(e.T)
     assert np.max(np.abs(emp - cov)) < 0.03
+
+
+def test_wez_oracle_carries_a_45_float_state(oracle):
+    """The WEZ model's state (45 float slots: floats, a bool and per-adversary
+    uint16 / bool fields) through the oracle's closed loop: the packed words
+    keep valid fields (bools 0 / 1, step counters), and engagement zones
+    switch on."""
+    from mppi_metal_b200 import models
+    w = models.wez_batch(seed=11, N=3, K=256, H=12, T=8)
+    r = oracle.simulate_batch(oracle_problem(w), w.num_agents, w.num_steps, 0, w.seed, w.x0,
+                              cost_params_packed=w.cost_params_packed, cost_stride=w.cost_stride)
+    st = r["states"].astype(np.float32)
+    adv_words = np.ascontiguousarray(st[..., [9 + 5 * i for i in range(models.WEZ_ADVERSARIES)]])
+    bits = adv_words.view(np.uint32)
+    assert np.all(((bits >> 16) & 0xFF) <= 1) and np.all((bits >> 24) <= 1)
+    assert np.count_nonzero((bits >> 16) & 0xFF) > 0
+    cont = [0, 1, 2, 3] + [5 + 5 * i + j for i in range(8) for j in range(4)]
+    assert np.all(np.isfinite(st[..., cont]))
+    # the first state is the workload's x0, bit for bit
+    assert np.array_equal(st[0].view(np.uint32), w.x0.view(np.uint32))
