@@ -141,7 +141,7 @@ struct LaunchGeom {
   uint32_t pstride = 0;
   size_t smem = 0;
   // cooperative form: lanes per sample (0: one thread per sample); its CTAs
-  // have 128 threads, block = 128 / coop samples
+  // have block * coop threads
   uint32_t coop = 0;
 };
 
@@ -314,10 +314,11 @@ bool valid_identifier(const char* s) {
 // is resident at once with it; otherwise the noise is regenerated in chunks
 // after the costs are known.
 // The cooperative form (the plugin's stage cost split over lanes, module
-// coop_lanes > 0) serves launches whose plain form would have at most two
-// CTAs per SM: there each sample's serial chain sets the time, and splitting
-// its cost terms over lanes shortens it; with more CTAs the SMs' issue slots
-// are full and the lanes' repeated dynamics would only add work.  A fixed
+// coop_lanes > 0) serves launches whose plain form would have at most one
+// CTA per four SMs: there each sample's serial chain sets the time, and
+// splitting its cost terms over lanes shortens it; with more CTAs the SMs'
+// issue slots fill and the lanes' repeated dynamics only add work (measured:
+// the proposal workload's 256 CTAs ran 25% slower cooperative).  A fixed
 // rule of the launch shape, never a timing, so one problem always runs the
 // same arithmetic (the cooperative form sums a sample's cost terms in its
 // own order).
@@ -325,7 +326,7 @@ bool use_coop(const mppi_backend* b, uint32_t N) {
   if (b->ragged || !b->mod || b->mod->coop_lanes == 0 || b->coop_pin < 0) return false;
   if (b->coop_pin > 0) return true;
   const size_t plain_ctas = (size_t)N * ((b->K + 127) / 128);
-  return N > 0 && plain_ctas <= 2 * (size_t)b->num_sms;
+  return N > 0 && plain_ctas <= (size_t)b->num_sms / 4;
 }
 
 LaunchGeom choose_geometry(const mppi_backend* b, uint32_t N) {
@@ -333,13 +334,15 @@ LaunchGeom choose_geometry(const mppi_backend* b, uint32_t N) {
   const size_t HM = b->HM();
   const size_t budget = std::min<size_t>(b->max_smem_optin ? b->max_smem_optin : 232448, 232448);
   if (use_coop(b, N)) {
-    // 128 threads, 128 / lanes samples per CTA; the whole horizon staged when
-    // it fits the per-CTA share of four CTAs per SM, else in chunks
+    // 128 samples (128 * lanes threads, one CTA per SM) per CTA; the whole
+    // horizon staged when it fits the SM's shared memory, else in chunks
     g.coop = b->mod->coop_lanes;
-    g.block = 128 / g.coop;
+    g.block = 128;
     g.variant = 1;
     const size_t el = b->stage_elem;
-    const size_t per_cta = rollout_dynamic_share(b, b->mod->coop_static_smem, budget);
+    const size_t overhead = b->smem_reserved + b->mod->coop_static_smem;
+    const size_t per_cta =
+        std::min(budget, b->smem_per_sm > overhead ? b->smem_per_sm - overhead : (size_t)4096);
     const size_t fixed = nominal_bytes(b) + (size_t)g.block * 4;
     const size_t full = fixed + HM * g.block * el;
     if (full <= per_cta) {
@@ -736,7 +739,8 @@ cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a, bool ws = f
   if (b->geom.coop)
     return launch_dependent(b, fused ? (const void*)b->mod->rollout_coop_fused
                                      : (const void*)b->mod->rollout_coop,
-                            dim3(b->geom.nblk, b->N), dim3(128), b->geom.smem, args);
+                            dim3(b->geom.nblk, b->N), dim3(b->geom.block * b->geom.coop),
+                            b->geom.smem, args);
   return launch_dependent(b, fused ? (const void*)b->mod->rollout_fused[b->geom.variant]
                                    : (const void*)b->mod->rollout[b->geom.variant],
                           dim3(b->geom.nblk, b->N), dim3(b->geom.block), b->geom.smem, args);
@@ -2075,7 +2079,7 @@ int launch_step_with_scratch(mppi_backend* b, uint64_t step_index, const float* 
   float* stats = partials + (size_t)g.nblk * g.pstride;
   const void* rk = g.coop ? (const void*)b->mod->rollout_coop
                           : (const void*)b->mod->rollout[g.variant];
-  const uint32_t threads = g.coop ? 128u : g.block;
+  const uint32_t threads = g.coop ? g.block * g.coop : g.block;
   if (g.smem > 48 * 1024) {
     // raise the kernel's dynamic shared memory limit if it is below this
     // launch's need; never lower it (a prepared batch may need more)

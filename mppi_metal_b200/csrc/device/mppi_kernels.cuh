@@ -474,6 +474,10 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
       eps[d] = from_stage(stage_s[(size_t)((t - row0) * kM + d) * BLOCK + col]);
       u[d] = clampf(un_s[t * kM + d] + eps[d], lo[d], hi[d]);
     }
+    // the step's cost terms are added together first, then into the
+    // compensated sum once (the control cost lambda * u_nom^T Sigma^-1 eps
+    // with the stage cost, or with part 0 of a split stage cost)
+    float cterm = 0.0f;
 #if MPPI_CONTROL_COST
     {
       float cc = 0.0f;
@@ -489,7 +493,7 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
 #pragma unroll
       for (int i = 0; i < kM; ++i) cc = fmaf(un_s[t * kM + i], sinv[i] * eps[i], cc);
 #endif
-      acc_cost(J, Jlo, (LANES == 1 || sub == 0) ? a.lambda * cc : 0.0f);
+      cterm = (LANES == 1 || sub == 0) ? a.lambda * cc : 0.0f;
     }
 #endif
     MPPI_DYNAMICS_FN(reinterpret_cast<DynStateT>(reinterpret_cast<void*>(st)), u, mp,
@@ -497,11 +501,13 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
     if constexpr (LANES > 1)
       acc_cost(J, Jlo,
                StageSplit::part(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u, mp,
-                                cp, (int)sub));
+                                cp, (int)sub) +
+                   cterm);
     else
       acc_cost(J, Jlo,
                MPPI_STAGE_COST_FN(reinterpret_cast<StageStateT>(reinterpret_cast<void*>(st)), u,
-                                  mp, cp));
+                                  mp, cp) +
+                   cterm);
   };
   if constexpr (WS) {
     if (staged) {
@@ -991,16 +997,19 @@ extern "C" __global__ void __launch_bounds__(256, 2)
   mppi::rollout_body<128, true, true>(a);
 }
 
-// Cooperative forms (plugins with MPPI_STAGE_COST_SPLIT): 128 threads, i.e.
-// 128 / kCoopLanes samples per CTA.  Without a split the entries exist but
-// the host never launches them (mppi_coop_lanes reads 0).
-constexpr int kCoopBlock = mppi::kCoopLanes > 0 ? 128 / mppi::kCoopLanes : 128;
+// Cooperative forms (plugins with MPPI_STAGE_COST_SPLIT): 128 samples per
+// CTA, kCoopLanes * 128 threads -- as many partial records per agent as the
+// one-thread form, so the combine's work and its last-CTA count stay the
+// same.  Without a split the entries exist but the host never launches them
+// (mppi_coop_lanes reads 0).
+constexpr int kCoopBlock = 128;
 extern "C" __device__ const uint32_t mppi_coop_lanes = mppi::kCoopLanes;
-extern "C" __global__ void __launch_bounds__(128, 4) mppi_rollout_coop(const MppiRolloutArgs a) {
+extern "C" __global__ void __launch_bounds__(128 * (mppi::kCoopLanes > 0 ? mppi::kCoopLanes : 1), 1)
+    mppi_rollout_coop(const MppiRolloutArgs a) {
   if constexpr (mppi::kCoopLanes > 1)
     mppi::rollout_body<kCoopBlock, false, false, mppi::kCoopLanes>(a);
 }
-extern "C" __global__ void __launch_bounds__(128, 4)
+extern "C" __global__ void __launch_bounds__(128 * (mppi::kCoopLanes > 0 ? mppi::kCoopLanes : 1), 1)
     mppi_rollout_coop_fused(const MppiRolloutArgs a) {
   if constexpr (mppi::kCoopLanes > 1)
     mppi::rollout_body<kCoopBlock, true, false, mppi::kCoopLanes>(a);

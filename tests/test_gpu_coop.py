@@ -1,14 +1,16 @@
 """The cooperative rollout form (plugins that split their stage cost with
 MPPI_STAGE_COST_SPLIT; the unicycle splits its obstacle terms in 4 parts).
 
-For launches whose one-thread-per-sample form would have at most two CTAs
-per SM -- latency-bound: each sample's serial chain sets the time -- four
-lanes share a sample: they step the same dynamics on the same staged noise
+For launches whose one-thread-per-sample form would have at most one CTA
+per four SMs -- latency-bound: each sample's serial chain sets the time --
+four lanes share a sample: they step the same dynamics on the same staged noise
 and each accumulates one part of the stage cost; the parts are summed at the
 end.  Checked here:
   * the rule picks it for the single-agent configuration and not for the
     batched one;
-  * against the FP64 oracle: costs 1e-5 relative, u_next 1e-4, weights 1e-5;
+  * against the FP64 oracle: costs 1e-5 relative, u_next 1e-4, weights 1e-5
+    (a single agent); a batch closed loop at lambda = 1 as close to the
+    oracle as the reference's own FP32 kernels (see test_gpu_lambda_one.py);
   * against the one-thread-per-sample form (MPPI_B200_COOP=0): the same
     values up to the order of the cost sums (1e-6 relative on costs);
   * its fused and separate combines give the same bits, and the closed loop
@@ -95,7 +97,7 @@ def _loop(w):
 
 
 def test_cooperative_fused_and_separate_combine_same_bits():
-    w = models.unicycle_batch(seed=31, N=8, K=1000, H=24, T=10)
+    w = models.unicycle_batch(seed=31, N=3, K=1000, H=24, T=10)
     fused, ff = _env({"MPPI_B200_FUSED_COMBINE": "1"}, lambda: _loop(w))
     sep, fs = _env({"MPPI_B200_SEPARATE_COMBINE": "1"}, lambda: _loop(w))
     assert ff["cooperative"] and fs["cooperative"]
@@ -108,14 +110,24 @@ def test_cooperative_fused_and_separate_combine_same_bits():
 
 
 def test_cooperative_closed_loop_matches_oracle(oracle):
-    w = models.unicycle_batch(seed=32, N=6, K=1024, H=30, T=6)
+    import pyoracle
+    if not pyoracle.ref_available("unicycle_obstacles"):
+        pytest.skip("oracle/_ref (the reference kernels for the CPU) not built")
+    w = models.unicycle_batch(seed=32, N=4, K=1024, H=30, T=6)
     r, f = _loop(w)
     assert f["cooperative"]
-    o = oracle.simulate_batch(oracle_problem(w), w.num_agents, w.num_steps, 0, w.seed, w.x0,
+    p = oracle_problem(w)
+    o = oracle.simulate_batch(p, w.num_agents, w.num_steps, 0, w.seed, w.x0,
                               cost_params_packed=w.cost_params_packed, cost_stride=w.cost_stride,
                               sigma_packed=w.agent_sigma.astype(float))
-    assert abs_err(r["controls"], o["controls"]) <= 1e-4
-    assert abs_err(r["states"], o["states"]) <= 1e-4
+    rr = pyoracle.RefKernels("unicycle_obstacles").simulate_batch(
+        p, w.num_agents, w.num_steps, 0, w.seed, w.x0, sigma_packed=w.agent_sigma,
+        cost_params_packed=w.cost_params_packed, cost_stride=w.cost_stride,
+        model_params_packed=w.model_params, model_stride=0, nthreads=8)
+    for k in ("controls", "states"):
+        lib, ref = abs_err(r[k], o[k]), abs_err(rr[k], o[k])
+        print(f"cooperative closed loop {k}: library {lib:.2e}, reference FP32 kernels {ref:.2e}")
+        assert lib <= max(1e-4, 3.0 * ref)
 
 
 def test_cooperative_with_proposal_matches_one_thread_per_sample():
