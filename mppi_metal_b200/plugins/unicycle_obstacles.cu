@@ -161,14 +161,16 @@ __device__ float mppi_terminal_cost(const float* s, const uint8_t* model_params_
 //   [7..31)  the 8 obstacles of least clearance |p - c_i(t)| - r_i (ties:
 //            lower index first), each as its centre's body-frame offset / 10
 //            and its radius; missing obstacles give zeros
-// Everything stays in registers: the clearances of the 16 slots are ranked
-// by 8 unrolled arg-min passes, each taking its winner out of the running.
+// The ranking is computed all at once: obstacle i's rank is the number of
+// obstacles that come before it (smaller clearance, or equal clearance and
+// lower index), 256 independent comparisons instead of eight dependent
+// arg-min passes; the parameters are read into registers once.
 __device__ void mppi_proposal_features(const float* s, const uint8_t* model_params_raw,
                                        const uint8_t* cost_params_raw, float* f) {
   const UnicycleCostParams* c = reinterpret_cast<const UnicycleCostParams*>(cost_params_raw);
   const float x = s[0], y = s[1], t = s[3];
   float sn, cs;
-  sincosf(s[2], &sn, &cs);
+  mppi_sincosf(s[2], &sn, &cs);
   f[0] = x * 0.1f;
   f[1] = y * 0.1f;
   f[2] = cs;
@@ -180,31 +182,24 @@ __device__ void mppi_proposal_features(const float* s, const uint8_t* model_para
   const unsigned n = c->num_obs < MPPI_UNICYCLE_MAX_OBS ? c->num_obs : MPPI_UNICYCLE_MAX_OBS;
   const float inf = __int_as_float(0x7f800000);
   float ex[MPPI_UNICYCLE_MAX_OBS], ey[MPPI_UNICYCLE_MAX_OBS], clr[MPPI_UNICYCLE_MAX_OBS];
+  float rad[MPPI_UNICYCLE_MAX_OBS];
 #pragma unroll
   for (unsigned i = 0; i < MPPI_UNICYCLE_MAX_OBS; ++i) {
+    rad[i] = c->obs_r[i];
     ex[i] = fmaf(c->obs_vx[i], t, c->obs_cx[i]) - x;
     ey[i] = fmaf(c->obs_vy[i], t, c->obs_cy[i]) - y;
-    clr[i] = i < n ? sqrtf(ex[i] * ex[i] + ey[i] * ey[i]) - c->obs_r[i] : inf;
+    clr[i] = i < n ? sqrtf(ex[i] * ex[i] + ey[i] * ey[i]) - rad[i] : inf;
   }
 #pragma unroll
-  for (unsigned j = 0; j < 8; ++j) {
-    float bv = inf, bx = 0.0f, by = 0.0f, br = 0.0f;
-    unsigned best = MPPI_UNICYCLE_MAX_OBS;
+  for (unsigned i = 0; i < MPPI_UNICYCLE_MAX_OBS; ++i) {
+    unsigned rank = 0;
 #pragma unroll
-    for (unsigned i = 0; i < MPPI_UNICYCLE_MAX_OBS; ++i) {
-      const bool take = clr[i] < bv;  // strict: the lower index wins ties
-      bv = take ? clr[i] : bv;
-      bx = take ? ex[i] : bx;
-      by = take ? ey[i] : by;
-      br = take ? c->obs_r[i] : br;
-      best = take ? i : best;
-    }
-#pragma unroll
-    for (unsigned i = 0; i < MPPI_UNICYCLE_MAX_OBS; ++i) clr[i] = i == best ? inf : clr[i];
-    if (best < MPPI_UNICYCLE_MAX_OBS) {
-      f[7 + 3 * j] = (cs * bx + sn * by) * 0.1f;
-      f[8 + 3 * j] = (cs * by - sn * bx) * 0.1f;
-      f[9 + 3 * j] = br;
+    for (unsigned j = 0; j < MPPI_UNICYCLE_MAX_OBS; ++j)
+      rank += (clr[j] < clr[i] || (j < i && clr[j] == clr[i])) ? 1u : 0u;
+    if (i < n && rank < 8) {
+      f[7 + 3 * rank] = (cs * ex[i] + sn * ey[i]) * 0.1f;
+      f[8 + 3 * rank] = (cs * ey[i] - sn * ex[i]) * 0.1f;
+      f[9 + 3 * rank] = rad[i];
     }
   }
 }
