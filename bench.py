@@ -60,11 +60,11 @@ L2_FLUSH_BYTES = 256 << 20
 # issue-rate roofline.
 ROLLOUT_COUNTERS = {
     # workload: (warp-inst per rollout-step, DRAM bytes per launch)
-    "batch": (496386048 / 52428800, 237568),          # 9.47
-    "uneven": (178922783 / 16410677, 122880),         # 10.90
-    "single": (247536 / 30720, 39680),                # 8.06
-    "quadrotor/fp32": (6911910084 / 209715200, 153088),   # 32.96
-    "quadrotor/mixed": (6401390457 / 209715200, 124416),  # 30.52
+    "batch": (511516672 / 52428800, 239616),          # 9.76
+    "uneven": (183201988 / 16410677, 125440),         # 11.16
+    "single": (247536 / 30720, 39680),                # 8.06 (the build before compensated sums)
+    "quadrotor/fp32": (6963287662 / 209715200, 208640),   # 33.20
+    "quadrotor/mixed": (6449554461 / 209715200, 198656),  # 30.75
 }
 
 
@@ -683,6 +683,30 @@ def proposal_spec(name: str) -> dict:
                 desc="128 unicycle agents per GPU (16 moving obstacles, sigma U[0.2,0.8])")
 
 
+def net_roofline(per_agent: bool, flops: float, net_ms: float, rows: int, bf16_peak: float,
+                 peaks: dict, mhz: float) -> dict:
+    """The network pass of the proposal stage against its bound: the
+    per-agent form (CUDA cores, one CTA per agent, BF16 weights streamed from
+    L2) against the FP32 FMA rate, the tensor-core batch kernel against the
+    measured BF16 peak."""
+    achieved = flops / (net_ms / 1e3) / 1e12
+    if per_agent:
+        fma_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+        return {"kernel": "mppi_proposal_rows (per-agent network, CUDA cores)", "bound": "issue",
+                "achieved": achieved, "peak": fma_peak, "unit": "TFLOP/s",
+                "frac": achieved / fma_peak, "traffic": None,
+                "note": f"{rows} agents, one CTA each; every CTA streams the 354 KB of BF16 "
+                        "weights from L2 (latency-bound: four dependent layers per agent); "
+                        f"peak = 148 SMs x 128 FP32 FMA/clk x 2 x {mhz:.0f} MHz; the dominant "
+                        "kernel of the step is the rollout (issue-bound, see the batch workload)"}
+    return {"kernel": "mlp_forward_cluster_kernel (proposal network forward)", "bound": "tensor",
+            "achieved": achieved, "peak": bf16_peak, "unit": "TFLOP/s",
+            "frac": achieved / bf16_peak, "traffic": None,
+            "note": f"M = {rows} rows: 8-CTA clusters, latency-bound; the dominant kernel of the "
+                    "step is the rollout (issue-bound, see the batch workload); peak = measured "
+                    "bf16 burst" + ("" if peaks.get("bf16_tflops") else " (fallback)")}
+
+
 def measure_proposal(ctx, args, name: str, steps: int, warmup: int) -> dict:
     """Proposal-MPPI against plain MPPI with more samples, on the same agents
     (proposal_spec).  value = control steps/s of the first proposal arm;
@@ -750,6 +774,7 @@ def measure_proposal(ctx, args, name: str, steps: int, warmup: int) -> dict:
         form = prop.launch_info()
         rollout_ms, combine_ms = prop.time_passes(20)
         feat_ms, net_ms = prop.time_proposal(20)
+        per_agent = prop.proposal_stage()[2]
         prop.set_proposal(None)
         prop.close()
         value = ctx.world * N * T * steps / (prop_ms / 1e3)
@@ -777,16 +802,8 @@ def measure_proposal(ctx, args, name: str, steps: int, warmup: int) -> dict:
             "launch_geometry": form,
             "kernel_ms_per_pass": {"rollout": rollout_ms, "combine": combine_ms,
                                    "features_kernel": feat_ms, "network": net_ms},
-            "roofline": {"kernel": "mlp_forward_cluster_kernel (proposal network forward)",
-                         "bound": "tensor",
-                         "achieved": mlp_flops / (net_ms / 1e3) / 1e12, "peak": bf16_peak,
-                         "unit": "TFLOP/s",
-                         "frac": mlp_flops / (net_ms / 1e3) / 1e12 / bf16_peak,
-                         "traffic": None,
-                         "note": f"M = {N} rows: one 8-CTA cluster, latency-bound; the "
-                                 "dominant kernel of the step is the rollout (issue-bound, "
-                                 "see the batch workload); peak = measured bf16 burst"
-                                 + ("" if peaks.get("bf16_tflops") else " (fallback)")},
+            "roofline": net_roofline(per_agent, mlp_flops, net_ms, N, bf16_peak, peaks,
+                                     clk.get("sm_mhz") or 1965.0),
             "clocks": clk,
         })
     first = arms[0]

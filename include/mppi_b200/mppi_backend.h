@@ -180,6 +180,11 @@ int mppi_backend_batch_fetch(mppi_backend* b, float* states_out, float* controls
  * Per-sample costs of the last control step for agents [a0, a0 + n): [n][K]. */
 int mppi_backend_last_costs(mppi_backend* b, uint32_t a0, uint32_t n, float* out, char* err,
                             size_t err_len);
+/* The same costs exactly as the rollout accumulated them (each a pair of
+ * floats, hi + lo, returned as one double): what the weights were computed
+ * from. */
+int mppi_backend_last_cost_pairs(mppi_backend* b, uint32_t a0, uint32_t n, double* out,
+                                 char* err, size_t err_len);
 /* Normalised weights of the last control step for agents [a0, a0 + n): [n][K]. */
 int mppi_backend_last_weights(mppi_backend* b, uint32_t a0, uint32_t n, float* out,
                               char* err, size_t err_len);
@@ -320,7 +325,9 @@ int mppi_backend_batch_fetch_ustar(mppi_backend* b, float* ustar_out, char* err,
 int mppi_backend_proposal_stage(mppi_backend* b, float* features_out, float* outputs_out,
                                 uint32_t* per_agent, char* err, size_t err_len);
 /* Device time (CUDA events) of the proposal stage of one pass on the
- * prepared batch: the feature kernel and the network's forward pass. */
+ * prepared batch: the feature kernel, and the network's forward pass (the
+ * tensor-core batch kernel, or the per-agent network on the features
+ * already computed). */
 int mppi_backend_time_proposal(mppi_backend* b, uint32_t iters, float* features_ms,
                                float* network_ms, char* err, size_t err_len);
 

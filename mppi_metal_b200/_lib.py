@@ -117,6 +117,7 @@ SIGNATURES = {
     "mppi_backend_batch_fetch": (ctypes.c_int, [c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr,
                                                 c_ptr] + _ERR),
     "mppi_backend_last_costs": (ctypes.c_int, [c_ptr, c_u32, c_u32, c_ptr] + _ERR),
+    "mppi_backend_last_cost_pairs": (ctypes.c_int, [c_ptr, c_u32, c_u32, c_ptr] + _ERR),
     "mppi_backend_last_weights": (ctypes.c_int, [c_ptr, c_u32, c_u32, c_ptr] + _ERR),
     "mppi_backend_sample_noise": (ctypes.c_int, [c_ptr, c_u64, c_u32, c_u32, c_u32, c_ptr,
                                                  c_ptr, c_ptr] + _ERR),

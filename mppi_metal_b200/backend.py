@@ -256,6 +256,14 @@ class Backend:
         _check(self.lib.mppi_backend_last_costs(self.h, a0, n, _p(out), eb, len(eb)), eb)
         return out
 
+    def last_cost_pairs(self, a0: int = 0, n: Optional[int] = None) -> np.ndarray:
+        """The last step's per-sample costs exactly (hi + lo pairs as float64)."""
+        n = self.N - a0 if n is None else n
+        out = np.zeros((n, self.K), np.float64)
+        eb = _lib.err_buf()
+        _check(self.lib.mppi_backend_last_cost_pairs(self.h, a0, n, _p(out), eb, len(eb)), eb)
+        return out
+
     def last_weights(self, a0: int = 0, n: Optional[int] = None) -> np.ndarray:
         n = self.N - a0 if n is None else n
         out = np.zeros((n, self.K), np.float32)

@@ -314,19 +314,16 @@ bool valid_identifier(const char* s) {
 // is resident at once with it; otherwise the noise is regenerated in chunks
 // after the costs are known.
 // The cooperative form (the plugin's stage cost split over lanes, module
-// coop_lanes > 0) serves launches whose plain form would have at most one
-// CTA per four SMs: there each sample's serial chain sets the time, and
-// splitting its cost terms over lanes shortens it; with more CTAs the SMs'
-// issue slots fill and the lanes' repeated dynamics only add work (measured:
-// the proposal workload's 256 CTAs ran 25% slower cooperative).  A fixed
-// rule of the launch shape, never a timing, so one problem always runs the
-// same arithmetic (the cooperative form sums a sample's cost terms in its
-// own order).
+// coop_lanes > 0) runs when MPPI_B200_COOP=1 pins it.  It is not chosen on
+// its own: measured on the latency-bound single agent it issued 2.4x the
+// one-thread form's instructions (each lane repeats the dynamics) and ran
+// slower in the closed loop (5.35e4 against 6.05e4 control-steps/s; with
+// 32-sample CTAs its 4x partial records lengthened the combine tail
+// instead), and the proposal workload's 256 CTAs ran 25% slower with it.
+// Pinned, it is the same for every shape, so one problem always runs the
+// same arithmetic (it sums a sample's cost terms in its own order).
 bool use_coop(const mppi_backend* b, uint32_t N) {
-  if (b->ragged || !b->mod || b->mod->coop_lanes == 0 || b->coop_pin < 0) return false;
-  if (b->coop_pin > 0) return true;
-  const size_t plain_ctas = (size_t)N * ((b->K + 127) / 128);
-  return N > 0 && plain_ctas <= (size_t)b->num_sms / 4;
+  return !b->ragged && b->mod && b->mod->coop_lanes > 0 && b->coop_pin > 0 && N > 0;
 }
 
 LaunchGeom choose_geometry(const mppi_backend* b, uint32_t N) {
@@ -669,9 +666,11 @@ cudaError_t launch_network(mppi_backend* b) {
                                              b->pdl);
 }
 
-// Features and the network per agent, one CTA per agent (the rows kernel).
-cudaError_t launch_proposal_rows(mppi_backend* b) {
+// Features and the network per agent, one CTA per agent (the rows kernel);
+// given_features: the network alone on the features already in d_feat.
+cudaError_t launch_proposal_rows(mppi_backend* b, bool given_features = false) {
   MppiProposalRowsArgs a{};
+  a.given_features = given_features ? 1u : 0u;
   a.f.rows = b->N;
   a.f.agents_mod = b->N;
   a.f.x_stride = b->n;
@@ -1633,6 +1632,22 @@ int mppi_backend_last_costs(mppi_backend* b, uint32_t a0, uint32_t n, float* out
   return MPPI_OK;
 }
 
+int mppi_backend_last_cost_pairs(mppi_backend* b, uint32_t a0, uint32_t n, double* out,
+                                 char* err, size_t err_len) {
+  if (int rc = check_init(b, err, err_len)) return rc;
+  if (int rc = check_step_costs(b, a0, n, reinterpret_cast<const float*>(out), err, err_len))
+    return rc;
+  const size_t cnt = (size_t)n * b->K;
+  std::vector<float> hi(cnt), lo(cnt);
+  const float* base = b->d_costs.as<float>() + (size_t)a0 * b->K;
+  CK(cudaMemcpyAsync(hi.data(), base, cnt * 4, cudaMemcpyDeviceToHost, b->stream));
+  CK(cudaMemcpyAsync(lo.data(), base + (size_t)b->N * b->K, cnt * 4, cudaMemcpyDeviceToHost,
+                     b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  for (size_t i = 0; i < cnt; ++i) out[i] = (double)hi[i] + (double)lo[i];
+  return MPPI_OK;
+}
+
 int mppi_backend_last_weights(mppi_backend* b, uint32_t a0, uint32_t n, float* out, char* err,
                               size_t err_len) {
   if (int rc = check_init(b, err, err_len)) return rc;
@@ -1730,7 +1745,8 @@ int mppi_backend_time_proposal(mppi_backend* b, uint32_t iters, float* features_
   }
   float ms = 0.0f;
   if (net_per_agent(b)) {
-    // features kernel alone, then the rows kernel (features and network)
+    // features kernel alone, then the rows kernel on those features (the
+    // per-agent network alone)
     CK(cudaEventRecord(b->ev0, b->stream));
     for (uint32_t i = 0; i < iters; ++i) CK(launch_features(b));
     CK(cudaEventRecord(b->ev1, b->stream));
@@ -1738,7 +1754,7 @@ int mppi_backend_time_proposal(mppi_backend* b, uint32_t iters, float* features_
     CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
     if (features_ms) *features_ms = ms / iters;
     CK(cudaEventRecord(b->ev0, b->stream));
-    for (uint32_t i = 0; i < iters; ++i) CK(launch_proposal_rows(b));
+    for (uint32_t i = 0; i < iters; ++i) CK(launch_proposal_rows(b, true));
     CK(cudaEventRecord(b->ev1, b->stream));
     CK(cudaEventSynchronize(b->ev1));
     CK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));

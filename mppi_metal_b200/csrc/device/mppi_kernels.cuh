@@ -1070,7 +1070,11 @@ extern "C" __global__ void __launch_bounds__(128) mppi_proposal_rows(const MppiP
   const MppiFeaturesArgs& fa = a.f;
   // the states come from the previous kernel (no-op in plain launches)
   mppi::mppi_grid_dependency_wait();
-  if (threadIdx.x == 0) {
+  if (a.given_features) {
+    if (threadIdx.x < (uint32_t)MPPI_MAX_FEATURES)
+      feat_s[threadIdx.x] =
+          threadIdx.x < fa.out_stride ? fa.out[(size_t)r * fa.out_stride + threadIdx.x] : 0.0f;
+  } else if (threadIdx.x == 0) {
     const uint32_t agent = r % fa.agents_mod;
     __align__(16) float st[mppi::kNPad];
     const float* xr = fa.x + (size_t)r * fa.x_stride;

@@ -172,6 +172,8 @@ struct MppiFeaturesArgs {
 struct MppiProposalRowsArgs {
   MppiFeaturesArgs f;
   MppiNetRows net;
+  uint32_t given_features;  // 1: read the features from f.out instead (timing)
+  uint32_t pad0;
 };
 
 // Normalised weights from the per-sample costs and the combine statistics

@@ -1,13 +1,12 @@
 """The cooperative rollout form (plugins that split their stage cost with
 MPPI_STAGE_COST_SPLIT; the unicycle splits its obstacle terms in 4 parts).
 
-For launches whose one-thread-per-sample form would have at most one CTA
-per four SMs -- latency-bound: each sample's serial chain sets the time --
-four lanes share a sample: they step the same dynamics on the same staged noise
+Pinned with MPPI_B200_COOP=1 (the backend does not choose it by itself: on
+the shipped workloads it measured slower than the one-thread forms), four
+lanes share a sample: they step the same dynamics on the same staged noise
 and each accumulates one part of the stage cost; the parts are summed at the
 end.  Checked here:
-  * the rule picks it for the single-agent configuration and not for the
-    batched one;
+  * it runs only when pinned;
   * against the FP64 oracle: costs 1e-5 relative, u_next 1e-4, weights 1e-5
     (a single agent); a batch closed loop at lambda = 1 as close to the
     oracle as the reference's own FP32 kernels (see test_gpu_lambda_one.py);
@@ -28,6 +27,11 @@ from helpers import abs_err, backend_for, oracle_problem, rel_err
 from mppi_metal_b200 import models
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(autouse=True)
+def _cooperative(monkeypatch):
+    monkeypatch.setenv("MPPI_B200_COOP", "1")
 
 
 def _env(pairs, fn):
@@ -51,15 +55,11 @@ def _step(w, x0, u_nom, step=3):
     return out
 
 
-def test_rule_picks_cooperative_form_by_launch_shape():
+def test_cooperative_form_runs_only_when_pinned(monkeypatch):
     w = models.unicycle_single(seed=0, K=1024, H=30)
     assert _step(w, w.x0[0], np.zeros(60, np.float32))[4]["cooperative"]
-    wb = models.unicycle_batch(seed=1, N=256, K=4096, H=50, T=1)
-    b = backend_for(wb)
-    b.prepare(wb.num_agents, 1, wb.x0, cost_params=wb.cost_params_packed,
-              cost_stride=wb.cost_stride, sigma=wb.agent_sigma)
-    b.run(0)
-    assert not b.launch_info()["form"]["cooperative"]
+    monkeypatch.delenv("MPPI_B200_COOP")
+    assert not _step(w, w.x0[0], np.zeros(60, np.float32))[4]["cooperative"]
 
 
 @pytest.mark.parametrize("K,H", [(1024, 30), (777, 17)])

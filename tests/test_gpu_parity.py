@@ -156,7 +156,7 @@ def test_weights_and_ess_on_device_costs(oracle):
     b = backend_for(w)
     un = np.zeros(60, np.float32)
     _, diag = b.dispatch_rollout(0, w.x0[0], un)
-    costs = b.last_costs()[0]
+    costs = b.last_cost_pairs()[0]
     weights = b.last_weights()[0]
     w_o, d_o = oracle.weights(costs, w.lam)
     assert abs_err(weights, w_o) < TOL_WEIGHT
@@ -173,10 +173,14 @@ def test_update_stage_isolated_lambda_one(oracle):
     p = oracle_problem(w)
     un = np.random.default_rng(1).uniform(-0.3, 0.3, 100).astype(np.float32)
     u_out, diag = b.dispatch_rollout(2, w.x0[0], un)
-    costs = b.last_costs()[0]
+    # the costs as the device accumulated them (compensated pairs), which
+    # its weights were computed from
+    costs = b.last_cost_pairs()[0]
+    assert np.array_equal(costs.astype(np.float32), b.last_costs()[0])
     w_o, d_o = oracle.weights(costs, w.lam)
     u_o = oracle.update(p, 2, w.seed, w_o, un)
     assert abs_err(u_out, u_o) < TOL_U
+    assert abs_err(b.last_weights()[0], w_o) < TOL_WEIGHT
     assert rel_err([diag[2]], [d_o[2]]) < TOL_WEIGHT
 
 

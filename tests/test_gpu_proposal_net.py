@@ -201,8 +201,11 @@ def test_per_agent_network_closed_loop_matches_tensor_core_form():
         b.close()
         return r, kps
 
-    per_agent, k1 = run()
-    tensor_core, k2 = _with_env("MPPI_B200_NET_PER_AGENT", "0", run)
-    assert k2 == k1 + 1  # the tensor-core form launches the network every step
+    # the combine pinned inside the rollout, so the step forms differ only
+    # in the network
+    per_agent, k1 = _with_env("MPPI_B200_FUSED_COMBINE", "1", run)
+    tensor_core, k2 = _with_env("MPPI_B200_FUSED_COMBINE", "1",
+                                lambda: _with_env("MPPI_B200_NET_PER_AGENT", "0", run))
+    assert (k1, k2) == (1, 2)  # the tensor-core form launches the network every step
     assert np.abs(per_agent["controls"] - tensor_core["controls"]).max() <= 1e-3
     assert np.abs(per_agent["states"] - tensor_core["states"]).max() <= 1e-3
