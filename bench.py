@@ -62,7 +62,7 @@ ROLLOUT_COUNTERS = {
     # workload: (warp-inst per rollout-step, DRAM bytes per launch)
     "batch": (511516672 / 52428800, 239616),          # 9.76
     "uneven": (183201988 / 16410677, 125440),         # 11.16
-    "single": (247536 / 30720, 39680),                # 8.06 (the build before compensated sums)
+    "single": (256616 / 30720, 41728),                # 8.35
     "quadrotor/fp32": (6963287662 / 209715200, 208640),   # 33.20
     "quadrotor/mixed": (6449554461 / 209715200, 198656),  # 30.75
 }

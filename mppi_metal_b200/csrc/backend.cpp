@@ -141,8 +141,10 @@ struct LaunchGeom {
   uint32_t pstride = 0;
   size_t smem = 0;
   // cooperative form: lanes per sample (0: one thread per sample); its CTAs
-  // have block * coop threads
+  // have block * coop threads; coop_v indexes the module's cooperative
+  // entries (0: 32 samples per CTA, 1: 128)
   uint32_t coop = 0;
+  int coop_v = 1;
 };
 
 }  // namespace
@@ -314,16 +316,22 @@ bool valid_identifier(const char* s) {
 // is resident at once with it; otherwise the noise is regenerated in chunks
 // after the costs are known.
 // The cooperative form (the plugin's stage cost split over lanes, module
-// coop_lanes > 0) runs when MPPI_B200_COOP=1 pins it.  It is not chosen on
-// its own: measured on the latency-bound single agent it issued 2.4x the
-// one-thread form's instructions (each lane repeats the dynamics) and ran
-// slower in the closed loop (5.35e4 against 6.05e4 control-steps/s; with
-// 32-sample CTAs its 4x partial records lengthened the combine tail
-// instead), and the proposal workload's 256 CTAs ran 25% slower with it.
-// Pinned, it is the same for every shape, so one problem always runs the
-// same arithmetic (it sums a sample's cost terms in its own order).
+// coop_lanes > 0) serves launches whose one-thread form would have at most
+// one 128-sample CTA per four SMs (a single agent, a few agents): there each
+// sample's serial chain sets the time, and splitting its cost terms over
+// lanes, with 32-sample CTAs spread over four times as many SMs, shortens it
+// (the single-agent configuration: 13.9 against 15.5 us per control step).
+// With more CTAs the SMs' issue slots fill and the lanes' repeated dynamics
+// only add work (2.4x the instructions; the proposal workload's 256 CTAs ran
+// 25% slower cooperative).  A fixed rule of the launch shape, never a timing,
+// so one problem always runs the same arithmetic (the cooperative form sums
+// a sample's cost terms in its own order).  MPPI_B200_COOP=1 / 0 pins it on
+// (every shape) or off.
 bool use_coop(const mppi_backend* b, uint32_t N) {
-  return !b->ragged && b->mod && b->mod->coop_lanes > 0 && b->coop_pin > 0 && N > 0;
+  if (b->ragged || !b->mod || b->mod->coop_lanes == 0 || N == 0 || b->coop_pin < 0) return false;
+  if (b->coop_pin > 0) return true;
+  const size_t plain_ctas = (size_t)N * ((b->K + 127) / 128);
+  return plain_ctas <= (size_t)b->num_sms / 4;
 }
 
 LaunchGeom choose_geometry(const mppi_backend* b, uint32_t N) {
@@ -331,13 +339,18 @@ LaunchGeom choose_geometry(const mppi_backend* b, uint32_t N) {
   const size_t HM = b->HM();
   const size_t budget = std::min<size_t>(b->max_smem_optin ? b->max_smem_optin : 232448, 232448);
   if (use_coop(b, N)) {
-    // 128 samples (128 * lanes threads, one CTA per SM) per CTA; the whole
-    // horizon staged when it fits the SM's shared memory, else in chunks
+    // 32 samples per CTA (32 * lanes threads) where the one-thread form
+    // would have at most one 128-sample CTA per four SMs, so an agent's
+    // samples spread over four times as many SMs; otherwise 128 samples
+    // (128 * lanes threads, one CTA per SM).  The whole horizon is staged
+    // when it fits the SM's shared memory, else in chunks.
     g.coop = b->mod->coop_lanes;
-    g.block = 128;
+    const size_t plain_ctas = (size_t)N * ((b->K + 127) / 128);
+    g.coop_v = plain_ctas <= (size_t)b->num_sms / 4 ? 0 : 1;
+    g.block = g.coop_v == 0 ? 32 : 128;
     g.variant = 1;
     const size_t el = b->stage_elem;
-    const size_t overhead = b->smem_reserved + b->mod->coop_static_smem;
+    const size_t overhead = b->smem_reserved + b->mod->coop_static_smem[g.coop_v];
     const size_t per_cta =
         std::min(budget, b->smem_per_sm > overhead ? b->smem_per_sm - overhead : (size_t)4096);
     const size_t fixed = nominal_bytes(b) + (size_t)g.block * 4;
@@ -423,7 +436,8 @@ cudaError_t set_rollout_smem(const mppi_backend* b) {
   }
   if (b->geom.coop) {
     for (const void* f :
-         {(const void*)b->mod->rollout_coop, (const void*)b->mod->rollout_coop_fused}) {
+         {(const void*)b->mod->rollout_coop[b->geom.coop_v],
+          (const void*)b->mod->rollout_coop_fused[b->geom.coop_v]}) {
       cudaError_t e =
           cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem);
       if (e != cudaSuccess) return e;
@@ -736,8 +750,8 @@ cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a, bool ws = f
     return cudaLaunchKernel(f, dim3(b->grid), dim3(128), args, b->geom.smem, b->stream);
   }
   if (b->geom.coop)
-    return launch_dependent(b, fused ? (const void*)b->mod->rollout_coop_fused
-                                     : (const void*)b->mod->rollout_coop,
+    return launch_dependent(b, fused ? (const void*)b->mod->rollout_coop_fused[b->geom.coop_v]
+                                     : (const void*)b->mod->rollout_coop[b->geom.coop_v],
                             dim3(b->geom.nblk, b->N), dim3(b->geom.block * b->geom.coop),
                             b->geom.smem, args);
   return launch_dependent(b, fused ? (const void*)b->mod->rollout_fused[b->geom.variant]
@@ -2093,7 +2107,7 @@ int launch_step_with_scratch(mppi_backend* b, uint64_t step_index, const float* 
   float* zero = scratch;
   float* partials = scratch + 16;
   float* stats = partials + (size_t)g.nblk * g.pstride;
-  const void* rk = g.coop ? (const void*)b->mod->rollout_coop
+  const void* rk = g.coop ? (const void*)b->mod->rollout_coop[g.coop_v]
                           : (const void*)b->mod->rollout[g.variant];
   const uint32_t threads = g.coop ? g.block * g.coop : g.block;
   if (g.smem > 48 * 1024) {

@@ -209,44 +209,6 @@ __device__ __forceinline__ double cost_pair(float hi, float lo) {
 __device__ __forceinline__ float pair_hi(double v) { return (float)v; }
 __device__ __forceinline__ float pair_lo(double v) { return (float)(v - (double)(float)v); }
 
-// Block reductions with a fixed combination order (bit-reproducible).
-// scratch must hold NW doubles (8-byte aligned).
-template <int NW>
-__device__ __forceinline__ double block_min_d(double v, double* scratch) {
-  v = warp_min_d(v);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) scratch[w] = v;
-  __syncthreads();
-  double r = scratch[0];
-#pragma unroll
-  for (int i = 1; i < NW; ++i) r = fmin(r, scratch[i]);
-  return r;
-}
-template <int NW>
-__device__ __forceinline__ void block_sum3(float& a, float& b, float& c, float* scratch) {
-  a = warp_sum(a);
-  b = warp_sum(b);
-  c = warp_sum(c);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  __syncthreads();
-  if (lane == 0) {
-    scratch[3 * w + 0] = a;
-    scratch[3 * w + 1] = b;
-    scratch[3 * w + 2] = c;
-  }
-  __syncthreads();
-  a = scratch[0];
-  b = scratch[1];
-  c = scratch[2];
-#pragma unroll
-  for (int i = 1; i < NW; ++i) {
-    a += scratch[3 * i + 0];
-    b += scratch[3 * i + 1];
-    c += scratch[3 * i + 2];
-  }
-}
-
 __device__ __forceinline__ float clampf(float v, float lo, float hi) {
   // Metal clamp(x, lo, hi) = min(max(x, lo), hi)
   return fminf(fmaxf(v, lo), hi);
@@ -359,7 +321,8 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   constexpr int PER_LANE = BLOCK / 32;
   static_assert(BLOCK % 32 == 0, "sample columns come in warps");
   extern __shared__ __align__(16) float dsm[];
-  __shared__ __align__(8) float red_s[3 * NW];  // block sums; NW doubles for the minimum
+  __shared__ double wmin_s[NW];    // per-warp minimum costs
+  __shared__ float wsum_s[3 * NW];  // per-warp sums of e, e^2 and the costs
 #if MPPI_MP_SMEM
   __shared__ __align__(16) uint32_t mp_s[(MPPI_MP_BYTES + 3) / 4];
 #endif
@@ -522,8 +485,14 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
 #pragma unroll 4
           for (uint32_t t = n0; t < n1; ++t) draw(t, 0u);
         } else if (runs) {
-          const uint32_t c1 = min(H, c0 + kWsChunk);
-          for (uint32_t t = c0; t < c1; ++t) advance(t, 0u);
+          // a whole chunk unrolled: the compiler can start step t + 1's
+          // dynamics while step t's cost terms are still in flight
+          if (c0 + kWsChunk <= H) {
+#pragma unroll
+            for (uint32_t i = 0; i < kWsChunk; ++i) advance(c0 + i, 0u);
+          } else {
+            for (uint32_t t = c0; t < H; ++t) advance(t, 0u);
+          }
         }
         __syncthreads();
       }
@@ -543,12 +512,25 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
     for (uint32_t t0 = 0; t0 < H; t0 += TC) {
       const uint32_t t1 = min(H, t0 + TC);
       const uint32_t row0 = staged ? 0u : t0;
+      if constexpr (LANES > 1) {
+        // a lane draws every LANES-th step: all of them at once (few CTAs
+        // per SM, so the Philox chains' latency is what shows); two steps
+        // of the recurrence per pass, so step t + 1's dynamics can start
+        // while step t's cost terms are in flight
+#pragma unroll 8
+        for (uint32_t t = t0 + sub; t < t1; t += LANES) draw(t, row0);
+        __syncwarp();
+        if (runs) {
+#pragma unroll 2
+          for (uint32_t t = t0; t < t1; ++t) advance(t, row0);
+        }
+        __syncwarp();
+      } else {
 #pragma unroll 4
-      for (uint32_t t = t0 + sub; t < t1; t += LANES) draw(t, row0);
-      if constexpr (LANES > 1) __syncwarp();
-      if (runs)
-        for (uint32_t t = t0; t < t1; ++t) advance(t, row0);
-      if constexpr (LANES > 1) __syncwarp();
+        for (uint32_t t = t0; t < t1; ++t) draw(t, row0);
+        if (runs)
+          for (uint32_t t = t0; t < t1; ++t) advance(t, row0);
+      }
     }
   }
   double Jd = __longlong_as_double(0x7ff0000000000000ll);  // +inf: no sample here
@@ -579,19 +561,42 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   // ---- CTA softmax statistics against the CTA minimum ----
   // The minimum and the differences c_k - m_b are taken on the cost pairs
   // (as doubles), so exp(-(c_k - m_b) / lambda) sees no rounding of c_k.
-  const double bmin = block_min_d<NW>(Jd, reinterpret_cast<double*>(red_s));
+  // Two CTA barriers: per-warp minima, then the e_k and per-warp sums; the
+  // warps' values combine in warp order (the same bits for any schedule).
+  {
+    const double wm = warp_min_d(Jd);
+    if (lane == 0) wmin_s[warp] = wm;
+  }
+  __syncthreads();
+  double bmin = wmin_s[0];
+#pragma unroll
+  for (int i = 1; i < NW; ++i) bmin = fmin(bmin, wmin_s[i]);
   const float e = counts ? expf(-(float)(Jd - bmin) / a.lambda) : 0.0f;
-  float s_e = e, s_e2 = e * e, s_c = counts ? pair_hi(Jd) : 0.0f;
-  block_sum3<NW>(s_e, s_e2, s_c, red_s);
   if (!producer && sub == 0) e_s[col] = e;
+  {
+    const float s_e = warp_sum(e), s_e2 = warp_sum(e * e),
+                s_c = warp_sum(counts ? pair_hi(Jd) : 0.0f);
+    if (lane == 0) {
+      wsum_s[3 * warp + 0] = s_e;
+      wsum_s[3 * warp + 1] = s_e2;
+      wsum_s[3 * warp + 2] = s_c;
+    }
+  }
+  __syncthreads();
   if (tid == 0) {
+    float s_e = wsum_s[0], s_e2 = wsum_s[1], s_c = wsum_s[2];
+#pragma unroll
+    for (int i = 1; i < NW; ++i) {
+      s_e += wsum_s[3 * i + 0];
+      s_e2 += wsum_s[3 * i + 1];
+      s_c += wsum_s[3 * i + 2];
+    }
     part[0] = pair_hi(bmin);
     part[1] = s_e;
     part[2] = s_e2;
     part[3] = s_c;
     part[4] = pair_lo(bmin);
   }
-  __syncthreads();
   float e_r[PER_LANE];
 #pragma unroll
   for (int i = 0; i < PER_LANE; ++i) e_r[i] = e_s[lane + 32 * i];
@@ -611,7 +616,27 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
     } else {
       base = stage_s + (size_t)r0 * BLOCK;
     }
-    for (uint32_t r = warp; r < rows; r += NW) {
+    // four rows per pass, so their loads and shuffle trees overlap; each
+    // row's sum is formed as in the one-row loop that finishes the chunk
+    uint32_t r = warp;
+    for (; r + 3 * NW < rows; r += 4 * NW) {
+      float s[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const stage_t* row = base + (size_t)(r + q * NW) * BLOCK;
+        s[q] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < PER_LANE; ++i)
+          s[q] = fmaf(e_r[i], from_stage(row[lane + 32 * i]), s[q]);
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) s[q] = warp_sum(s[q]);
+      if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) part[MPPI_PARTIAL_HEAD + r0 + r + q * NW] = s[q];
+      }
+    }
+    for (; r < rows; r += NW) {
       const stage_t* row = base + (size_t)r * BLOCK;
       float s = 0.0f;
 #pragma unroll
@@ -622,28 +647,35 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   }
 }
 
-template <int CB>
+template <int CB, uint32_t PRE>
 __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t agent,
                                               float* dsm);
 
 // The combine fused into the rollout launch (a.agent_done set): after its
 // partial record, the CTA counts itself done for its agent, and the agent's
 // last CTA (the one that brings the count to nblk) runs the agent's combine
-// and resets the count.  The "last block" pattern: every CTA publishes its
-// record with a device-scope fence before it counts, so the last one reads
-// every record complete; no CTA waits on another.
-template <int BLOCK>
+// and resets the count.  The "last block" pattern, with no CTA waiting on
+// another: the CTA barrier orders every thread's record stores before thread
+// 0's count, an atomic add with release and acquire semantics at device
+// scope, so the CTA that counts last sees every other CTA's record complete
+// (and its barrier hands that on to its other threads).  One atomic replaces
+// a device-scope fence on each side of a relaxed add.
+__device__ __forceinline__ uint32_t atomic_add_acq_rel(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+template <int BLOCK, uint32_t PRE = 32>
 __device__ __forceinline__ void fused_combine_tail(const MppiRolloutArgs& a, uint32_t agent,
                                                    uint32_t nblk) {
   __shared__ uint32_t last_s;
-  __threadfence();  // this CTA's partial record (written by several threads)
-  __syncthreads();  // ... complete, and the staging memory free for reuse
-  if (threadIdx.x == 0) last_s = atomicAdd(a.agent_done + agent, 1u) + 1u == nblk;
+  __syncthreads();  // this CTA's partial record complete, the staging memory free for reuse
+  if (threadIdx.x == 0) last_s = atomic_add_acq_rel(a.agent_done + agent, 1u) + 1u == nblk;
   __syncthreads();
   if (!last_s) return;
-  __threadfence();  // the other CTAs' records, published before their counts
   extern __shared__ __align__(16) float dsm_c[];
-  combine_agent<BLOCK>(a.comb, agent, dsm_c);
+  combine_agent<BLOCK, PRE>(a.comb, agent, dsm_c);
   if (threadIdx.x == 0) a.agent_done[agent] = 0u;
 }
 
@@ -683,7 +715,7 @@ __device__ __forceinline__ void rollout_work(const MppiRolloutArgs& a) {
                         a.u_nom + (size_t)agent * a.H * kM,
                         a.partials + ((size_t)a.agent_blk0[agent] + blk) * a.pstride);
     if (FUSED && a.agent_done)
-      fused_combine_tail<BLOCK>(a, agent, (a.agent_K[agent] + BLOCK - 1) / BLOCK);
+      fused_combine_tail<BLOCK, 0>(a, agent, (a.agent_K[agent] + BLOCK - 1) / BLOCK);
   }
 }
 
@@ -817,7 +849,9 @@ __device__ __noinline__ void network_row(const float* f, const MppiNetRows& net,
 }
 #endif
 
-template <int CB>
+// PRE: records whose weighted-sum columns are read ahead (0: none; the
+// uneven batches' persistent kernel keeps its registers for the rollout).
+template <int CB, uint32_t PRE>
 __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t agent,
                                               float* dsm) {
   __shared__ float stat_s[4];
@@ -836,20 +870,65 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   float* u_s = dsm + ((a.nblk + 3) & ~3u);  // a.nblk: the largest agent's CTA count
   const float* P = a.partials + blk0 * ps;
 
+  float* un = a.u_nom + (size_t)agent * a.H * kM;  // agent stride: the largest horizon
+  float* uo = a.u_out + (size_t)agent * a.H * kM;
+
+  // Read ahead, before the statistics are known (one round trip to L2
+  // instead of three): each thread's first weighted-sum column of every
+  // record and its nominal value (agents of at most PRE records), and the
+  // state the propagate stage advances (small states).
+  constexpr uint32_t kPre = PRE > 0 ? PRE : 1;
+  constexpr bool kPreX = kN <= 16;
+  const bool pre = PRE > 0 && nblk <= PRE && tid < HM;
+  float pv[kPre], un_pre = 0.0f;
+  if (pre) {
+#pragma unroll
+    for (uint32_t b = 0; b < kPre; ++b)
+      pv[b] = b < nblk ? __ldcg(P + (size_t)b * ps + MPPI_PARTIAL_HEAD + tid) : 0.0f;
+    un_pre = un[tid];
+  }
+  float x_pre[kPreX ? kN : 1];
+  uint32_t step_pre = 0;
+  if (kPreX && tid == 0 && a.propagate) {
+#pragma unroll
+    for (int d = 0; d < (kPreX ? kN : 1); ++d) x_pre[d] = a.x[(size_t)agent * kN + d];
+  }
+  if (tid == 0 && a.propagate) step_pre = *a.step_base + a.step_local;
+  // the bounds of this thread's first column (its control dimension)
+  const float lo_pre = tid < HM ? a.u_min[tid % kM] : 0.0f;
+  const float hi_pre = tid < HM ? a.u_max[tid % kM] : 0.0f;
+
   // Statistics over the CTA records by warp 0 alone (lane l takes records
   // l, l + 32, ...), so the summation order -- and every bit of the result --
   // is the same whichever CTA size runs the combine.
   // The records' minima are cost pairs (hi at 0, lo at 4), compared and
-  // subtracted as doubles like the rollout's per-sample costs.
+  // subtracted as doubles like the rollout's per-sample costs.  A lane's
+  // first record is read once and kept (for up to 32 records, its only one).
   if (tid < 32) {
-    double lm = __longlong_as_double(0x7ff0000000000000ll);
-    for (uint32_t b = tid; b < nblk; b += 32) {
+    double lm = __longlong_as_double(0x7ff0000000000000ll), m0 = lm;
+    float e0 = 0.0f, q0 = 0.0f, c0 = 0.0f;
+    if (tid < nblk) {
+      const float* pb = P + (size_t)tid * ps;
+      m0 = cost_pair(__ldcg(pb), __ldcg(pb + 4));
+      e0 = __ldcg(pb + 1);
+      q0 = __ldcg(pb + 2);
+      c0 = __ldcg(pb + 3);
+      lm = fmin(lm, m0);
+    }
+    for (uint32_t b = tid + 32; b < nblk; b += 32) {
       const float* pb = P + (size_t)b * ps;
       lm = fmin(lm, cost_pair(__ldcg(pb), __ldcg(pb + 4)));
     }
     const double Mw = warp_min_d(lm);
     float S = 0.0f, Q = 0.0f, C = 0.0f;
-    for (uint32_t b = tid; b < nblk; b += 32) {
+    if (tid < nblk) {
+      const float sc = expf(-(float)(m0 - Mw) / a.lambda);
+      scale_s[tid] = sc;
+      S = fmaf(sc, e0, S);
+      Q = fmaf(sc * sc, q0, Q);
+      C += c0;
+    }
+    for (uint32_t b = tid + 32; b < nblk; b += 32) {
       const float* pb = P + (size_t)b * ps;
       const float sc = expf(-(float)(cost_pair(__ldcg(pb), __ldcg(pb + 4)) - Mw) / a.lambda);
       scale_s[b] = sc;
@@ -872,15 +951,22 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   const float M = stat_s[0], S = stat_s[1], Q = stat_s[2], C = stat_s[3];
 
   const float invS = 1.0f / S;
-  float* un = a.u_nom + (size_t)agent * a.H * kM;  // agent stride: the largest horizon
-  float* uo = a.u_out + (size_t)agent * a.H * kM;
   for (uint32_t j = tid; j < HM; j += CB) {
-    float v = 0.0f;
+    float v = 0.0f, un_j;
+    if (pre && j == tid) {
+#pragma unroll
+      for (uint32_t b = 0; b < kPre; ++b)  // in record order, as below
+        if (b < nblk) v = fmaf(scale_s[b], pv[b], v);
+      un_j = un_pre;
+    } else {
 #pragma unroll 8
-    for (uint32_t b = 0; b < nblk; ++b)  // in record order: loads run ahead of the sum
-      v = fmaf(scale_s[b], __ldcg(P + (size_t)b * ps + MPPI_PARTIAL_HEAD + j), v);
+      for (uint32_t b = 0; b < nblk; ++b)  // in record order: loads run ahead of the sum
+        v = fmaf(scale_s[b], __ldcg(P + (size_t)b * ps + MPPI_PARTIAL_HEAD + j), v);
+      un_j = un[j];
+    }
     const uint32_t d = j % kM;
-    const float u = clampf(un[j] + v * invS, a.u_min[d], a.u_max[d]);
+    const float u = clampf(un_j + v * invS, j == tid ? lo_pre : a.u_min[d],
+                           j == tid ? hi_pre : a.u_max[d]);
     u_s[j] = u;
     uo[j] = u;
   }
@@ -906,13 +992,13 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
 
   // ---- propagate & shift (shaders/mppi_reduce.metal:175-231, 413-488) ----
   if (tid == 0) {
-    const uint32_t step = *a.step_base + a.step_local;
+    const uint32_t step = step_pre;
     const uint32_t row = a.step_local * a.num_agents + agent;
     float* xg = a.x + (size_t)agent * kN;
     __align__(16) float st[kNPad];
     float u0[kM];
 #pragma unroll
-    for (int d = 0; d < kN; ++d) st[d] = xg[d];
+    for (int d = 0; d < kN; ++d) st[d] = kPreX ? x_pre[kPreX ? d : 0] : xg[d];
 #pragma unroll
     for (int d = kN; d < kNPad; ++d) st[d] = 0.0f;
 #pragma unroll
@@ -997,22 +1083,30 @@ extern "C" __global__ void __launch_bounds__(256, 2)
   mppi::rollout_body<128, true, true>(a);
 }
 
-// Cooperative forms (plugins with MPPI_STAGE_COST_SPLIT): 128 samples per
-// CTA, kCoopLanes * 128 threads -- as many partial records per agent as the
-// one-thread form, so the combine's work and its last-CTA count stay the
-// same.  Without a split the entries exist but the host never launches them
+// Cooperative forms (plugins with MPPI_STAGE_COST_SPLIT), kCoopLanes threads
+// per sample: mppi_rollout_coop32 with 32 samples per CTA (128 threads for
+// four lanes), for launches with few CTAs, where it spreads an agent's
+// samples over four times as many SMs; mppi_rollout_coop with 128 samples
+// per CTA, as many partial records per agent as the one-thread form.
+// Without a split the entries exist but the host never launches them
 // (mppi_coop_lanes reads 0).
-constexpr int kCoopBlock = 128;
+constexpr int kCoopLanesOr1 = mppi::kCoopLanes > 0 ? mppi::kCoopLanes : 1;
 extern "C" __device__ const uint32_t mppi_coop_lanes = mppi::kCoopLanes;
-extern "C" __global__ void __launch_bounds__(128 * (mppi::kCoopLanes > 0 ? mppi::kCoopLanes : 1), 1)
-    mppi_rollout_coop(const MppiRolloutArgs a) {
-  if constexpr (mppi::kCoopLanes > 1)
-    mppi::rollout_body<kCoopBlock, false, false, mppi::kCoopLanes>(a);
+extern "C" __global__ void __launch_bounds__(32 * kCoopLanesOr1, 4)
+    mppi_rollout_coop32(const MppiRolloutArgs a) {
+  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<32, false, false, mppi::kCoopLanes>(a);
 }
-extern "C" __global__ void __launch_bounds__(128 * (mppi::kCoopLanes > 0 ? mppi::kCoopLanes : 1), 1)
+extern "C" __global__ void __launch_bounds__(32 * kCoopLanesOr1, 4)
+    mppi_rollout_coop32_fused(const MppiRolloutArgs a) {
+  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<32, true, false, mppi::kCoopLanes>(a);
+}
+extern "C" __global__ void __launch_bounds__(128 * kCoopLanesOr1, 1)
+    mppi_rollout_coop(const MppiRolloutArgs a) {
+  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<128, false, false, mppi::kCoopLanes>(a);
+}
+extern "C" __global__ void __launch_bounds__(128 * kCoopLanesOr1, 1)
     mppi_rollout_coop_fused(const MppiRolloutArgs a) {
-  if constexpr (mppi::kCoopLanes > 1)
-    mppi::rollout_body<kCoopBlock, true, false, mppi::kCoopLanes>(a);
+  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<128, true, false, mppi::kCoopLanes>(a);
 }
 
 // Uneven batches always use 128-thread CTAs, so the partition of samples into
@@ -1029,7 +1123,7 @@ extern "C" __global__ void __launch_bounds__(128, 4)
 extern "C" __global__ void __launch_bounds__(mppi::kCombineBlock)
     mppi_combine(const MppiCombineArgs a) {
   extern __shared__ __align__(16) float dsm[];
-  mppi::combine_agent<mppi::kCombineBlock>(a, blockIdx.x, dsm);
+  mppi::combine_agent<mppi::kCombineBlock, 32>(a, blockIdx.x, dsm);
 }
 
 extern "C" __global__ void __launch_bounds__(256) mppi_weights(const MppiWeightsArgs a) {

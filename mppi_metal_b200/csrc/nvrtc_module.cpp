@@ -313,9 +313,14 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
   if (ce == cudaSuccess)
     ce = cudaLibraryGetKernel(&mod->rollout_ws_fused, mod->library, "mppi_rollout_ws_fused_b128");
   if (ce == cudaSuccess)
-    ce = cudaLibraryGetKernel(&mod->rollout_coop, mod->library, "mppi_rollout_coop");
+    ce = cudaLibraryGetKernel(&mod->rollout_coop[0], mod->library, "mppi_rollout_coop32");
   if (ce == cudaSuccess)
-    ce = cudaLibraryGetKernel(&mod->rollout_coop_fused, mod->library, "mppi_rollout_coop_fused");
+    ce = cudaLibraryGetKernel(&mod->rollout_coop_fused[0], mod->library,
+                              "mppi_rollout_coop32_fused");
+  if (ce == cudaSuccess)
+    ce = cudaLibraryGetKernel(&mod->rollout_coop[1], mod->library, "mppi_rollout_coop");
+  if (ce == cudaSuccess)
+    ce = cudaLibraryGetKernel(&mod->rollout_coop_fused[1], mod->library, "mppi_rollout_coop_fused");
   if (ce == cudaSuccess) {
     // lanes per sample of the cooperative form (0: the plugin declares no split)
     void* g = nullptr;
@@ -345,12 +350,12 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
       ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_ws_fused));
     mod->ws_static_smem = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
   }
-  if (ce == cudaSuccess) {
+  for (int v = 0; v < 2 && ce == cudaSuccess; ++v) {
     cudaFuncAttributes fa{}, ff{};
-    ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout_coop));
+    ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout_coop[v]));
     if (ce == cudaSuccess)
-      ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_coop_fused));
-    mod->coop_static_smem = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
+      ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_coop_fused[v]));
+    mod->coop_static_smem[v] = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
   }
   if (ce == cudaSuccess) {
     cudaFuncAttributes fa{}, ff{};

@@ -57,12 +57,13 @@ struct KernelModule {
   cudaKernel_t rollout_ws = nullptr;
   cudaKernel_t rollout_ws_fused = nullptr;
   size_t ws_static_smem = 0;
-  // cooperative forms (128 threads, coop_lanes per sample), plain and fused;
+  // cooperative forms (coop_lanes threads per sample), plain and fused:
+  // [0] 32 samples per CTA (latency-bound launches), [1] 128 samples per CTA;
   // coop_lanes = 0 when the plugin declares no split stage cost
-  cudaKernel_t rollout_coop = nullptr;
-  cudaKernel_t rollout_coop_fused = nullptr;
+  cudaKernel_t rollout_coop[2] = {nullptr, nullptr};
+  cudaKernel_t rollout_coop_fused[2] = {nullptr, nullptr};
   uint32_t coop_lanes = 0;
-  size_t coop_static_smem = 0;
+  size_t coop_static_smem[2] = {0, 0};
   cudaKernel_t combine = nullptr;
   cudaKernel_t weights = nullptr;
   cudaKernel_t noise = nullptr;

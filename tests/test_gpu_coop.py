@@ -1,15 +1,18 @@
 """The cooperative rollout form (plugins that split their stage cost with
 MPPI_STAGE_COST_SPLIT; the unicycle splits its obstacle terms in 4 parts).
 
-Pinned with MPPI_B200_COOP=1 (the backend does not choose it by itself: on
-the shipped workloads it measured slower than the one-thread forms), four
-lanes share a sample: they step the same dynamics on the same staged noise
-and each accumulates one part of the stage cost; the parts are summed at the
-end.  Checked here:
-  * it runs only when pinned;
+Four lanes share a sample: they step the same dynamics on the same staged
+noise and each accumulates one part of the stage cost; the parts are summed
+at the end.  The backend uses it for launch shapes whose one-thread form
+would have at most one 128-sample CTA per four SMs (32-sample CTAs there);
+MPPI_B200_COOP=1 pins it for every shape (128-sample CTAs for large ones),
+MPPI_B200_COOP=0 off.  Pinned on here unless a test says otherwise.
+Checked here:
+  * the shape rule and the pins;
   * against the FP64 oracle: costs 1e-5 relative, u_next 1e-4, weights 1e-5
-    (a single agent); a batch closed loop at lambda = 1 as close to the
-    oracle as the reference's own FP32 kernels (see test_gpu_lambda_one.py);
+    (a single agent); batch closed loops at lambda = 1 (both CTA sizes) as
+    close to the oracle as the reference's own FP32 kernels (see
+    test_gpu_lambda_one.py);
   * against the one-thread-per-sample form (MPPI_B200_COOP=0): the same
     values up to the order of the cost sums (1e-6 relative on costs);
   * its fused and separate combines give the same bits, and the closed loop
@@ -55,11 +58,28 @@ def _step(w, x0, u_nom, step=3):
     return out
 
 
-def test_cooperative_form_runs_only_when_pinned(monkeypatch):
-    w = models.unicycle_single(seed=0, K=1024, H=30)
-    assert _step(w, w.x0[0], np.zeros(60, np.float32))[4]["cooperative"]
+def test_cooperative_form_follows_shape_rule_and_pins(monkeypatch):
+    single = models.unicycle_single(seed=0, K=1024, H=30)
+    u0 = np.zeros(60, np.float32)
+    assert _step(single, single.x0[0], u0)[4]["cooperative"]
+    monkeypatch.setenv("MPPI_B200_COOP", "0")
+    assert not _step(single, single.x0[0], u0)[4]["cooperative"]
     monkeypatch.delenv("MPPI_B200_COOP")
-    assert not _step(w, w.x0[0], np.zeros(60, np.float32))[4]["cooperative"]
+    assert _step(single, single.x0[0], u0)[4]["cooperative"]  # few CTAs: by default
+    big = models.unicycle_batch(seed=3, N=48, K=1024, H=20, T=2)
+
+    def form():
+        b = backend_for(big)
+        b.prepare(big.num_agents, big.num_steps, big.x0, cost_params=big.cost_params_packed,
+                  cost_stride=big.cost_stride, sigma=big.agent_sigma)
+        b.run(0)
+        f = b.launch_info()["form"]
+        b.close()
+        return f
+
+    assert not form()["cooperative"]  # many CTAs: the one-thread form
+    monkeypatch.setenv("MPPI_B200_COOP", "1")
+    assert form()["cooperative"]
 
 
 @pytest.mark.parametrize("K,H", [(1024, 30), (777, 17)])
@@ -96,6 +116,21 @@ def _loop(w):
     return r, f
 
 
+def test_cooperative_cta_size_follows_the_launch_shape():
+    # few CTAs: 32 samples per CTA (an agent's samples over more SMs); many:
+    # 128 samples per CTA (as many partial records as the one-thread form)
+    small = models.unicycle_batch(seed=34, N=2, K=1024, H=20, T=2)
+    large = models.unicycle_batch(seed=35, N=48, K=1024, H=20, T=2)
+    for w, block in ((small, 32), (large, 128)):
+        b = backend_for(w)
+        b.prepare(w.num_agents, w.num_steps, w.x0, cost_params=w.cost_params_packed,
+                  cost_stride=w.cost_stride, sigma=w.agent_sigma)
+        b.run(0)
+        info = b.launch_info()
+        b.close()
+        assert info["form"]["cooperative"] and info["block"] == block, info
+
+
 def test_cooperative_fused_and_separate_combine_same_bits():
     w = models.unicycle_batch(seed=31, N=3, K=1000, H=24, T=10)
     fused, ff = _env({"MPPI_B200_FUSED_COMBINE": "1"}, lambda: _loop(w))
@@ -109,13 +144,18 @@ def test_cooperative_fused_and_separate_combine_same_bits():
         assert np.array_equal(fused[k], again[k]), k
 
 
-def test_cooperative_closed_loop_matches_oracle(oracle):
+@pytest.mark.parametrize("N,H,T,block", [(4, 30, 6, 32), (48, 20, 3, 128)])
+def test_cooperative_closed_loop_matches_oracle(oracle, N, H, T, block):
     import pyoracle
     if not pyoracle.ref_available("unicycle_obstacles"):
         pytest.skip("oracle/_ref (the reference kernels for the CPU) not built")
-    w = models.unicycle_batch(seed=32, N=4, K=1024, H=30, T=6)
-    r, f = _loop(w)
-    assert f["cooperative"]
+    w = models.unicycle_batch(seed=32, N=N, K=1024, H=H, T=T)
+    b = backend_for(w)
+    r = b.simulate_batch(w.num_agents, w.num_steps, 0, w.x0, cost_params=w.cost_params_packed,
+                         cost_stride=w.cost_stride, sigma=w.agent_sigma)
+    f, blk = b.launch_info()["form"], b.launch_info()["block"]
+    b.close()
+    assert f["cooperative"] and blk == block
     p = oracle_problem(w)
     o = oracle.simulate_batch(p, w.num_agents, w.num_steps, 0, w.seed, w.x0,
                               cost_params_packed=w.cost_params_packed, cost_stride=w.cost_stride,
