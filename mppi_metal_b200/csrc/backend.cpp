@@ -444,7 +444,9 @@ cudaError_t set_rollout_smem(const mppi_backend* b) {
     }
   }
   if (!b->ragged) {
-    for (const void* f : {(const void*)b->mod->rollout_ws, (const void*)b->mod->rollout_ws_fused}) {
+    for (const void* f : {(const void*)b->mod->rollout_ws, (const void*)b->mod->rollout_ws_fused,
+                          (const void*)b->mod->rollout_early,
+                          (const void*)b->mod->rollout_early_fused}) {
       cudaError_t e =
           cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->geom.smem);
       if (e != cudaSuccess) return e;
@@ -729,6 +731,16 @@ cudaError_t launch_dependent(const mppi_backend* b, const void* func, dim3 grid,
   return cudaLaunchKernelExC(&cfg, func, args);
 }
 
+// The one-thread 128-sample form with the early noise (drawn before the
+// wait for the previous launch): uniform batches with the whole horizon
+// staged and no proposal attached.  Same bits as mppi_rollout_b128; its own
+// entry, because the early path's extra live state cost the chunked
+// quadrotor rollout 132 bytes of spills.
+bool early_noise(const mppi_backend* b) {
+  return !b->ragged && !b->geom.coop && b->geom.variant == 1 && b->geom.block == 128 &&
+         b->geom.stage_rows >= b->HM() && !(b->proposal && b->spec.proposal);
+}
+
 // A rollout launch with prepared arguments (uniform grid, or the uneven
 // batch's work items).
 cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a, bool ws = false) {
@@ -754,6 +766,10 @@ cudaError_t launch_rollout_args(mppi_backend* b, MppiRolloutArgs& a, bool ws = f
                                      : (const void*)b->mod->rollout_coop[b->geom.coop_v],
                             dim3(b->geom.nblk, b->N), dim3(b->geom.block * b->geom.coop),
                             b->geom.smem, args);
+  if (early_noise(b))
+    return launch_dependent(b, fused ? (const void*)b->mod->rollout_early_fused
+                                     : (const void*)b->mod->rollout_early,
+                            dim3(b->geom.nblk, b->N), dim3(b->geom.block), b->geom.smem, args);
   return launch_dependent(b, fused ? (const void*)b->mod->rollout_fused[b->geom.variant]
                                    : (const void*)b->mod->rollout[b->geom.variant],
                           dim3(b->geom.nblk, b->N), dim3(b->geom.block), b->geom.smem, args);

@@ -311,7 +311,7 @@ constexpr int kCoopLanes = StageSplit::parts;
 static_assert(kCoopLanes == 0 || kCoopLanes == 2 || kCoopLanes == 4,
               "MPPI_STAGE_COST_SPLIT: the part count must be 2 or 4");
 
-template <int BLOCK, bool WS = false, int LANES = 1>
+template <int BLOCK, bool WS = false, int LANES = 1, bool EARLY = false>
 __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t agent,
                                              uint32_t blk, uint32_t K, uint32_t H,
                                              const float* un_g, float* part) {
@@ -378,43 +378,55 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
   float sinv[kSig];
   load_sigma(a.sigma_inv + (size_t)a.sigma_inv_stride * agent, sinv);
 #endif
-  // Everything above is constant over a closed loop; the nominal, the state
-  // and the proposal's output below are written by the previous launches.
-  mppi_grid_dependency_wait();
-  for (uint32_t i = tid; i < HM; i += NT) un_s[i] = un_g[i];
 #if MPPI_PROPOSAL
   // samples k < pcount draw around the network's predicted sequence; the
   // shift and the scales live in shared memory, not in registers, so the
   // rollout's register budget stays the plain kernel's
   __shared__ float ps_s[kM];
   const uint32_t pcount = a.prop_out ? a.prop_count : 0u;
-  if (pcount) {
-    const float* po = a.prop_out + (size_t)agent * a.prop_stride;
-    for (uint32_t i = tid; i < HM; i += NT)
-      sh_s[i] = i < a.prop_ls_offset ? po[i] - un_g[i] : 0.0f;
-    if (tid < (uint32_t)kM)
-      ps_s[tid] = expf(clampf(po[a.prop_ls_offset + tid], a.prop_ls_min, a.prop_ls_max));
-  }
+#else
+  constexpr uint32_t pcount = 0;
 #endif
-  __syncthreads();
-
-  // ---- rollout: noise -> clamp -> dynamics -> stage cost; terminal cost ----
-  // Time is processed in chunks of TC steps (the whole horizon when the
-  // staging buffer holds it).  Phase A draws the chunk's noise into this
-  // thread's own staging column: Philox chains of different steps are
-  // independent, so they overlap.  Phase B runs the state recurrence, reading
-  // the noise back.  No thread touches another's column until the weighted
-  // sums, so neither phase needs a barrier.
+  // Early noise: the noise depends on the step index, the sample and the
+  // agent's sigma only -- nothing an earlier launch writes -- so without a
+  // proposal the first chunk of it (the whole horizon when the staging
+  // buffer holds it) is drawn before the wait for the previous launch.  A
+  // step whose CTAs are resident early (a launch of few CTAs, programmatic
+  // dependent launch) draws it while the previous step still runs, off the
+  // critical path.  The values are the ones drawn after the wait would be.
+  // Compiled in where EARLY is set (the cooperative entries and the
+  // mppi_rollout_early_* entries, which the host launches with the whole
+  // horizon staged), so the other kernels keep their register allocation.
+  const bool early = EARLY && !WS && pcount == 0u;
   float J = 0.0f, Jlo = 0.0f;  // the sample's cost as the pair J + Jlo (acc_cost)
   __align__(16) float st[kNPad];
   const bool runs = active && !producer;  // this thread runs a sample's recurrence
-  if (runs) {
-    const float* xg = a.x + (size_t)agent * kN;
-#pragma unroll
-    for (int d = 0; d < kN; ++d) st[d] = xg[d];
-  }
 #pragma unroll
   for (int d = kN; d < kNPad; ++d) st[d] = 0.0f;
+  // The wait for the previous launch, then what it wrote: the nominal, the
+  // proposal's output and (MPPI_LOAD_STATE, at each call site: no register
+  // array captured by the lambda) the state.  Everything before it is
+  // constant over a closed loop.  Ends with a CTA barrier (the nominal, the
+  // proposal's shift and any noise rows drawn before it visible to all).
+#define MPPI_LOAD_STATE()                                \
+  if (runs) {                                            \
+    const float* xg_ = a.x + (size_t)agent * kN;         \
+    _Pragma("unroll") for (int d_ = 0; d_ < kN; ++d_) st[d_] = xg_[d_]; \
+  }
+  auto wait_and_load = [&]() {
+    mppi_grid_dependency_wait();
+    for (uint32_t i = tid; i < HM; i += NT) un_s[i] = un_g[i];
+#if MPPI_PROPOSAL
+    if (pcount) {
+      const float* po = a.prop_out + (size_t)agent * a.prop_stride;
+      for (uint32_t i = tid; i < HM; i += NT)
+        sh_s[i] = i < a.prop_ls_offset ? po[i] - un_g[i] : 0.0f;
+      if (tid < (uint32_t)kM)
+        ps_s[tid] = expf(clampf(po[a.prop_ls_offset + tid], a.prop_ls_min, a.prop_ls_max));
+    }
+#endif
+    __syncthreads();
+  };
   // Noise of step t into this thread's staging column (row (t - row0) * m + d).
   auto draw = [&](uint32_t t, uint32_t row0) {
     float n[2 * kP], eps[kM];
@@ -472,18 +484,43 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
                                   mp, cp) +
                    cterm);
   };
+  // ---- rollout: noise -> clamp -> dynamics -> stage cost; terminal cost ----
+  // Time is processed in chunks of TC steps (the whole horizon when the
+  // staging buffer holds it).  Phase A draws the chunk's noise into this
+  // sample's staging column: Philox chains of different steps are
+  // independent, so they overlap.  Phase B runs the state recurrence,
+  // reading the noise back.  No thread touches another sample's column until
+  // the weighted sums, so the phases need no CTA barrier of their own; the
+  // lanes of a cooperative sample (one warp) share a column and meet at a
+  // warp barrier between the phases.  The wait for the previous launch comes
+  // first, or (early noise) after the first chunk's phase A.
+  if (!early) {
+    wait_and_load();
+    MPPI_LOAD_STATE();
+  }
   if constexpr (WS) {
     if (staged) {
-      // producers stay one chunk ahead; the barrier after each chunk makes
-      // the next chunk's rows visible to the recurrence warps
-      if (producer)
-        for (uint32_t t = 0; t < min(H, kWsChunk); ++t) draw(t, 0u);
-      __syncthreads();
+      // producers draw the first chunk (early noise: the whole horizon) and
+      // then stay one chunk ahead; the barrier after each chunk makes the
+      // next chunk's rows visible to the recurrence warps
+      const uint32_t first = early ? H : min(H, kWsChunk);
+      if (producer) {
+#pragma unroll 4
+        for (uint32_t t = 0; t < first; ++t) draw(t, 0u);
+      }
+      if (early) {
+        wait_and_load();
+        MPPI_LOAD_STATE();
+      } else {
+        __syncthreads();
+      }
       for (uint32_t c0 = 0; c0 < H; c0 += kWsChunk) {
         if (producer) {
-          const uint32_t n0 = c0 + kWsChunk, n1 = min(H, n0 + kWsChunk);
+          if (!early) {
+            const uint32_t n0 = c0 + kWsChunk, n1 = min(H, n0 + kWsChunk);
 #pragma unroll 4
-          for (uint32_t t = n0; t < n1; ++t) draw(t, 0u);
+            for (uint32_t t = n0; t < n1; ++t) draw(t, 0u);
+          }
         } else if (runs) {
           // a whole chunk unrolled: the compiler can start step t + 1's
           // dynamics while step t's cost terms are still in flight
@@ -494,45 +531,46 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
             for (uint32_t t = c0; t < H; ++t) advance(t, 0u);
           }
         }
-        __syncthreads();
+        if (!early) __syncthreads();
       }
     } else {
+      if (early) wait_and_load();
       J = __int_as_float(0x7fc00000);  // the host never runs this form chunked: NaN marks it
     }
   } else {
-    // Time is processed in chunks of TC steps (the whole horizon when the
-    // staging buffer holds it).  Phase A draws the chunk's noise into this
-    // sample's staging column: Philox chains of different steps are
-    // independent, so they overlap.  Phase B runs the state recurrence,
-    // reading the noise back.  No thread touches another sample's column
-    // until the weighted sums, so neither phase needs a CTA barrier; the
-    // lanes of a cooperative sample (one warp) share a column and meet at a
-    // warp barrier between the phases.
     const uint32_t TC = staged ? H : a.stage_rows / kM;
+    if (early && H == 0u) wait_and_load();
     for (uint32_t t0 = 0; t0 < H; t0 += TC) {
       const uint32_t t1 = min(H, t0 + TC);
       const uint32_t row0 = staged ? 0u : t0;
       if constexpr (LANES > 1) {
-        // a lane draws every LANES-th step: all of them at once (few CTAs
-        // per SM, so the Philox chains' latency is what shows); two steps
-        // of the recurrence per pass, so step t + 1's dynamics can start
-        // while step t's cost terms are in flight
-#pragma unroll 8
+        // a lane draws every LANES-th step
+#pragma unroll 4
         for (uint32_t t = t0 + sub; t < t1; t += LANES) draw(t, row0);
-        __syncwarp();
-        if (runs) {
-#pragma unroll 2
-          for (uint32_t t = t0; t < t1; ++t) advance(t, row0);
-        }
-        __syncwarp();
       } else {
 #pragma unroll 4
         for (uint32_t t = t0; t < t1; ++t) draw(t, row0);
-        if (runs)
-          for (uint32_t t = t0; t < t1; ++t) advance(t, row0);
       }
+      if (early && t0 == 0u) {
+        wait_and_load();  // its CTA barrier also orders the lanes' rows
+        MPPI_LOAD_STATE();
+      } else if constexpr (LANES > 1) {
+        __syncwarp();
+      }
+      if (runs) {
+        if constexpr (LANES > 1) {
+          // two steps per pass: step t + 1's dynamics can start while step
+          // t's cost terms are in flight
+#pragma unroll 2
+          for (uint32_t t = t0; t < t1; ++t) advance(t, row0);
+        } else {
+          for (uint32_t t = t0; t < t1; ++t) advance(t, row0);
+        }
+      }
+      if constexpr (LANES > 1) __syncwarp();
     }
   }
+#undef MPPI_LOAD_STATE
   double Jd = __longlong_as_double(0x7ff0000000000000ll);  // +inf: no sample here
   if constexpr (LANES > 1) {
     // part 0 carries the terminal cost; the parts meet in a butterfly
@@ -682,11 +720,11 @@ __device__ __forceinline__ void fused_combine_tail(const MppiRolloutArgs& a, uin
 // Uniform batch: grid (nblk, num_agents), every agent K samples, horizon H.
 // FUSED: the kernel form with the combine tail (a separate entry point, so
 // the plain form keeps its register allocation).
-template <int BLOCK, bool FUSED, bool WS = false, int LANES = 1>
+template <int BLOCK, bool FUSED, bool WS = false, int LANES = 1, bool EARLY = false>
 __device__ __forceinline__ void rollout_body(const MppiRolloutArgs& a) {
   mppi_allow_dependent_launch();
   const uint32_t agent = blockIdx.y, blk = blockIdx.x;
-  rollout_item<BLOCK, WS, LANES>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
+  rollout_item<BLOCK, WS, LANES, EARLY>(a, agent, blk, a.K, a.H, a.u_nom + (size_t)agent * a.H * kM,
                                  a.partials + ((size_t)agent * a.nblk + blk) * a.pstride);
   if (FUSED && a.agent_done)
     fused_combine_tail<WS ? 2 * BLOCK : BLOCK * LANES>(a, agent, a.nblk);
@@ -876,9 +914,10 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   // Read ahead, before the statistics are known (one round trip to L2
   // instead of three): each thread's first weighted-sum column of every
   // record and its nominal value (agents of at most PRE records), and the
-  // state the propagate stage advances (small states).
+  // state the propagate stage advances (small states).  Nothing is read
+  // ahead with PRE = 0.
   constexpr uint32_t kPre = PRE > 0 ? PRE : 1;
-  constexpr bool kPreX = kN <= 16;
+  constexpr bool kPreX = PRE > 0 && kN <= 16;
   const bool pre = PRE > 0 && nblk <= PRE && tid < HM;
   float pv[kPre], un_pre = 0.0f;
   if (pre) {
@@ -893,10 +932,10 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
 #pragma unroll
     for (int d = 0; d < (kPreX ? kN : 1); ++d) x_pre[d] = a.x[(size_t)agent * kN + d];
   }
-  if (tid == 0 && a.propagate) step_pre = *a.step_base + a.step_local;
+  if (PRE > 0 && tid == 0 && a.propagate) step_pre = *a.step_base + a.step_local;
   // the bounds of this thread's first column (its control dimension)
-  const float lo_pre = tid < HM ? a.u_min[tid % kM] : 0.0f;
-  const float hi_pre = tid < HM ? a.u_max[tid % kM] : 0.0f;
+  const float lo_pre = PRE > 0 && tid < HM ? a.u_min[tid % kM] : 0.0f;
+  const float hi_pre = PRE > 0 && tid < HM ? a.u_max[tid % kM] : 0.0f;
 
   // Statistics over the CTA records by warp 0 alone (lane l takes records
   // l, l + 32, ...), so the summation order -- and every bit of the result --
@@ -965,8 +1004,9 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
       un_j = un[j];
     }
     const uint32_t d = j % kM;
-    const float u = clampf(un_j + v * invS, j == tid ? lo_pre : a.u_min[d],
-                           j == tid ? hi_pre : a.u_max[d]);
+    const bool first = PRE > 0 && j == tid;
+    const float u = clampf(un_j + v * invS, first ? lo_pre : a.u_min[d],
+                           first ? hi_pre : a.u_max[d]);
     u_s[j] = u;
     uo[j] = u;
   }
@@ -992,7 +1032,7 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
 
   // ---- propagate & shift (shaders/mppi_reduce.metal:175-231, 413-488) ----
   if (tid == 0) {
-    const uint32_t step = step_pre;
+    const uint32_t step = PRE > 0 ? step_pre : *a.step_base + a.step_local;
     const uint32_t row = a.step_local * a.num_agents + agent;
     float* xg = a.x + (size_t)agent * kN;
     __align__(16) float st[kNPad];
@@ -1073,6 +1113,17 @@ MPPI_ROLLOUT_ENTRY(64)
 MPPI_ROLLOUT_ENTRY(128)
 MPPI_ROLLOUT_ENTRY(256)
 
+// 128-sample forms with the early noise (drawn before the wait for the
+// previous launch): launched for uniform batches with the whole horizon
+// staged and no proposal output to read.
+extern "C" __global__ void __launch_bounds__(128, 4) mppi_rollout_early_b128(const MppiRolloutArgs a) {
+  mppi::rollout_body<128, false, false, 1, true>(a);
+}
+extern "C" __global__ void __launch_bounds__(128, 4)
+    mppi_rollout_early_fused_b128(const MppiRolloutArgs a) {
+  mppi::rollout_body<128, true, false, 1, true>(a);
+}
+
 // Warp-specialised forms for 128-sample CTAs (256 threads: 128 running the
 // recurrence, 128 drawing the noise ahead), whole horizon staged.
 extern "C" __global__ void __launch_bounds__(256, 2) mppi_rollout_ws_b128(const MppiRolloutArgs a) {
@@ -1094,19 +1145,19 @@ constexpr int kCoopLanesOr1 = mppi::kCoopLanes > 0 ? mppi::kCoopLanes : 1;
 extern "C" __device__ const uint32_t mppi_coop_lanes = mppi::kCoopLanes;
 extern "C" __global__ void __launch_bounds__(32 * kCoopLanesOr1, 4)
     mppi_rollout_coop32(const MppiRolloutArgs a) {
-  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<32, false, false, mppi::kCoopLanes>(a);
+  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<32, false, false, mppi::kCoopLanes, true>(a);
 }
 extern "C" __global__ void __launch_bounds__(32 * kCoopLanesOr1, 4)
     mppi_rollout_coop32_fused(const MppiRolloutArgs a) {
-  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<32, true, false, mppi::kCoopLanes>(a);
+  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<32, true, false, mppi::kCoopLanes, true>(a);
 }
 extern "C" __global__ void __launch_bounds__(128 * kCoopLanesOr1, 1)
     mppi_rollout_coop(const MppiRolloutArgs a) {
-  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<128, false, false, mppi::kCoopLanes>(a);
+  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<128, false, false, mppi::kCoopLanes, true>(a);
 }
 extern "C" __global__ void __launch_bounds__(128 * kCoopLanesOr1, 1)
     mppi_rollout_coop_fused(const MppiRolloutArgs a) {
-  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<128, true, false, mppi::kCoopLanes>(a);
+  if constexpr (mppi::kCoopLanes > 1) mppi::rollout_body<128, true, false, mppi::kCoopLanes, true>(a);
 }
 
 // Uneven batches always use 128-thread CTAs, so the partition of samples into

@@ -309,6 +309,11 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
   if (ce == cudaSuccess)
     ce = cudaLibraryGetKernel(&mod->rollout_work_fused, mod->library,
                               "mppi_rollout_work_fused_b128");
+  if (ce == cudaSuccess)
+    ce = cudaLibraryGetKernel(&mod->rollout_early, mod->library, "mppi_rollout_early_b128");
+  if (ce == cudaSuccess)
+    ce = cudaLibraryGetKernel(&mod->rollout_early_fused, mod->library,
+                              "mppi_rollout_early_fused_b128");
   if (ce == cudaSuccess) ce = cudaLibraryGetKernel(&mod->rollout_ws, mod->library, "mppi_rollout_ws_b128");
   if (ce == cudaSuccess)
     ce = cudaLibraryGetKernel(&mod->rollout_ws_fused, mod->library, "mppi_rollout_ws_fused_b128");
@@ -342,6 +347,15 @@ int load_module(const ModuleSpec& spec, std::shared_ptr<const KernelModule>* out
     if (ce == cudaSuccess)
       ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_fused[i]));
     mod->rollout_static_smem[i] = std::max(fa.sharedSizeBytes, ff.sharedSizeBytes);
+  }
+  if (ce == cudaSuccess) {
+    // the early-noise 128-sample forms share the 128-sample geometry
+    cudaFuncAttributes fa{}, ff{};
+    ce = cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(mod->rollout_early));
+    if (ce == cudaSuccess)
+      ce = cudaFuncGetAttributes(&ff, reinterpret_cast<const void*>(mod->rollout_early_fused));
+    mod->rollout_static_smem[1] =
+        std::max(mod->rollout_static_smem[1], std::max(fa.sharedSizeBytes, ff.sharedSizeBytes));
   }
   if (ce == cudaSuccess) {
     cudaFuncAttributes fa{}, ff{};

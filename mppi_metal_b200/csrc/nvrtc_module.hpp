@@ -54,6 +54,9 @@ struct KernelModule {
   cudaKernel_t rollout_fused[3] = {nullptr, nullptr, nullptr};
   cudaKernel_t rollout_work_fused = nullptr;
   // warp-specialised 128-sample forms (256 threads), plain and fused
+  // 128-sample forms with the early noise (whole horizon staged), plain and fused
+  cudaKernel_t rollout_early = nullptr;
+  cudaKernel_t rollout_early_fused = nullptr;
   cudaKernel_t rollout_ws = nullptr;
   cudaKernel_t rollout_ws_fused = nullptr;
   size_t ws_static_smem = 0;
