@@ -654,6 +654,22 @@ __device__ __forceinline__ void rollout_item(const MppiRolloutArgs& a, uint32_t 
     } else {
       base = stage_s + (size_t)r0 * BLOCK;
     }
+    if constexpr (BLOCK == 32) {
+      // 32 samples (the cooperative 32-sample CTA): one thread per row, over
+      // the samples from a rotated start (row r from sample r mod 32), so a
+      // warp's shared-memory reads hit 32 different banks
+      for (uint32_t r = tid; r < rows; r += NT) {
+        const stage_t* row = base + (size_t)r * BLOCK;
+        float s = 0.0f;
+#pragma unroll
+        for (uint32_t i = 0; i < 32u; ++i) {
+          const uint32_t c = (i + r) & 31u;
+          s = fmaf(e_s[c], from_stage(row[c]), s);
+        }
+        part[MPPI_PARTIAL_HEAD + r0 + r] = s;
+      }
+      continue;
+    }
     // four rows per pass, so their loads and shuffle trees overlap; each
     // row's sum is formed as in the one-row loop that finishes the chunk
     uint32_t r = warp;
@@ -911,6 +927,17 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   float* un = a.u_nom + (size_t)agent * a.H * kM;  // agent stride: the largest horizon
   float* uo = a.u_out + (size_t)agent * a.H * kM;
 
+  // Warp 0's lanes load their first record's head first: the statistics
+  // wait on it, so it goes ahead of the reads below in the memory pipeline.
+  float h0 = 0.0f, l0 = 0.0f, e0 = 0.0f, q0 = 0.0f, c0 = 0.0f;
+  if (tid < 32 && tid < nblk) {
+    const float* pb = P + (size_t)tid * ps;
+    h0 = __ldcg(pb);
+    l0 = __ldcg(pb + 4);
+    e0 = __ldcg(pb + 1);
+    q0 = __ldcg(pb + 2);
+    c0 = __ldcg(pb + 3);
+  }
   // Read ahead, before the statistics are known (one round trip to L2
   // instead of three): each thread's first weighted-sum column of every
   // record and its nominal value (agents of at most PRE records), and the
@@ -945,13 +972,8 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   // first record is read once and kept (for up to 32 records, its only one).
   if (tid < 32) {
     double lm = __longlong_as_double(0x7ff0000000000000ll), m0 = lm;
-    float e0 = 0.0f, q0 = 0.0f, c0 = 0.0f;
     if (tid < nblk) {
-      const float* pb = P + (size_t)tid * ps;
-      m0 = cost_pair(__ldcg(pb), __ldcg(pb + 4));
-      e0 = __ldcg(pb + 1);
-      q0 = __ldcg(pb + 2);
-      c0 = __ldcg(pb + 3);
+      m0 = cost_pair(h0, l0);
       lm = fmin(lm, m0);
     }
     for (uint32_t b = tid + 32; b < nblk; b += 32) {
