@@ -437,6 +437,18 @@ def e2e_bytes(w, ks=None):
     return h2d, d2h
 
 
+def rollout_kernel_name(w, geom: dict, ragged: bool) -> str:
+    """The rollout kernel the launch-time measurement runs (the form without
+    the combine tail) for the prepared launch shape."""
+    if ragged:
+        return "mppi_rollout_work_b128"
+    if geom["form"]["cooperative"]:
+        return "mppi_rollout_coop32" if geom["block"] == 32 else "mppi_rollout_coop"
+    if geom["block"] == 128 and geom["stage_rows"] >= w.horizon * w.control_dim:
+        return "mppi_rollout_early_b128"  # whole horizon staged, no proposal: early noise
+    return "mppi_rollout_b%d" % geom["block"]
+
+
 def measure_workload(ctx, args, name: str, numeric: str, steps: int, warmup: int,
                      with_cpu: bool) -> dict:
     """One plain-MPPI workload: device-resident closed loops (value), the
@@ -514,7 +526,7 @@ def measure_workload(ctx, args, name: str, numeric: str, steps: int, warmup: int
                                 "sample": "2 agents x 2 closed-loop steps, one thread"}}
 
     rollout_units = rollout_steps_per_control_step(w)  # rollout-steps per rollout launch
-    kname = "mppi_rollout_work_b128" if ks is not None else "mppi_rollout_b%d" % geom["block"]
+    kname = rollout_kernel_name(w, geom, ks is not None)
     key = name + ("/" + numeric if name == "quadrotor" else "")
     inst, dram = ROLLOUT_COUNTERS.get(key, (None, None))
     roof = {"kernel": kname, "bound": "issue",
