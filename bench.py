@@ -59,12 +59,13 @@ L2_FLUSH_BYTES = 256 << 20
 # of the launch.  Used only to express the live-timed kernel against the SM
 # issue-rate roofline.
 ROLLOUT_COUNTERS = {
-    # workload: (warp-inst per rollout-step, DRAM bytes per launch)
-    "batch": (511516672 / 52428800, 239616),          # 9.76
-    "uneven": (183201988 / 16410677, 125440),         # 11.16
-    "single": (256616 / 30720, 41728),                # 8.35
-    "quadrotor/fp32": (6963287662 / 209715200, 208640),   # 33.20
-    "quadrotor/mixed": (6449554461 / 209715200, 198656),  # 30.75
+    # workload: (warp-inst per rollout-step, DRAM bytes per launch) of the
+    # kernel rollout_kernel_name() names for the workload's launch shape
+    "batch": (492249088 / 52428800, 267776),          # 9.39  mppi_rollout_early_b128
+    "uneven": (182619694 / 16410677, 128085),         # 11.13 mppi_rollout_work_b128
+    "single": (584832 / 30720, 51328),                # 19.04 mppi_rollout_coop32 (4 lanes/sample)
+    "quadrotor/fp32": (6955357806 / 209715200, 235904),   # 33.17 mppi_rollout_b128
+    "quadrotor/mixed": (6440772637 / 209715200, 270720),  # 30.71 mppi_rollout_b128
 }
 
 
