@@ -9,8 +9,10 @@
 //                                           1: sigma = Cholesky factor L
 //   MPPI_CONTROL_COST                       1: add lambda * u_nom^T Sigma^-1 eps
 //   MPPI_NOISE_HALF                         1: noise drawn with approximate
-//                                           transcendentals, rounded to FP16,
-//                                           staged in FP16 (kFp16 / kMixed)
+//                                           transcendentals (four 16-bit
+//                                           uniforms per Philox call for
+//                                           m >= 3), rounded to FP16, staged
+//                                           in FP16 (kFp16 / kMixed)
 //   MPPI_DYNAMICS_FN / _STAGE_COST_FN / _TERMINAL_COST_FN   callable names
 //   MPPI_MP_BYTES / MPPI_CP_BYTES           ParamLayout blob sizes
 //   MPPI_PROPOSAL                           1: a share of the samples draws
@@ -217,11 +219,32 @@ __device__ __forceinline__ float clampf(float v, float lo, float hi) {
 // Standard normals n[0..m) and shaped noise eps[0..m) of sample k at time t.
 // Pair p of step t uses counter (step, k*H*P + t*P + p); its first normal is
 // dim 2p, its second dim 2p+1 (dropped for odd m).
+// Half-precision noise with three or more controls: one Philox call per
+// four normals (mppi_box_muller_fast16), call q of step t at counter
+// (step, k*H*Q + t*Q + q), Q = ceil(m/4); its word x gives dims 4q, 4q+1,
+// word y dims 4q+2, 4q+3.
+constexpr bool kNoise16 = MPPI_NOISE_HALF && kM >= 3;
+constexpr int kQ = (kM + 3) / 4;
+
 __device__ __forceinline__ void sample_noise(uint32_t step, uint32_t key, uint32_t k,
                                              uint32_t H, uint32_t t, const float (&sig)[kSig],
                                              float (&n)[2 * kP], float (&eps)[kM]) {
+  if constexpr (kNoise16) {
 #pragma unroll
-  for (int p = 0; p < kP; ++p) {
+    for (int q = 0; q < kQ; ++q) {
+      const uint2 w = mppi_philox2x32_10(make_uint2(step, mppi_noise_ctr(k, H, kQ, t, q)), key);
+      const float2 g0 = mppi_box_muller_fast16(w.x);
+      n[4 * q] = g0.x;
+      if (4 * q + 1 < kM) n[4 * q + 1] = g0.y;
+      if (4 * q + 2 < kM) {
+        const float2 g1 = mppi_box_muller_fast16(w.y);
+        n[4 * q + 2] = g1.x;
+        if (4 * q + 3 < kM) n[4 * q + 3] = g1.y;
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < (kNoise16 ? 0 : kP); ++p) {
     const uint2 w = mppi_philox2x32_10(make_uint2(step, mppi_noise_ctr(k, H, kP, t, p)), key);
 #if MPPI_NOISE_HALF
     const float2 g = mppi_box_muller_fast(w);

@@ -311,6 +311,21 @@ __device__ __forceinline__ float2 mppi_box_muller_fast(uint2 w) {
   return make_float2(-r * c, -r * s);
 }
 
+// The same from one 32-bit Philox word split into two 16-bit uniforms,
+// u = (h + 1/2) 2^-16 (lower half u1, upper half u2), for the half-precision
+// noise mode of models with three or more controls: 16 bits of uniform
+// suffice for a normal rounded to 11 significant bits, so one Philox call
+// gives four normals instead of two (its tails end at 4.9 sigma, where
+// u1 = 2^-17).
+__device__ __forceinline__ float2 mppi_box_muller_fast16(uint32_t w) {
+  const float u1 = __fmul_rn(__fadd_rn(__uint2float_rn(w & 0xffffu), 0.5f), 0x1p-16f);
+  const float u2 = __fmul_rn(__fadd_rn(__uint2float_rn(w >> 16), 0.5f), 0x1p-16f);
+  const float r = mppi_sqrt_approx(-2.0f * __logf(u1));
+  float s, c;
+  __sincosf(6.28318530717958647692f * (u2 - 0.5f), &s, &c);
+  return make_float2(-r * c, -r * s);
+}
+
 // Reference-compatible spellings for plugins ported from MSL
 // (examples/wez_environment_batch/wez_environment.metal:166-173 draws with
 // philox2x32_10 / uint_to_01 inside its dynamics).

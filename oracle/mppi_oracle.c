@@ -75,16 +75,35 @@ int oracle_cholesky(uint32_t m, const double* a, double* l) {
  *   ctr = (step, k*H*P + t*P + d/2), P = ceil(m/2), key = agent key;
  *   the pair's first normal goes to dim d (even), the second to d+1.
  * Shaping: diagonal eps_d = n_d * sigma_d (sigma = std-dev); full covariance
- * eps = L n with L the Cholesky factor of sigma (project extension). */
+ * eps = L n with L the Cholesky factor of sigma (project extension).
+ * Half-precision noise modes with m >= 3 (project extension, the device's
+ * mppi_box_muller_fast16): ctr = (step, k*H*Q + t*Q + q), Q = ceil(m/4); each
+ * 32-bit word gives two 16-bit uniforms u = (h + 1/2) / 65536 (lower half
+ * u1, upper u2) and one Box-Muller pair: word x dims 4q, 4q+1, word y dims
+ * 4q+2, 4q+3; the shaped value is rounded to binary16. */
 void oracle_sample_noise(const oracle_problem* p, uint32_t step, uint32_t key,
                          uint32_t k, const double* sigma, double* normals,
                          double* eps) {
   const uint32_t H = p->horizon, m = p->control_dim, P = (m + 1) / 2;
   double L[MAX_CTRL * MAX_CTRL];
   if (p->cov_full) oracle_cholesky(m, sigma, L);
+  const int noise16 = p->noise_half && m >= 3; /* four 16-bit uniforms per call */
+  const uint32_t Q = (m + 3) / 4;
   for (uint32_t t = 0; t < H; ++t) {
-    double n[MAX_CTRL + 1];
-    for (uint32_t d = 0; d < m; d += 2) {
+    double n[MAX_CTRL + 4];
+    for (uint32_t q = 0; noise16 && q < Q; ++q) {
+      const uint32_t c1 = k * H * Q + t * Q + q; /* uint32 wrap as on the device */
+      uint32_t w[2];
+      oracle_philox2x32_10(step, c1, key, w);
+      for (int h = 0; h < 2; ++h) {
+        const double u1 = ((double)(w[h] & 0xffffu) + 0.5) / 65536.0;
+        const double u2 = ((double)(w[h] >> 16) + 0.5) / 65536.0;
+        const double r = sqrt(-2.0 * log(u1));
+        n[4 * q + 2 * h] = r * cos(2.0 * ORACLE_PI * u2);
+        n[4 * q + 2 * h + 1] = r * sin(2.0 * ORACLE_PI * u2);
+      }
+    }
+    for (uint32_t d = 0; !noise16 && d < m; d += 2) {
       const uint32_t pair = t * P + d / 2;
       const uint32_t c1 = k * H * P + pair; /* uint32 wrap as on the device */
       uint32_t w[2];
