@@ -3,7 +3,8 @@
 The noise is drawn with the SM's approximate transcendentals and rounded
 once to FP16; rollout and update use that rounded value.  Checked against
 the oracle restating the same method (its FP64 noise rounded to FP16), on the
-quadrotor model (m = 4, two Philox pairs per step):
+quadrotor model (m = 4: one Philox call per step, its two words split into
+four 16-bit uniforms):
   shaped noise      within one FP16 rounding step of the oracle's, plus
                     2e-3 * sigma absolute (approximate log near u1 -> 1)
   costs, u_next     on the device's own noise, the oracle's rollout reproduces
