@@ -204,6 +204,15 @@ __device__ __forceinline__ void acc_cost(float& hi, float& lo, float x) {
   lo += err;
 }
 
+// A load through L2 that the compiler keeps where it is written (volatile
+// asm): the combine issues its reads of other CTAs' records ahead of the
+// statistics that wait on them, so they overlap instead of following.
+__device__ __forceinline__ float ld_early(const float* p) {
+  float v;
+  asm volatile("ld.global.cg.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+
 // The pair as one double (exact: |lo| is far below hi's last bit times 2^29).
 __device__ __forceinline__ double cost_pair(float hi, float lo) {
   return (double)hi + (double)lo;
@@ -935,6 +944,13 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   __shared__ double min_s;
 #ifdef MPPI_FEATURES_FN
   __shared__ float feat_s[MPPI_MAX_FEATURES];  // the next step's network input
+#if MPPI_CP_SMEM
+  // the agent's cost parameters for the feature callable, copied in by all
+  // threads at the start (one thread runs the callable, and its reads then
+  // hit shared memory instead of L2)
+  __shared__ __align__(16) uint32_t fcp_s[(MPPI_CP_BYTES + 3) / 4];
+  if (a.features) copy_words(fcp_s, a.cost_params + a.cost_stride * agent, MPPI_CP_BYTES);
+#endif
 #endif
   const uint32_t tid = threadIdx.x;
   const bool ragged = a.agent_K != nullptr;
@@ -955,11 +971,11 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   float h0 = 0.0f, l0 = 0.0f, e0 = 0.0f, q0 = 0.0f, c0 = 0.0f;
   if (tid < 32 && tid < nblk) {
     const float* pb = P + (size_t)tid * ps;
-    h0 = __ldcg(pb);
-    l0 = __ldcg(pb + 4);
-    e0 = __ldcg(pb + 1);
-    q0 = __ldcg(pb + 2);
-    c0 = __ldcg(pb + 3);
+    h0 = ld_early(pb);
+    l0 = ld_early(pb + 4);
+    e0 = ld_early(pb + 1);
+    q0 = ld_early(pb + 2);
+    c0 = ld_early(pb + 3);
   }
   // Read ahead, before the statistics are known (one round trip to L2
   // instead of three): each thread's first weighted-sum column of every
@@ -973,19 +989,19 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
   if (pre) {
 #pragma unroll
     for (uint32_t b = 0; b < kPre; ++b)
-      pv[b] = b < nblk ? __ldcg(P + (size_t)b * ps + MPPI_PARTIAL_HEAD + tid) : 0.0f;
-    un_pre = un[tid];
+      pv[b] = b < nblk ? ld_early(P + (size_t)b * ps + MPPI_PARTIAL_HEAD + tid) : 0.0f;
+    un_pre = ld_early(un + tid);
   }
   float x_pre[kPreX ? kN : 1];
   uint32_t step_pre = 0;
   if (kPreX && tid == 0 && a.propagate) {
 #pragma unroll
-    for (int d = 0; d < (kPreX ? kN : 1); ++d) x_pre[d] = a.x[(size_t)agent * kN + d];
+    for (int d = 0; d < (kPreX ? kN : 1); ++d) x_pre[d] = ld_early(a.x + (size_t)agent * kN + d);
   }
   if (PRE > 0 && tid == 0 && a.propagate) step_pre = *a.step_base + a.step_local;
   // the bounds of this thread's first column (its control dimension)
-  const float lo_pre = PRE > 0 && tid < HM ? a.u_min[tid % kM] : 0.0f;
-  const float hi_pre = PRE > 0 && tid < HM ? a.u_max[tid % kM] : 0.0f;
+  const float lo_pre = PRE > 0 && tid < HM ? ld_early(a.u_min + tid % kM) : 0.0f;
+  const float hi_pre = PRE > 0 && tid < HM ? ld_early(a.u_max + tid % kM) : 0.0f;
 
   // Statistics over the CTA records by warp 0 alone (lane l takes records
   // l, l + 32, ...), so the summation order -- and every bit of the result --
@@ -1113,8 +1129,12 @@ __device__ __forceinline__ void combine_agent(const MppiCombineArgs& a, uint32_t
     // the next step's proposal features, from the state just propagated
     if (a.features) {
       float f[MPPI_MAX_FEATURES];
-      compute_features(st, a.model_params + a.model_stride * agent,
-                       a.cost_params + a.cost_stride * agent, f);
+#if MPPI_CP_SMEM
+      const uint8_t* fcp = reinterpret_cast<const uint8_t*>(fcp_s);
+#else
+      const uint8_t* fcp = a.cost_params + a.cost_stride * agent;
+#endif
+      compute_features(st, a.model_params + a.model_stride * agent, fcp, f);
       float* o = a.features + (size_t)agent * a.feature_stride;
 #pragma unroll
       for (int i = 0; i < MPPI_MAX_FEATURES; ++i) {
