@@ -873,7 +873,8 @@ __device__ __noinline__ void network_row(const float* f, const MppiNetRows& net,
     float* hout = h_s[l & 1];
     const uint4* W = reinterpret_cast<const uint4*>(net.w[l]);
     // two outputs per pass (n and n + nt), their weight loads issued in
-    // batches of 8 k-blocks each, so 16 loads are in flight per thread
+    // batches of 8 k-blocks each, so 16 loads are in flight per thread (one
+    // output: batches of 16 of its k-blocks)
     for (uint32_t n0 = tid; n0 < N; n0 += 2 * nt) {
       const uint32_t n1 = n0 + nt;
       const bool two = n1 < N;
@@ -882,39 +883,47 @@ __device__ __noinline__ void network_row(const float* f, const MppiNetRows& net,
       const uint4* wr1 = W + (size_t)(n1 >> 3) * K + (n1 & 7u);
       float acc0[4] = {0.0f, 0.0f, 0.0f, 0.0f}, acc1[4] = {0.0f, 0.0f, 0.0f, 0.0f};
       const uint32_t nb = K / 8;
-      for (uint32_t b0 = 0; b0 < nb; b0 += 8) {
+      // one k-block (8 inputs) of one output into its partial sum b mod 4
+      auto block = [&](float (&acc)[4], const uint4& w, uint32_t b) {
+        const float4 h0 = *reinterpret_cast<const float4*>(hin + 8 * b);
+        const float4 h1 = *reinterpret_cast<const float4*>(hin + 8 * b + 4);
+        float& s = acc[b & 3u];
+        s = fmaf(bf16_lo(w.x), h0.x, s);
+        s = fmaf(bf16_hi(w.x), h0.y, s);
+        s = fmaf(bf16_lo(w.y), h0.z, s);
+        s = fmaf(bf16_hi(w.y), h0.w, s);
+        s = fmaf(bf16_lo(w.z), h1.x, s);
+        s = fmaf(bf16_hi(w.z), h1.y, s);
+        s = fmaf(bf16_lo(w.w), h1.z, s);
+        s = fmaf(bf16_hi(w.w), h1.w, s);
+      };
+      // with one output, the second bank of loads holds its next 8 k-blocks
+      // (16 in flight either way); the blocks still go in ascending order
+      const uint32_t step = two ? 8u : 16u;
+      for (uint32_t b0 = 0; b0 < nb; b0 += step) {
         uint4 w0[8], w1[8];
 #pragma unroll
         for (uint32_t i = 0; i < 8; ++i) {
-          const bool in = b0 + i < nb;
-          w0[i] = in ? __ldg(wr0 + 8 * (b0 + i)) : make_uint4(0u, 0u, 0u, 0u);
-          w1[i] = (in && two) ? __ldg(wr1 + 8 * (b0 + i)) : make_uint4(0u, 0u, 0u, 0u);
+          const bool in0 = b0 + i < nb, in1 = two ? in0 : b0 + 8 + i < nb;
+          w0[i] = in0 ? __ldg(wr0 + 8 * (b0 + i)) : make_uint4(0u, 0u, 0u, 0u);
+          w1[i] = in1 ? __ldg(two ? wr1 + 8 * (b0 + i) : wr0 + 8 * (b0 + 8 + i))
+                      : make_uint4(0u, 0u, 0u, 0u);
         }
+        if (two) {
 #pragma unroll
-        for (uint32_t i = 0; i < 8; ++i) {
-          const uint32_t b = b0 + i;
-          if (b < nb) {
-            const float4 h0 = *reinterpret_cast<const float4*>(hin + 8 * b);
-            const float4 h1 = *reinterpret_cast<const float4*>(hin + 8 * b + 4);
-            float& s0 = acc0[b & 3u];
-            float& s1 = acc1[b & 3u];
-            s0 = fmaf(bf16_lo(w0[i].x), h0.x, s0);
-            s1 = fmaf(bf16_lo(w1[i].x), h0.x, s1);
-            s0 = fmaf(bf16_hi(w0[i].x), h0.y, s0);
-            s1 = fmaf(bf16_hi(w1[i].x), h0.y, s1);
-            s0 = fmaf(bf16_lo(w0[i].y), h0.z, s0);
-            s1 = fmaf(bf16_lo(w1[i].y), h0.z, s1);
-            s0 = fmaf(bf16_hi(w0[i].y), h0.w, s0);
-            s1 = fmaf(bf16_hi(w1[i].y), h0.w, s1);
-            s0 = fmaf(bf16_lo(w0[i].z), h1.x, s0);
-            s1 = fmaf(bf16_lo(w1[i].z), h1.x, s1);
-            s0 = fmaf(bf16_hi(w0[i].z), h1.y, s0);
-            s1 = fmaf(bf16_hi(w1[i].z), h1.y, s1);
-            s0 = fmaf(bf16_lo(w0[i].w), h1.z, s0);
-            s1 = fmaf(bf16_lo(w1[i].w), h1.z, s1);
-            s0 = fmaf(bf16_hi(w0[i].w), h1.w, s0);
-            s1 = fmaf(bf16_hi(w1[i].w), h1.w, s1);
+          for (uint32_t i = 0; i < 8; ++i) {
+            if (b0 + i < nb) {
+              block(acc0, w0[i], b0 + i);
+              block(acc1, w1[i], b0 + i);
+            }
           }
+        } else {
+#pragma unroll
+          for (uint32_t i = 0; i < 8; ++i)
+            if (b0 + i < nb) block(acc0, w0[i], b0 + i);
+#pragma unroll
+          for (uint32_t i = 0; i < 8; ++i)
+            if (b0 + 8 + i < nb) block(acc0, w1[i], b0 + 8 + i);
         }
       }
       const float z0 = ((acc0[0] + acc0[1]) + (acc0[2] + acc0[3])) + net.b[l][n0];
