@@ -65,7 +65,7 @@ ROLLOUT_COUNTERS = {
     "uneven": (182619694 / 16410677, 128085),         # 11.13 mppi_rollout_work_b128
     "single": (584832 / 30720, 51328),                # 19.04 mppi_rollout_coop32 (4 lanes/sample)
     "quadrotor/fp32": (6955357806 / 209715200, 235904),   # 33.17 mppi_rollout_b128
-    "quadrotor/mixed": (6440772637 / 209715200, 270720),  # 30.71 mppi_rollout_b128
+    "quadrotor/mixed": (6147972631 / 209715200, 438528),  # 29.32 mppi_rollout_b128 (16-bit uniforms)
 }
 
 
