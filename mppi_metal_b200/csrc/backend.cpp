@@ -192,6 +192,9 @@ struct mppi_backend {
   // MPPI_B200_COOP=1 / 0 pins the cooperative form on / off (0 = the shape
   // rule of choose_geometry)
   int coop_pin = 0;
+  // MPPI_B200_NO_EARLY_NOISE=1: the 128-sample one-thread forms draw their
+  // noise after the grid wait (the same bits; for comparisons)
+  bool no_early = false;
   // MPPI_B200_NET_PER_AGENT=1 / 0 pins the proposal network's form (0 = by
   // the batch size, kNetPerAgentMax)
   int net_pin = 0;
@@ -737,8 +740,9 @@ cudaError_t launch_dependent(const mppi_backend* b, const void* func, dim3 grid,
 // entry, because the early path's extra live state cost the chunked
 // quadrotor rollout 132 bytes of spills.
 bool early_noise(const mppi_backend* b) {
-  return !b->ragged && !b->geom.coop && b->geom.variant == 1 && b->geom.block == 128 &&
-         b->geom.stage_rows >= b->HM() && !(b->proposal && b->spec.proposal);
+  return !b->no_early && !b->ragged && !b->geom.coop && b->geom.variant == 1 &&
+         b->geom.block == 128 && b->geom.stage_rows >= b->HM() &&
+         !(b->proposal && b->spec.proposal);
 }
 
 // A rollout launch with prepared arguments (uniform grid, or the uneven
@@ -1161,6 +1165,8 @@ int mppi_backend_create(mppi_backend** out) {
       (*out)->coop_pin = *co == '0' ? -1 : 1;
     if (const char* np = getenv("MPPI_B200_NET_PER_AGENT"); np && *np)
       (*out)->net_pin = *np == '0' ? -1 : 1;
+    if (const char* ne = getenv("MPPI_B200_NO_EARLY_NOISE"); ne && *ne && *ne != '0')
+      (*out)->no_early = true;
   }
   return *out ? MPPI_OK : MPPI_ERR_INVALID;
 }
